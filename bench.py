@@ -1,0 +1,382 @@
+"""Benchmark: kernel evaluations/s of the tiled fixed-bandwidth KDE on B200.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mgk|reference]
+                  [--workload single_large] [--scale S]
+
+Workload (default): the single large KDE — 1,000,000 points from a
+50-component Gaussian mixture in a 10,000 x 10,000 domain with lognormal(0,
+0.5) weights, density raster 10,000 x 10,000 at cell 1 under a random
+polygon mask (~80 % valid), edge-correction raster 2,500 x 2,500 at cell 4
+with the same polygon, h = 50, FP32-compensated.  Seeded synthetic data.
+
+One step = the whole path over device-resident inputs: boundary marking,
+point-to-boundary distances, edge-correction weights, index build, density
+over the full raster.  Unit of work = one kernel evaluation, i.e. one
+(point, target) pair inside the 3h cutoff, target = valid density cell or
+valid edge-mask cell; the count is algorithmic (the kernels count exactly the
+oracle's pairs).  value = evals of all ranks / max-over-ranks step time.
+
+Multi-GPU (torchrun): the path shards by tiles with no exchange; rank r runs
+its own tile band of the study (a workload with seed 1 + r), so per-GPU work
+is fixed (weak scaling) and no collective touches the data path.
+
+--impl reference times the reference program's own CPU path (built from its
+sources into oracle/_ref; the FP64 oracle port if that binary is absent) on
+the host cores, on bounded crops of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+sys.path.insert(0, os.path.join(REPO, "oracle"))
+
+from mgpukde_tiled_b200 import synth  # noqa: E402
+
+METRIC = "kernel evals/s (FP32-compensated, rel err <= 1e-6 vs FP64 oracle)"
+UNIT = "evals/s"
+REF_BIN = os.path.join(REPO, "oracle", "_ref", "mgkde_ref")
+FLOP_PER_EVAL = 8.0  # 7 FP32 flops + 1 exp per in-cutoff pair (algorithmic)
+
+
+def env_rank():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def load_peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f), "measured"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                      "--format=csv,noheader,nounits", "-lms", "200"],
+                                     stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_workload(name, scale, seed):
+    if name != "single_large":
+        raise SystemExit(f"unknown workload {name}")
+    c = synth.single_large(scale=scale, seed=seed)
+    dg = c["density_grid"]
+    c["density_mask"] = synth.rasterize_polygon(c["polygon"], dg)
+    return c
+
+
+# ------------------------------------------------------------------ CPU legs --
+def crop_inputs(c, side):
+    """A side x side window at the centre of the density raster, its halo
+    points (within 3h) and their slice of everything."""
+    dg = c["density_grid"]
+    r0 = (dg.nrows - side) // 2
+    c0 = (dg.ncols - side) // 2
+    x0 = dg.xll + c0 * dg.cs
+    x1 = x0 + side * dg.cs
+    y1 = dg.yll + (dg.nrows - r0) * dg.cs
+    y0 = y1 - side * dg.cs
+    reach = 3.0 * c["h"]
+    x, y = c["x"], c["y"]
+    keep = (x > x0 - reach) & (x < x1 + reach) & (y > y0 - reach) & (y < y1 + reach)
+    g = synth.Grid(side, side, np.float32(x0), np.float32(y0), dg.cs, dg.nodata)
+    return dict(x=x[keep], y=y[keep], w=c["w"][keep], grid=g, mask=c["density_mask"][r0:r0 + side, c0:c0 + side],
+                window=(r0, c0, side, side))
+
+
+def crop_evals(c, crop):
+    import oracle_py as o
+    eg = o.grid(*c["edge_grid"].astuple())
+    b = o.mark_boundary(eg, c["edge_mask"])
+    d2 = o.dist2_boundary(crop["x"], crop["y"], eg, b)
+    ew, eev = o.edge_weights(crop["x"], crop["y"], c["h"], d2, eg, c["edge_mask"])
+    _, dev = o.density(crop["x"], crop["y"], crop["w"], ew, c["h"], o.grid(*crop["grid"].astuple()), crop["mask"])
+    return dev, eev, ew
+
+
+def run_reference_binary(c, crop, threads):
+    from mgpukde_tiled_b200 import tiff
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "p.csv"), "w") as f:
+            f.write("x,y,h,w\n")
+            for a, b, w in zip(crop["x"], crop["y"], crop["w"]):
+                f.write("%.9g,%.9g,%.9g,%.9g\n" % (a, b, c["h"], w))
+        eg = c["edge_grid"]
+        tiff.write(os.path.join(d, "e.tif"), tiff.GeoRaster(c["edge_mask"], (float(eg.xll), float(eg.cs), 0.0,
+                   float(eg.yll) + eg.nrows * float(eg.cs), 0.0, -float(eg.cs)), eg.nodata))
+        g = crop["grid"]
+        tiff.write(os.path.join(d, "d.tif"), tiff.GeoRaster(crop["mask"], (float(g.xll), float(g.cs), 0.0,
+                   float(g.yll) + g.nrows * float(g.cs), 0.0, -float(g.cs)), g.nodata))
+        p = subprocess.run([REF_BIN, "1", "p.csv", "e.tif", "d.tif", "-1", "1", "1", "0", "1", str(threads), "1",
+                            "den_cpu.tif", "den_gpu.tif", "0"], cwd=d, capture_output=True, text=True, timeout=1800)
+        if p.returncode != 0:
+            raise RuntimeError(p.stdout[-1000:] + p.stderr[-1000:])
+        t_den = float(re.search(r"KernelDesityEstimation took (\d+) ms", p.stdout).group(1))
+        t_edge = float(re.search(r"EdgeCorrectionWeightsExact took (\d+) ms", p.stdout).group(1))
+        return (t_den + t_edge) / 1e3
+
+
+def cpu_baseline(c, side=384):
+    """The reference's CPU path (or the FP64 oracle port) on a crop of the workload."""
+    threads = os.cpu_count() or 1
+    crop = crop_inputs(c, side)
+    dev, eev, ew = crop_evals(c, crop)
+    if os.path.exists(REF_BIN):
+        t = run_reference_binary(c, crop, threads)
+        kind = "reference"
+    else:
+        import oracle_py as o
+        o.set_threads(threads)
+        t0 = time.perf_counter()
+        o.density(crop["x"], crop["y"], crop["w"], ew, c["h"], o.grid(*crop["grid"].astuple()), crop["mask"])
+        t = time.perf_counter() - t0
+        kind = "port"
+    sample = (f"{side}x{side} density window at the raster centre with its {len(crop['x'])} halo points "
+              f"(density + edge-correction evals {dev + eev}); reference brute-force CPU path, "
+              f"{'mode 1, h_option -1' if kind == 'reference' else 'FP64 oracle'}")
+    return {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+            "seconds": t}
+
+
+def run_reference_arm(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return 0
+    c = build_workload(args.workload, args.scale, seed=1)
+    side = 256
+    vals = []
+    for k in range(args.warmup + args.steps):
+        cb = cpu_baseline(c, side)
+        if k >= args.warmup:
+            vals.append(cb)
+    v = float(np.mean([b["value"] for b in vals]))
+    secs = float(np.mean([b["seconds"] for b in vals]))
+    cb = dict(vals[-1])
+    cb["value"] = v
+    out = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": secs * 1e3, "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
+           "config": config_of(args), "cpu_baseline": cb,
+           "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out))
+    return 0
+
+
+def config_of(args):
+    return {"workload": f"{args.workload}: 1e6 mixture points (50 comps) in 1e4^2, lognormal weights, "
+                        f"density 1e4^2 @ cell 1 polygon mask, edge mask 2500^2 @ cell 4, h=50"
+                        + ("" if args.scale == 1.0 else f" (scaled x{args.scale})"),
+            "scale": args.scale, "tile": "whole raster (one tile)", "parallelism": f"tiles x{args.gpus} (no exchange)",
+            "l2": "inputs larger than L2 (density mask and output 400 MB each)"}
+
+
+# ------------------------------------------------------------------ GPU arm --
+def run_mgk(args):
+    import torch
+    import torch.distributed as dist
+
+    import mgpukde_tiled_b200 as mk
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
+    c = build_workload(args.workload, args.scale, seed=1 + rank)
+    dg, eg = mk.Grid.of(c["density_grid"]), mk.Grid.of(c["edge_grid"])
+    h = float(c["h"])
+    stream = torch.cuda.current_stream()
+    ctx = mk.Context(local, stream=stream)
+    dev = "cuda"
+    dx = torch.from_numpy(c["x"]).to(dev)
+    dy = torch.from_numpy(c["y"]).to(dev)
+    dw = torch.from_numpy(c["w"]).to(dev)
+    demask = torch.from_numpy(c["edge_mask"]).to(dev)
+    ddmask = torch.from_numpy(c["density_mask"]).to(dev)
+    dout = torch.empty((dg.nrows, dg.ncols), dtype=torch.float32, device=dev)
+    pts = mk.Points.wrap(ctx, dx, dy, dw)
+    em = mk.Raster.wrap(ctx, eg, demask)
+
+    def step(count=False):
+        mk.mark_boundary(ctx, em)
+        mk.calc_dist2_boundary(ctx, pts, em)
+        ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=count)
+        idx = mk.Index(ctx, pts, h)
+        ev_d = mk.density_tile(ctx, idx, dg, 0, 0, dg.nrows, dg.ncols, ddmask, dout, count=count)
+        idx.close()
+        return ev_e, ev_d
+
+    ev_e, ev_d = step(count=True)
+    evals = ev_e + ev_d
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dens_ms = []
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        dens_ms.append(ctx.last_density_ms)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    launches = (ctx.kernel_launches - l0) / args.steps
+    ms = e0.elapsed_time(e1) / args.steps
+    t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    ms_max = float(t.item())
+    total_evals = evals * world
+    value = total_evals / (ms_max / 1e3)
+
+    # end to end: the C ABI from pinned host buffers (inputs H2D and the raster D2H every step)
+    hx = torch.from_numpy(c["x"]).pin_memory()
+    hy = torch.from_numpy(c["y"]).pin_memory()
+    hw = torch.from_numpy(c["w"]).pin_memory()
+    hem = torch.from_numpy(c["edge_mask"]).pin_memory()
+    hdm = torch.from_numpy(c["density_mask"]).pin_memory()
+    hout = torch.empty((dg.nrows, dg.ncols), dtype=torch.float32).pin_memory()
+    e2e_steps = max(1, min(args.steps, 5))
+
+    def e2e_step():
+        mk.kde_raster(ctx, hx.numpy(), hy.numpy(), hw.numpy(), h, dg, hdm.numpy(), eg, hem.numpy(),
+                      out=hout.numpy())
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = torch.tensor([e0.elapsed_time(e1) / e2e_steps], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
+    e2e_val = total_evals / (float(e2e_ms.item()) / 1e3)
+    h2d = 4 * (3 * len(c["x"]) + c["edge_mask"].size + c["density_mask"].size)
+    d2h = 4 * dg.nrows * dg.ncols
+
+    # roofline of the density kernel (FP32-issue bound; no measured FP32 peak exists, nominal used)
+    peaks, peak_kind = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    nsm = torch.cuda.get_device_properties(local).multi_processor_count
+    fp32_peak_tflops = nsm * 128 * 2 * sm_max * 1e6 / 1e12
+    dens_s = float(np.mean(dens_ms)) / 1e3
+    achieved = ev_d * FLOP_PER_EVAL / dens_s / 1e12
+    traffic = None
+    tp = os.path.join(REPO, "profiles", "density_traffic.json")
+    if os.path.exists(tp):
+        with open(tp) as f:
+            tj = json.load(f)
+        traffic = tj.get("bytes_per_launch_scaled")
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)", "config": config_of(args),
+        "evals_per_step_per_gpu": evals, "density_evals": ev_d, "edge_evals": ev_e,
+        "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                "ms_per_step": float(e2e_ms.item())},
+        "gpu_launches": launches,
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
+                     "frac": achieved / fp32_peak_tflops, "traffic": traffic, "kernel": "k_density",
+                     "kernel_ms": dens_s * 1e3, "flop_per_eval": FLOP_PER_EVAL,
+                     "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                                  f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"},
+        "clocks": clocks,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            out["cpu_baseline"] = cpu_baseline(c)
+        except Exception as e:  # reported, not fatal
+            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(out))
+    pts.close()
+    em.close()
+    ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="mgk", choices=["mgk", "reference"])
+    ap.add_argument("--workload", default="single_large")
+    ap.add_argument("--scale", type=float, default=1.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference_arm(args)
+    return run_mgk(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

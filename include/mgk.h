@@ -1,0 +1,204 @@
+/*
+ * mgk.h — C ABI of the B200 (sm_100a) tiled fixed-bandwidth Gaussian KDE.
+ *
+ * The reference (mGPUKDE_tiled) has no plugin layer: its host driver launches
+ * CUDA kernels that take POD structs by value holding raw device pointers
+ * (SamplePoints, SamplePoints.h:9-17; AsciiRaster, AsciiRaster.h:9-33) and
+ * calls host functions over them.  Each entry point below replaces one of
+ * those launches or host functions; the citation says which.
+ *
+ * Conventions
+ *  - Every function returns an int status: 0 (MGK_OK) or a negative MGK_ERR_*.
+ *    Nothing calls exit(); mgk_ctx_last_error() gives the message.
+ *  - Work is ordered on the context's CUDA stream (mgk_ctx_set_stream).
+ *    Functions that return host-side results (counts, log likelihoods)
+ *    synchronise that stream before returning.
+ *  - Rasters are row-major with row 0 at the top, NoData passed through, as
+ *    in the reference.  Cell centres: x = xll + (col + 0.5) cs,
+ *    y = yll + (nrows - 0.5 - row) cs, computed in double and rounded to float
+ *    (Utilities.h:13-14).
+ *  - Device memory a context allocates counts against its HBM budget; a
+ *    request beyond it fails with MGK_ERR_BUDGET and leaves the device usable.
+ *  - One context per host thread.
+ */
+#ifndef MGK_H
+#define MGK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MGK_OK 0
+#define MGK_ERR_INVALID (-1)   /* bad argument */
+#define MGK_ERR_CUDA (-2)      /* CUDA runtime error */
+#define MGK_ERR_BUDGET (-3)    /* HBM budget exceeded */
+#define MGK_ERR_NO_DEVICE (-4) /* no CUDA device / wrong architecture */
+#define MGK_ERR_TIMEOUT (-5)   /* a bounded device-side wait ran out */
+#define MGK_ERR_IO (-6)        /* file read/write failure (host driver) */
+
+/* Raster geometry: the fields of AsciiRaster (AsciiRaster.h:9-33) that the
+ * path reads. */
+typedef struct mgk_grid {
+    int64_t ncols;
+    int64_t nrows;
+    float xll;
+    float yll;
+    float cs;
+    float nodata;
+} mgk_grid;
+
+typedef struct mgk_ctx mgk_ctx;       /* device, stream, HBM budget, last error */
+typedef struct mgk_points mgk_points; /* device-resident SamplePoints + per-point h, dist2, edge weights */
+typedef struct mgk_raster mgk_raster; /* device-resident mask raster (AsciiRaster) */
+typedef struct mgk_index mgk_index;   /* cell-binned point index (replaces KDtree/CUDA_KDTree) */
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Replaces the device selection and per-GPU stream setup of main()
+ * (kde_cuda_kdtr_tiled.cu:366-400).  hbm_budget_bytes = 0 means "free
+ * memory at creation".  Fails with MGK_ERR_NO_DEVICE unless the device is
+ * compute capability 10.x. */
+int mgk_ctx_create(int device, uint64_t hbm_budget_bytes, mgk_ctx** out);
+int mgk_ctx_destroy(mgk_ctx* ctx);
+/* Use an external stream (cudaStream_t as void*); NULL = the context's own. */
+int mgk_ctx_set_stream(mgk_ctx* ctx, void* cuda_stream);
+int mgk_ctx_synchronize(mgk_ctx* ctx);
+const char* mgk_ctx_last_error(const mgk_ctx* ctx);
+uint64_t mgk_ctx_bytes_in_use(const mgk_ctx* ctx);
+const char* mgk_status_string(int status);
+/* Instrumentation (no reference counterpart; the reference prints wall-clock
+ * phase timings, kde_cuda_kdtr_tiled.cu:994, 1521): number of kernels this
+ * context has launched, and the device time in ms of the last density
+ * kernel (CUDA events on the context stream around that one launch). */
+uint64_t mgk_ctx_kernel_launches(const mgk_ctx* ctx);
+float mgk_ctx_last_density_ms(const mgk_ctx* ctx);
+
+/* ---- points (SamplePoints) --------------------------------------------- */
+
+/* Host -> device copy of a point set; replaces AllocateDeviceSamplePoints +
+ * CopyToDeviceSamplePoints (kde_cuda_kdtr_tiled.cu:1713-1805) and the
+ * bandwidth upload (CopyToDeviceBandwidths).  w == NULL: unit weights.
+ * h == NULL: a fixed bandwidth is given per call; else per-point h
+ * (h_option -1, kde_cuda_kdtr_tiled.cu:413-421). */
+int mgk_points_upload(mgk_ctx* ctx, int64_t n, const float* x, const float* y,
+                      const float* w, const float* h, mgk_points** out);
+/* Same over caller-owned device arrays (no copy; they must outlive the
+ * handle).  dist2 / edge-weight storage is still allocated by the library. */
+int mgk_points_wrap(mgk_ctx* ctx, int64_t n, const float* d_x, const float* d_y,
+                    const float* d_w, const float* d_h, mgk_points** out);
+int mgk_points_destroy(mgk_points* pts);
+/* Device pointers of a point set (any may be NULL on output when absent):
+ * x, y, w, h (float), dist2 (double, squared distance to the boundary),
+ * ew (float, edge-correction weight). */
+int mgk_points_device_arrays(const mgk_points* pts, const float** x, const float** y,
+                             const float** w, const float** h, const double** dist2,
+                             const float** ew);
+/* Device -> host copy of the per-point results (either may be NULL);
+ * replaces ReformECWeights / CopyFromDevice* (kde_cuda_kdtr_tiled.cu:4589-4646). */
+int mgk_points_download(mgk_points* pts, double* dist2, float* ew);
+
+/* ---- rasters (AsciiRaster) -------------------------------------------- */
+
+/* Host -> device mask raster; replaces AllocateDeviceAsciiRaster +
+ * CopyToDeviceAsciiRaster (kde_cuda_kdtr_tiled.cu:2264-2373). */
+int mgk_raster_upload(mgk_ctx* ctx, const mgk_grid* g, const float* mask, mgk_raster** out);
+int mgk_raster_wrap(mgk_ctx* ctx, const mgk_grid* g, const float* d_mask, mgk_raster** out);
+int mgk_raster_destroy(mgk_raster* r);
+
+/* ---- boundary and distance --------------------------------------------- */
+
+/* dMarkBoundary + MarkBoundary (kde_kernel_kdtr.cu:1209-1281,
+ * kde_cuda_kdtr_tiled.cu:3956-3992): marks boundary cells of the mask and
+ * keeps their centres with the raster.  n_boundary (optional, host) gets the
+ * count. */
+int mgk_mark_boundary(mgk_ctx* ctx, mgk_raster* mask, int64_t* n_boundary);
+/* Optional copy of the boundary flags (uint8 per cell, row-major). */
+int mgk_raster_boundary_download(mgk_raster* mask, uint8_t* out);
+/* dCalcDist2Boundary + CalcDist2Boundary (kde_kernel_kdtr.cu:1285-1353,
+ * kde_cuda_kdtr_tiled.cu:4072-4137): exact FP64 squared distance from every
+ * point to the nearest boundary-cell centre (DBL_MAX when there is none).
+ * Marks the boundary first if mgk_mark_boundary has not run. */
+int mgk_boundary_dist(mgk_ctx* ctx, mgk_points* pts, mgk_raster* mask);
+
+/* ---- edge correction --------------------------------------------------- */
+
+/* CalcEdgeCorrectionWeights, both overloads (kde_kernel_kdtr.cu:117-265;
+ * CPU twins kde_cuda_kdtr_tiled.cu:2694-2807): weight 1 when dist2 >= 9 h^2,
+ * else 1 / sum over valid mask cells with d^2 < 9 h^2 of K_h(d) * cellArea.
+ * h > 0: fixed bandwidth; h <= 0: the points' per-point h.  Requires
+ * mgk_boundary_dist first (else MGK_ERR_INVALID).  evals (optional, host)
+ * receives the number of in-cutoff (point, cell) pairs. */
+int mgk_edge_weights(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h,
+                     int64_t* evals);
+/* Sets every edge weight to 1 (edge correction off; InitdWeights,
+ * kde_kernel_kdtr.cu:665-676). */
+int mgk_edge_weights_unit(mgk_ctx* ctx, mgk_points* pts);
+
+/* ---- cell-binned index -------------------------------------------------- */
+
+/* Replaces BuildCPUKDtree + BuildGPUKDtree (kde_cuda_kdtr_tiled.cu:4241-4275,
+ * CUDA_KDtree.cu:26-102) and the per-tile halo filter ExtractSamplePointsCurTile
+ * (kde_cuda_kdtr_tiled.cu:4672-4747): points are counting-sorted (stable LSD
+ * radix sort) into square bins of side bin_size (0 = chosen from h) and
+ * stored bin-major with w * e folded in.  h > 0: fixed h; h <= 0: per-point h.
+ * The index snapshots the points' current edge weights. */
+int mgk_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float bin_size, mgk_index** out);
+int mgk_index_destroy(mgk_index* idx);
+
+/* ---- density ------------------------------------------------------------ */
+
+/* KernelDesityEstimation_pPoints + InitCellDensities (kde_kernel_kdtr.cu:
+ * 268-294, 461-574) for one tile: rows [row0, row0+nr) x cols [col0, col0+nc)
+ * of the raster geometry g.  d_mask_tile: nr*nc floats, NoData cells are
+ * passed through (NULL = every cell valid).  d_out: nr*nc floats, density of
+ * valid cells (intensity, not probability).  evals (optional, host): number
+ * of in-cutoff (point, cell) pairs (synchronises). */
+int mgk_density_tile(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
+                     int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,
+                     float* d_out, int64_t* evals);
+/* Same with the plain FP64 form of the kernel (double throughout, no
+ * compensation): the comparator the FP32-compensated kernel is measured
+ * against. */
+int mgk_density_tile_fp64(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
+                          int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,
+                          float* d_out, int64_t* evals);
+
+/* ---- bandwidth selection ---------------------------------------------- */
+
+/* Batched LogLikelihood (kde_cuda_kdtr_tiled.cu:3214-3299) over nh fixed
+ * bandwidths in one pass: for each h, edge weights at h (when mask != NULL;
+ * needs mgk_boundary_dist), then
+ *   logL(h) = sum_j log(max(sum_{i != j, d^2 < 9h^2} K_h(d) w_i e_i(h), 1e-14f))
+ * reduced in FP64.  logL: nh doubles (host).  argmax (optional, host): index
+ * of the largest logL. */
+int mgk_loo_loglik_batch(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask,
+                         const float* h_grid, int nh, double* logL, int* argmax);
+/* MLE_FixedBandWidth (kde_cuda_kdtr_tiled.cu:3044-3093): golden-section
+ * search on [h0/20, 2 h0], at most 30 iterations, two logL evaluations per
+ * iteration (each one batched launch of nh=2); returns the bracket midpoint. */
+int mgk_mle_fixed_bandwidth(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h0,
+                            float* h_opt, int* iterations);
+/* Rule-of-thumb bandwidth (kde_cuda_kdtr_tiled.cu:64-68, 1563-1595), host
+ * arithmetic identical to the reference's. */
+float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w);
+
+/* ---- whole path from host buffers ------------------------------------- */
+
+/* The GPU section of main() (kde_cuda_kdtr_tiled.cu:877-1521) for one raster
+ * held in host memory: upload, boundary + distance + edge weights (when
+ * edge_correction), index, tiled density, download.  h_pp == NULL: fixed h.
+ * dens_mask == NULL: every density cell valid.  out_density: host,
+ * nrows*ncols of dens_g.  out_ew (optional): per-point edge weights.
+ * evals (optional): density + edge-correction in-cutoff pairs. */
+int mgk_kde_raster(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* w,
+                   const float* h_pp, float h, int edge_correction, const mgk_grid* edge_g,
+                   const float* edge_mask, const mgk_grid* dens_g, const float* dens_mask,
+                   int64_t tile_side, float* out_density, float* out_ew, int64_t* evals);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MGK_H */

@@ -1,0 +1,94 @@
+"""Loader and ctypes signatures of libmgk.so (include/mgk.h).
+
+The library is built in-tree (python -m mgpukde_tiled_b200.build).  There is
+no fallback: if it is missing or cannot be loaded, every call raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libmgk.so")
+
+MGK_OK = 0
+STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "HBM budget exceeded",
+          -4: "no suitable CUDA device", -5: "device wait timed out", -6: "I/O error"}
+
+# Every symbol include/mgk.h declares.
+EXPORTS = [
+    "mgk_ctx_create", "mgk_ctx_destroy", "mgk_ctx_set_stream", "mgk_ctx_synchronize",
+    "mgk_ctx_last_error", "mgk_ctx_bytes_in_use", "mgk_status_string",
+    "mgk_ctx_kernel_launches", "mgk_ctx_last_density_ms",
+    "mgk_points_upload", "mgk_points_wrap", "mgk_points_destroy", "mgk_points_device_arrays",
+    "mgk_points_download", "mgk_raster_upload", "mgk_raster_wrap", "mgk_raster_destroy",
+    "mgk_mark_boundary", "mgk_raster_boundary_download", "mgk_boundary_dist",
+    "mgk_edge_weights", "mgk_edge_weights_unit", "mgk_index_build", "mgk_index_destroy",
+    "mgk_density_tile", "mgk_density_tile_fp64", "mgk_loo_loglik_batch",
+    "mgk_mle_fixed_bandwidth", "mgk_rule_of_thumb", "mgk_kde_raster",
+]
+
+
+class MgkGrid(C.Structure):
+    _fields_ = [("ncols", C.c_int64), ("nrows", C.c_int64), ("xll", C.c_float),
+                ("yll", C.c_float), ("cs", C.c_float), ("nodata", C.c_float)]
+
+
+class MgkError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"mgk status {status} ({STATUS.get(status, '?')}): {msg}")
+        self.status = status
+
+
+_lib = None
+
+
+def lib():
+    """Loads libmgk.so; raises if it is absent (there is no CPU fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m mgpukde_tiled_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    P, I64, I = C.c_void_p, C.c_int64, C.c_int
+    PP = C.POINTER(C.c_void_p)
+    G = C.POINTER(MgkGrid)
+    sig = {
+        "mgk_ctx_create": (I, [I, C.c_uint64, PP]),
+        "mgk_ctx_destroy": (I, [P]),
+        "mgk_ctx_set_stream": (I, [P, P]),
+        "mgk_ctx_synchronize": (I, [P]),
+        "mgk_ctx_last_error": (C.c_char_p, [P]),
+        "mgk_ctx_bytes_in_use": (C.c_uint64, [P]),
+        "mgk_status_string": (C.c_char_p, [I]),
+        "mgk_ctx_kernel_launches": (C.c_uint64, [P]),
+        "mgk_ctx_last_density_ms": (C.c_float, [P]),
+        "mgk_points_upload": (I, [P, I64, P, P, P, P, PP]),
+        "mgk_points_wrap": (I, [P, I64, P, P, P, P, PP]),
+        "mgk_points_destroy": (I, [P]),
+        "mgk_points_device_arrays": (I, [P, PP, PP, PP, PP, PP, PP]),
+        "mgk_points_download": (I, [P, P, P]),
+        "mgk_raster_upload": (I, [P, G, P, PP]),
+        "mgk_raster_wrap": (I, [P, G, P, PP]),
+        "mgk_raster_destroy": (I, [P]),
+        "mgk_mark_boundary": (I, [P, P, C.POINTER(I64)]),
+        "mgk_raster_boundary_download": (I, [P, P]),
+        "mgk_boundary_dist": (I, [P, P, P]),
+        "mgk_edge_weights": (I, [P, P, P, C.c_float, C.POINTER(I64)]),
+        "mgk_edge_weights_unit": (I, [P, P]),
+        "mgk_index_build": (I, [P, P, C.c_float, C.c_float, PP]),
+        "mgk_index_destroy": (I, [P]),
+        "mgk_density_tile": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
+        "mgk_density_tile_fp64": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
+        "mgk_loo_loglik_batch": (I, [P, P, P, P, I, P, C.POINTER(I)]),
+        "mgk_mle_fixed_bandwidth": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(I)]),
+        "mgk_rule_of_thumb": (C.c_float, [I64, P, P, P]),
+        "mgk_kde_raster": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, P, I64, P, P, C.POINTER(I64)]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L

@@ -1,0 +1,573 @@
+// C ABI of libmgk (include/mgk.h): contexts, device-resident objects, and the
+// host-side sequencing of the path (the GPU section of the reference's
+// main(), kde_cuda_kdtr_tiled.cu:877-1521, for one GPU).
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "mgk_internal.cuh"
+
+// ---------------------------------------------------------------- helpers --
+int mgk_fail(mgk_ctx* ctx, int status, const std::string& msg) {
+    if (ctx) ctx->last_error = msg;
+    return status;
+}
+
+int mgk_cuda_fail(mgk_ctx* ctx, cudaError_t e, const char* what) {
+    (void)cudaGetLastError();  // clear sticky-less errors
+    return mgk_fail(ctx, e == cudaErrorMemoryAllocation ? MGK_ERR_BUDGET : MGK_ERR_CUDA,
+                    std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes) {
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    if (ctx->in_use + bytes > ctx->budget)
+        return mgk_fail(ctx, MGK_ERR_BUDGET,
+                        "HBM budget exceeded: need " + std::to_string(bytes) + " B, in use " +
+                            std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget));
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return mgk_cuda_fail(ctx, e, "cudaMalloc");
+    }
+    ctx->in_use += bytes;
+    return MGK_OK;
+}
+
+void mgk_free(mgk_ctx* ctx, void* p, size_t bytes) {
+    if (!p) return;
+    if (bytes == 0) bytes = 16;
+    cudaFree(p);
+    ctx->in_use -= std::min<uint64_t>(ctx->in_use, bytes);
+}
+
+extern "C" {
+
+const char* mgk_status_string(int status) {
+    switch (status) {
+        case MGK_OK: return "ok";
+        case MGK_ERR_INVALID: return "invalid argument";
+        case MGK_ERR_CUDA: return "CUDA error";
+        case MGK_ERR_BUDGET: return "HBM budget exceeded";
+        case MGK_ERR_NO_DEVICE: return "no suitable CUDA device";
+        case MGK_ERR_TIMEOUT: return "device wait timed out";
+        case MGK_ERR_IO: return "I/O error";
+        default: return "unknown status";
+    }
+}
+
+// ---------------------------------------------------------------- context --
+int mgk_ctx_create(int device, uint64_t hbm_budget_bytes, mgk_ctx** out) {
+    if (!out) return MGK_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        (void)cudaGetLastError();
+        return MGK_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return MGK_ERR_INVALID;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess) return MGK_ERR_NO_DEVICE;
+    if (prop.major != 10) return MGK_ERR_NO_DEVICE;  // built for sm_100a only
+    if (cudaSetDevice(device) != cudaSuccess) return MGK_ERR_CUDA;
+    mgk_ctx* c = new (std::nothrow) mgk_ctx();
+    if (!c) return MGK_ERR_INVALID;
+    c->device = device;
+    c->sm_count = prop.multiProcessorCount;
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    c->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)fr;
+    if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return MGK_ERR_CUDA;
+    }
+    c->stream = c->own_stream;
+    if (cudaMalloc(&c->d_counter, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMalloc(&c->d_sum, 256 * sizeof(double)) != cudaSuccess ||
+        cudaMallocHost(&c->h_counter, 8 * sizeof(unsigned long long)) != cudaSuccess ||
+        cudaMallocHost(&c->h_sum, 256 * sizeof(double)) != cudaSuccess ||
+        cudaEventCreate(&c->ev_a) != cudaSuccess || cudaEventCreate(&c->ev_b) != cudaSuccess) {
+        mgk_ctx_destroy(c);
+        return MGK_ERR_CUDA;
+    }
+    *out = c;
+    return MGK_OK;
+}
+
+int mgk_ctx_destroy(mgk_ctx* c) {
+    if (!c) return MGK_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->d_counter) cudaFree(c->d_counter);
+    if (c->d_sum) cudaFree(c->d_sum);
+    if (c->h_counter) cudaFreeHost(c->h_counter);
+    if (c->h_sum) cudaFreeHost(c->h_sum);
+    if (c->ev_a) cudaEventDestroy(c->ev_a);
+    if (c->ev_b) cudaEventDestroy(c->ev_b);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+    return MGK_OK;
+}
+
+int mgk_ctx_set_stream(mgk_ctx* c, void* stream) {
+    if (!c) return MGK_ERR_INVALID;
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    return MGK_OK;
+}
+
+int mgk_ctx_synchronize(mgk_ctx* c) {
+    if (!c) return MGK_ERR_INVALID;
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MGK_OK;
+}
+
+const char* mgk_ctx_last_error(const mgk_ctx* c) { return c ? c->last_error.c_str() : "no context"; }
+
+uint64_t mgk_ctx_bytes_in_use(const mgk_ctx* c) { return c ? c->in_use : 0; }
+
+uint64_t mgk_ctx_kernel_launches(const mgk_ctx* c) { return c ? c->launches : 0; }
+
+float mgk_ctx_last_density_ms(const mgk_ctx* c) { return c ? c->last_density_ms : 0.0f; }
+
+// ----------------------------------------------------------------- points --
+static int points_alloc_results(mgk_ctx* c, mgk_points* p) {
+    int st;
+    if ((st = mgk_alloc(c, (void**)&p->dist2, sizeof(double) * std::max<int64_t>(p->n, 1)))) return st;
+    if ((st = mgk_alloc(c, (void**)&p->ew, sizeof(float) * std::max<int64_t>(p->n, 1)))) return st;
+    return MGK_OK;
+}
+
+int mgk_points_upload(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h,
+                      mgk_points** out) {
+    if (!c || !out || n < 0 || (n > 0 && (!x || !y))) return mgk_fail(c, MGK_ERR_INVALID, "points_upload: bad arguments");
+    if (n >= (int64_t)INT32_MAX) return mgk_fail(c, MGK_ERR_INVALID, "points_upload: at most 2^31-1 points");
+    mgk_points* p = new (std::nothrow) mgk_points();
+    if (!p) return MGK_ERR_INVALID;
+    p->ctx = c;
+    p->n = n;
+    p->owns_xywh = true;
+    const size_t b = sizeof(float) * (size_t)std::max<int64_t>(n, 1);
+    int st = MGK_OK;
+    if ((st = mgk_alloc(c, (void**)&p->x, b)) || (st = mgk_alloc(c, (void**)&p->y, b)) ||
+        (w && (st = mgk_alloc(c, (void**)&p->w, b))) || (h && (st = mgk_alloc(c, (void**)&p->h, b))) ||
+        (st = points_alloc_results(c, p))) {
+        mgk_points_destroy(p);
+        return st;
+    }
+    const size_t nb = sizeof(float) * (size_t)n;
+    cudaStream_t s = c->stream;
+    cudaError_t e = cudaSuccess;
+    if (n > 0) {
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p->x, x, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(p->y, y, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && w) e = cudaMemcpyAsync(p->w, w, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && h) e = cudaMemcpyAsync(p->h, h, nb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // host buffers may be pageable/temporary
+    }
+    if (e != cudaSuccess) {
+        mgk_points_destroy(p);
+        return mgk_cuda_fail(c, e, "points_upload");
+    }
+    *out = p;
+    return MGK_OK;
+}
+
+int mgk_points_wrap(mgk_ctx* c, int64_t n, const float* d_x, const float* d_y, const float* d_w, const float* d_h,
+                    mgk_points** out) {
+    if (!c || !out || n < 0 || (n > 0 && (!d_x || !d_y))) return mgk_fail(c, MGK_ERR_INVALID, "points_wrap: bad arguments");
+    if (n >= (int64_t)INT32_MAX) return mgk_fail(c, MGK_ERR_INVALID, "points_wrap: at most 2^31-1 points");
+    mgk_points* p = new (std::nothrow) mgk_points();
+    if (!p) return MGK_ERR_INVALID;
+    p->ctx = c;
+    p->n = n;
+    p->owns_xywh = false;
+    p->x = const_cast<float*>(d_x);
+    p->y = const_cast<float*>(d_y);
+    p->w = const_cast<float*>(d_w);
+    p->h = const_cast<float*>(d_h);
+    int st = points_alloc_results(c, p);
+    if (st) {
+        mgk_points_destroy(p);
+        return st;
+    }
+    *out = p;
+    return MGK_OK;
+}
+
+int mgk_points_destroy(mgk_points* p) {
+    if (!p) return MGK_OK;
+    mgk_ctx* c = p->ctx;
+    const size_t b = sizeof(float) * (size_t)std::max<int64_t>(p->n, 1);
+    if (p->owns_xywh) {
+        mgk_free(c, p->x, b);
+        mgk_free(c, p->y, b);
+        mgk_free(c, p->w, b);
+        mgk_free(c, p->h, b);
+    }
+    mgk_free(c, p->dist2, sizeof(double) * (size_t)std::max<int64_t>(p->n, 1));
+    mgk_free(c, p->ew, b);
+    delete p;
+    return MGK_OK;
+}
+
+int mgk_points_device_arrays(const mgk_points* p, const float** x, const float** y, const float** w,
+                             const float** h, const double** dist2, const float** ew) {
+    if (!p) return MGK_ERR_INVALID;
+    if (x) *x = p->x;
+    if (y) *y = p->y;
+    if (w) *w = p->w;
+    if (h) *h = p->h;
+    if (dist2) *dist2 = p->has_dist2 ? p->dist2 : nullptr;
+    if (ew) *ew = p->has_ew ? p->ew : nullptr;
+    return MGK_OK;
+}
+
+int mgk_points_download(mgk_points* p, double* dist2, float* ew) {
+    if (!p) return MGK_ERR_INVALID;
+    mgk_ctx* c = p->ctx;
+    cudaStream_t s = c->stream;
+    if (dist2) {
+        if (!p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "points_download: no distances computed");
+        MGK_CHECK_CUDA(c, cudaMemcpyAsync(dist2, p->dist2, sizeof(double) * p->n, cudaMemcpyDeviceToHost, s));
+    }
+    if (ew) {
+        if (!p->has_ew) return mgk_fail(c, MGK_ERR_INVALID, "points_download: no edge weights computed");
+        MGK_CHECK_CUDA(c, cudaMemcpyAsync(ew, p->ew, sizeof(float) * p->n, cudaMemcpyDeviceToHost, s));
+    }
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(s));
+    return MGK_OK;
+}
+
+// ----------------------------------------------------------------- raster --
+static bool grid_ok(const mgk_grid* g) {
+    return g && g->ncols > 0 && g->nrows > 0 && g->cs > 0.0f && std::isfinite(g->cs) && std::isfinite(g->xll) &&
+           std::isfinite(g->yll);
+}
+
+int mgk_raster_upload(mgk_ctx* c, const mgk_grid* g, const float* mask, mgk_raster** out) {
+    if (!c || !out || !grid_ok(g) || !mask) return mgk_fail(c, MGK_ERR_INVALID, "raster_upload: bad arguments");
+    mgk_raster* r = new (std::nothrow) mgk_raster();
+    if (!r) return MGK_ERR_INVALID;
+    r->ctx = c;
+    r->g = *g;
+    r->owns = true;
+    const size_t b = sizeof(float) * (size_t)g->ncols * (size_t)g->nrows;
+    int st = mgk_alloc(c, (void**)&r->mask, b);
+    if (st) {
+        delete r;
+        return st;
+    }
+    cudaError_t e = cudaMemcpyAsync(r->mask, mask, b, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) {
+        mgk_raster_destroy(r);
+        return mgk_cuda_fail(c, e, "raster_upload");
+    }
+    *out = r;
+    return MGK_OK;
+}
+
+int mgk_raster_wrap(mgk_ctx* c, const mgk_grid* g, const float* d_mask, mgk_raster** out) {
+    if (!c || !out || !grid_ok(g) || !d_mask) return mgk_fail(c, MGK_ERR_INVALID, "raster_wrap: bad arguments");
+    mgk_raster* r = new (std::nothrow) mgk_raster();
+    if (!r) return MGK_ERR_INVALID;
+    r->ctx = c;
+    r->g = *g;
+    r->owns = false;
+    r->mask = const_cast<float*>(d_mask);
+    *out = r;
+    return MGK_OK;
+}
+
+int mgk_raster_destroy(mgk_raster* r) {
+    if (!r) return MGK_OK;
+    mgk_ctx* c = r->ctx;
+    const size_t ncell = (size_t)r->g.ncols * (size_t)r->g.nrows;
+    if (r->owns) mgk_free(c, r->mask, sizeof(float) * ncell);
+    mgk_free(c, r->boundary, ncell);
+    mgk_free(c, r->bcells, sizeof(float2) * (size_t)r->nb);
+    delete r;
+    return MGK_OK;
+}
+
+// --------------------------------------------------------------- boundary --
+int mgk_mark_boundary(mgk_ctx* c, mgk_raster* r, int64_t* n_boundary) {
+    if (!c || !r) return mgk_fail(c, MGK_ERR_INVALID, "mark_boundary: bad arguments");
+    int st = mgk_launch_mark_boundary(c, r);
+    if (st) return st;
+    if (n_boundary) *n_boundary = r->nb;
+    return MGK_OK;
+}
+
+int mgk_raster_boundary_download(mgk_raster* r, uint8_t* out) {
+    if (!r || !out) return MGK_ERR_INVALID;
+    mgk_ctx* c = r->ctx;
+    if (!r->marked) return mgk_fail(c, MGK_ERR_INVALID, "boundary not marked");
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(out, r->boundary, (size_t)r->g.ncols * r->g.nrows, cudaMemcpyDeviceToHost, c->stream));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    return MGK_OK;
+}
+
+int mgk_boundary_dist(mgk_ctx* c, mgk_points* p, mgk_raster* r) {
+    if (!c || !p || !r) return mgk_fail(c, MGK_ERR_INVALID, "boundary_dist: bad arguments");
+    int st;
+    if (!r->marked && (st = mgk_launch_mark_boundary(c, r))) return st;
+    if ((st = mgk_launch_dist2(c, p, r))) return st;
+    p->has_dist2 = true;
+    return MGK_OK;
+}
+
+// ------------------------------------------------------------ edge weights --
+static int fetch_counter(mgk_ctx* c, int64_t* out) {
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(c->h_counter, c->d_counter, sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                                      c->stream));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    *out = (int64_t)c->h_counter[0];
+    return MGK_OK;
+}
+
+int mgk_edge_weights(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, int64_t* evals) {
+    if (!c || !p || !r) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: bad arguments");
+    if (!p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: run mgk_boundary_dist first");
+    if (h <= 0.0f && !p->h) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: no bandwidth");
+    if (evals) MGK_CHECK_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
+    int st = mgk_launch_edge_weights(c, p->n, p->x, p->y, h > 0.0f ? nullptr : p->h, h, p->dist2, r, p->ew,
+                                     evals ? c->d_counter : nullptr);
+    if (st) return st;
+    p->has_ew = true;
+    if (evals) return fetch_counter(c, evals);
+    return MGK_OK;
+}
+
+__global__ static void k_fill1(int64_t n, float* a) {
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) a[i] = 1.0f;
+}
+
+int mgk_edge_weights_unit(mgk_ctx* c, mgk_points* p) {
+    if (!c || !p) return MGK_ERR_INVALID;
+    if (p->n) k_fill1<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->n, p->ew);
+    MGK_CHECK_LAUNCH(c, "k_fill1");
+    if (p->n) MGK_COUNT_LAUNCH(c, 1);
+    p->has_ew = true;
+    return MGK_OK;
+}
+
+// ------------------------------------------------------------------ index --
+int mgk_index_build(mgk_ctx* c, const mgk_points* p, float h, float bin_size, mgk_index** out) {
+    if (!c || !p || !out) return mgk_fail(c, MGK_ERR_INVALID, "index_build: bad arguments");
+    mgk_index* idx = new (std::nothrow) mgk_index();
+    if (!idx) return MGK_ERR_INVALID;
+    int st = mgk_launch_index_build(c, p, h, bin_size, idx);
+    if (st) {
+        mgk_index_destroy(idx);
+        return st;
+    }
+    *out = idx;
+    return MGK_OK;
+}
+
+int mgk_index_destroy(mgk_index* idx) {
+    if (!idx) return MGK_OK;
+    mgk_ctx* c = idx->ctx;
+    if (c) {
+        const size_t n1 = (size_t)std::max<int64_t>(idx->n, 1);
+        mgk_free(c, idx->bin_start, sizeof(int32_t) * (size_t)(idx->nbx * idx->nby + 1));
+        mgk_free(c, idx->pts, sizeof(float4) * n1);
+        mgk_free(c, idx->hk, sizeof(double2) * n1);
+        mgk_free(c, idx->perm, sizeof(int32_t) * n1);
+    }
+    delete idx;
+    return MGK_OK;
+}
+
+// ---------------------------------------------------------------- density --
+static int density_common(mgk_ctx* c, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                          int64_t nr, int64_t nc, const float* d_mask, float* d_out, int64_t* evals, bool fp64) {
+    if (!c || !idx || !grid_ok(g) || !d_out) return mgk_fail(c, MGK_ERR_INVALID, "density_tile: bad arguments");
+    if (row0 < 0 || col0 < 0 || nr < 0 || nc < 0 || row0 + nr > g->nrows || col0 + nc > g->ncols)
+        return mgk_fail(c, MGK_ERR_INVALID, "density_tile: tile outside the raster");
+    if (evals) MGK_CHECK_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
+    int st = mgk_launch_density(c, idx, g, row0, col0, nr, nc, d_mask, d_out, evals ? c->d_counter : nullptr, fp64);
+    if (st) return st;
+    if (evals) return fetch_counter(c, evals);
+    return MGK_OK;
+}
+
+int mgk_density_tile(mgk_ctx* c, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0, int64_t nr,
+                     int64_t nc, const float* d_mask, float* d_out, int64_t* evals) {
+    return density_common(c, idx, g, row0, col0, nr, nc, d_mask, d_out, evals, false);
+}
+
+int mgk_density_tile_fp64(mgk_ctx* c, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                          int64_t nr, int64_t nc, const float* d_mask, float* d_out, int64_t* evals) {
+    if (evals) *evals = -1;  // the FP64 form does not count
+    return density_common(c, idx, g, row0, col0, nr, nc, d_mask, d_out, nullptr, true);
+}
+
+// ------------------------------------------------------------ bandwidths --
+float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w) {
+    // MeanCenter (float accumulators), StandardDistance2 (double), BandWidth2,
+    // kde_cuda_kdtr_tiled.cu:64-68, 1563-1595.  Host code built for baseline
+    // x86-64 (no FMA instructions), so each operation rounds on its own as in
+    // the reference.
+    float sum_x = 0.0f, sum_y = 0.0f, sum_w = 0.0f;
+    for (int64_t p = 0; p < n; p++) {
+        const float wp = w ? w[p] : 1.0f;
+        sum_w += wp;
+        sum_x += wp * x[p];
+        sum_y += wp * y[p];
+    }
+    const float mx = sum_x / sum_w, my = sum_y / sum_w;
+    double s2 = 0.0, sw = 0.0;
+    for (int64_t p = 0; p < n; p++) {
+        const float wp = w ? w[p] : 1.0f;
+        sw += wp;
+        const double dx = (double)(x[p] - mx);
+        const double dy = (double)(y[p] - my);
+        s2 += wp * (dx * dx + dy * dy);
+    }
+    const double d2 = s2 / sw;
+    const unsigned int three_n = 3u * (unsigned int)n;
+    const double bw2 = (double)sqrtf(2.0f / (float)three_n) * d2;
+    return sqrtf((float)bw2);
+}
+
+// evaluates logL at each h; the index over the points (unit edge weights) is shared
+static int loglik_many(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const float* hs, int nh, double* logl) {
+    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
+    float hmin = FLT_MAX;
+    for (int k = 0; k < nh; k++) {
+        if (!(hs[k] > 0.0f) || !std::isfinite(hs[k])) return mgk_fail(c, MGK_ERR_INVALID, "loo: bandwidths must be positive");
+        hmin = std::min(hmin, hs[k]);
+    }
+    mgk_points view = *p;  // index over w only; e(h) is applied per h
+    view.has_ew = false;
+    view.h = nullptr;
+    mgk_index* idx = nullptr;
+    int st = mgk_index_build(c, &view, hmin, 1.5f * hmin, &idx);
+    if (st) return st;
+    float* ew = nullptr;
+    if (r && (st = mgk_alloc(c, (void**)&ew, sizeof(float) * std::max<int64_t>(p->n, 1)))) {
+        mgk_index_destroy(idx);
+        return st;
+    }
+    for (int k = 0; k < nh && st == MGK_OK; k++) {
+        if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, hs[k], p->dist2, r, ew, nullptr);
+        if (st == MGK_OK) st = mgk_launch_loo(c, idx, r ? ew : nullptr, hs[k], c->d_sum, nullptr);
+        if (st == MGK_OK) {
+            cudaError_t e = cudaMemcpy(&logl[k], c->d_sum, sizeof(double), cudaMemcpyDeviceToHost);
+            if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "loo result");
+        }
+    }
+    if (ew) mgk_free(c, ew, sizeof(float) * std::max<int64_t>(p->n, 1));
+    mgk_index_destroy(idx);
+    return st;
+}
+
+int mgk_loo_loglik_batch(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const float* h_grid, int nh, double* logl,
+                         int* argmax) {
+    if (!c || !p || !h_grid || nh <= 0 || !logl) return mgk_fail(c, MGK_ERR_INVALID, "loo_loglik_batch: bad arguments");
+    int st = loglik_many(c, p, r, h_grid, nh, logl);
+    if (st) return st;
+    if (argmax) {
+        int best = 0;
+        for (int k = 1; k < nh; k++)
+            if (logl[k] > logl[best]) best = k;
+        *argmax = best;
+    }
+    return MGK_OK;
+}
+
+int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h0, float* h_opt, int* iterations) {
+    if (!c || !p || !h_opt || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "mle_fixed_bandwidth: bad arguments");
+    // MLE_FixedBandWidth, kde_cuda_kdtr_tiled.cu:3044-3093 (float bracket arithmetic)
+    float hA = h0 / 20;
+    float hD = 2 * h0;
+    float width = hD - hA;
+    const float epsilon = width / 100;
+    const float factor = 1 + sqrtf(5.0f);
+    int it = 0;
+    while (width > epsilon && it < 30) {
+        const float hB = hA + width / factor;
+        const float hC = hD - width / factor;
+        const float hh[2] = {hB, hC};
+        double l[2];
+        int st = loglik_many(c, p, r, hh, 2, l);
+        if (st) return st;
+        if (l[0] > l[1]) hD = hC;
+        else hA = hB;
+        width = hD - hA;
+        it++;
+    }
+    *h_opt = (hA + hD) / 2;
+    if (iterations) *iterations = it;
+    return MGK_OK;
+}
+
+// ---------------------------------------------------------- whole raster --
+int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp, float h,
+                   int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
+                   const float* dmask, int64_t tile_side, float* out_density, float* out_ew, int64_t* evals) {
+    if (!c || !grid_ok(dg) || !out_density || (edge_correction && (!grid_ok(eg) || !emask)) ||
+        (!h_pp && !(h > 0.0f)))
+        return mgk_fail(c, MGK_ERR_INVALID, "kde_raster: bad arguments");
+    mgk_points* p = nullptr;
+    mgk_raster* em = nullptr;
+    mgk_index* idx = nullptr;
+    float *d_mask = nullptr, *d_out = nullptr;
+    int64_t ev_edge = 0, ev_den = 0;
+    const float hfix = h_pp ? 0.0f : h;
+    int st = mgk_points_upload(c, n, x, y, w, h_pp, &p);
+    if (st == MGK_OK) {
+        if (edge_correction) {
+            if ((st = mgk_raster_upload(c, eg, emask, &em)) == MGK_OK && (st = mgk_boundary_dist(c, p, em)) == MGK_OK)
+                st = mgk_edge_weights(c, p, em, hfix, evals ? &ev_edge : nullptr);
+        } else {
+            st = mgk_edge_weights_unit(c, p);
+        }
+    }
+    if (st == MGK_OK) st = mgk_index_build(c, p, hfix, 0.0f, &idx);
+    if (st == MGK_OK && out_ew) {
+        cudaError_t e = cudaMemcpyAsync(out_ew, p->ew, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "kde_raster ew");
+    }
+    // tile loop (kde_cuda_kdtr_tiled.cu:1373-1517): row-major tiles
+    const int64_t T = tile_side > 0 ? tile_side : std::max<int64_t>(dg->ncols, dg->nrows);
+    const int64_t tr = std::min<int64_t>(T, dg->nrows), tc = std::min<int64_t>(T, dg->ncols);
+    const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_out, tb);
+    if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask, tb);
+    for (int64_t r0 = 0; st == MGK_OK && r0 < dg->nrows; r0 += tr) {
+        for (int64_t c0 = 0; st == MGK_OK && c0 < dg->ncols; c0 += tc) {
+            const int64_t nr = std::min<int64_t>(tr, dg->nrows - r0), nc = std::min<int64_t>(tc, dg->ncols - c0);
+            cudaError_t e = cudaSuccess;
+            if (dmask)
+                e = cudaMemcpy2DAsync(d_mask, sizeof(float) * nc, dmask + r0 * dg->ncols + c0, sizeof(float) * dg->ncols,
+                                      sizeof(float) * nc, nr, cudaMemcpyHostToDevice, c->stream);
+            if (e != cudaSuccess) { st = mgk_cuda_fail(c, e, "kde_raster mask"); break; }
+            int64_t ev = 0;
+            st = mgk_density_tile(c, idx, dg, r0, c0, nr, nc, d_mask, d_out, evals ? &ev : nullptr);
+            if (st) break;
+            ev_den += ev;
+            e = cudaMemcpy2DAsync(out_density + r0 * dg->ncols + c0, sizeof(float) * dg->ncols, d_out,
+                                  sizeof(float) * nc, sizeof(float) * nc, nr, cudaMemcpyDeviceToHost, c->stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+            if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "kde_raster tile");
+        }
+    }
+    if (d_out) mgk_free(c, d_out, tb);
+    if (d_mask) mgk_free(c, d_mask, tb);
+    mgk_index_destroy(idx);
+    mgk_raster_destroy(em);
+    mgk_points_destroy(p);
+    if (st == MGK_OK && evals) *evals = ev_den + ev_edge;
+    return st;
+}
+
+}  // extern "C"

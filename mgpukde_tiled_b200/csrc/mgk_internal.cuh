@@ -1,0 +1,156 @@
+// Internal declarations shared by the CUDA translation units of libmgk.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <string>
+
+#include "../../include/mgk.h"
+
+// ---- constants of the reference (Utilities.h) -----------------------------
+// TWO_PI is a float constant in the reference (Utilities.h:8).
+#define MGK_TWO_PI_F 6.2831853071795862f
+// EPSILONDENSITY (Utilities.h:20), a float constant.
+#define MGK_EPS_DENSITY_F 0.00000000000001f
+// CUT_OFF_FACTOR (Utilities.h:27): the kernel is zero for d^2 >= 9 h^2.
+#define MGK_CUT 9.0
+#define MGK_LOG2E 1.4426950408889634
+#define MGK_LN2F 0.69314718055994531f
+
+// ---- host-side objects -----------------------------------------------------
+struct mgk_ctx {
+    int device = 0;
+    int sm_count = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    uint64_t budget = 0;
+    uint64_t in_use = 0;
+    std::string last_error;
+    // small pinned/device scratch for scalar results
+    unsigned long long* d_counter = nullptr;  // 8 counters
+    unsigned long long* h_counter = nullptr;  // pinned mirror
+    double* d_sum = nullptr;                  // 256 doubles
+    double* h_sum = nullptr;                  // pinned mirror
+    uint64_t launches = 0;                    // kernels launched by this context
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+    float last_density_ms = 0.0f;
+};
+
+#define MGK_COUNT_LAUNCH(ctx, k) ((ctx)->launches += (k))
+
+struct mgk_points {
+    mgk_ctx* ctx = nullptr;
+    int64_t n = 0;
+    float *x = nullptr, *y = nullptr, *w = nullptr, *h = nullptr;
+    bool owns_xywh = false;
+    double* dist2 = nullptr;
+    bool has_dist2 = false;
+    float* ew = nullptr;
+    bool has_ew = false;
+};
+
+struct mgk_raster {
+    mgk_ctx* ctx = nullptr;
+    mgk_grid g{};
+    float* mask = nullptr;
+    bool owns = false;
+    uint8_t* boundary = nullptr;  // per cell
+    float2* bcells = nullptr;     // boundary-cell centres (compacted)
+    int64_t nb = 0;
+    bool marked = false;
+};
+
+struct mgk_index {
+    mgk_ctx* ctx = nullptr;
+    int64_t n = 0;
+    bool varh = false;
+    // fixed-h constants (double): h^2 as the reference forms it, 9 h^2,
+    // log2(e)/(2 h^2), 1/(h^2 TWO_PI), 3 h
+    float h = 0.0f;
+    double h2 = 0, cut_d2 = 0, k2 = 0, k0 = 0, reach = 0;
+    // bin grid
+    double ox = 0, oy = 0, side = 1;
+    int64_t nbx = 1, nby = 1;
+    int32_t* bin_start = nullptr;  // nbx*nby + 1
+    // bin-major point data
+    float4* pts = nullptr;   // x, y, w*e (fixed h) or w*e/(h^2 TWO_PI) (per-point h), unused
+    double2* hk = nullptr;   // per-point h: (h^2, log2(e)/(2 h^2)); NULL for fixed h
+    int32_t* perm = nullptr; // sorted position -> input index
+    uint64_t bytes = 0;
+};
+
+// ---- helpers ---------------------------------------------------------------
+int mgk_fail(mgk_ctx* ctx, int status, const std::string& msg);
+int mgk_cuda_fail(mgk_ctx* ctx, cudaError_t e, const char* what);
+int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes);
+void mgk_free(mgk_ctx* ctx, void* p, size_t bytes);
+
+#define MGK_CHECK_CUDA(ctx, expr)                                   \
+    do {                                                            \
+        cudaError_t e_ = (expr);                                    \
+        if (e_ != cudaSuccess) return mgk_cuda_fail(ctx, e_, #expr); \
+    } while (0)
+
+#define MGK_CHECK_LAUNCH(ctx, name)                                   \
+    do {                                                              \
+        cudaError_t e_ = cudaGetLastError();                          \
+        if (e_ != cudaSuccess) return mgk_cuda_fail(ctx, e_, name);   \
+    } while (0)
+
+// ---- device helpers --------------------------------------------------------
+__device__ __host__ __forceinline__ int64_t mgk_min64(int64_t a, int64_t b) { return a < b ? a : b; }
+__device__ __host__ __forceinline__ int64_t mgk_max64(int64_t a, int64_t b) { return a > b ? a : b; }
+
+__device__ __forceinline__ float mgk_ex2(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// 2^-a for a double exponent a >= 0, to about the accuracy of ex2.approx:
+// the exponent is split into float hi + lo and the lo part applied to first
+// order (2^-(hi+lo) = 2^-hi (1 - lo ln2 + ...), |lo| <= 2^-24 hi).
+__device__ __forceinline__ float mgk_exp2_neg(double a) {
+    const float ah = __double2float_rn(a);
+    const float al = __double2float_rn(a - (double)ah);
+    const float e = mgk_ex2(-ah);
+    return fmaf(-al * MGK_LN2F, e, e);
+}
+
+// Cell centres as the reference computes them (Utilities.h:13-14): double
+// arithmetic, stored to float.
+__device__ __host__ __forceinline__ float mgk_cell_x(double xll, double cs, int64_t col) {
+    return (float)(xll + ((double)col + 0.5) * cs);
+}
+__device__ __host__ __forceinline__ float mgk_cell_y(double yll, double cs, int64_t nrows, int64_t row) {
+    return (float)(yll + ((double)nrows - 0.5 - (double)row) * cs);
+}
+
+// Exact squared distance of two float positions with the rounding of the
+// FP64 oracle (products and sum each rounded once, never fused).
+__device__ __forceinline__ double mgk_d2_exact(float x0, float y0, float x1, float y1) {
+    const double dx = __dsub_rn((double)x1, (double)x0);
+    const double dy = __dsub_rn((double)y1, (double)y0);
+    return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+// h^2 exactly as the reference's CPU path forms it: float product widened.
+__device__ __host__ __forceinline__ double mgk_h2(float h) {
+    const float hh = h * h;
+    return (double)hh;
+}
+
+// ---- kernels launched across translation units ------------------------------
+int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float bin_size, mgk_index* idx);
+int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
+                       int64_t col0, int64_t nr, int64_t nc, const float* d_mask, float* d_out,
+                       unsigned long long* d_evals, bool fp64);
+int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
+int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r);
+int mgk_launch_edge_weights(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp,
+                            float h, const double* dist2, const mgk_raster* r, float* ew_out,
+                            unsigned long long* d_evals);
+int mgk_launch_loo(mgk_ctx* ctx, const mgk_index* idx, const float* ew_sorted_or_null, float h,
+                   double* d_logl, unsigned long long* d_evals);
