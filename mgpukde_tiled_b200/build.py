@@ -70,8 +70,10 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
     cli_src = os.path.join(CSRC, "cli.cpp")
     cli = os.path.join(LIB, "mgkde_tiled")
     if os.path.exists(cli_src) and (force or not _newer(cli, [cli_src, so, *headers])):
+        cuda = os.path.dirname(os.path.dirname(os.path.realpath(nvcc())))
         subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-I", os.path.join(REPO, "include"),
-                        "-I", CSRC, cli_src, "-o", cli, "-L", LIB, "-lmgk", "-Wl,-rpath,$ORIGIN"],
+                        "-I", CSRC, "-I", os.path.join(cuda, "include"), cli_src, "-o", cli, "-L", LIB, "-lmgk",
+                        "-L", os.path.join(cuda, "lib64"), "-lcudart", "-Wl,-rpath,$ORIGIN"],
                        check=True)
     return so
 

@@ -378,8 +378,7 @@ int mgk_index_destroy(mgk_index* idx) {
     if (c) {
         const size_t n1 = (size_t)std::max<int64_t>(idx->n, 1);
         mgk_free(c, idx->bin_start, sizeof(int32_t) * (size_t)(idx->nbx * idx->nby + 1));
-        mgk_free(c, idx->pts, sizeof(float4) * n1);
-        mgk_free(c, idx->hk, sizeof(double2) * n1);
+        mgk_free(c, idx->pts, sizeof(MgkPt) * n1);
         mgk_free(c, idx->perm, sizeof(int32_t) * n1);
     }
     delete idx;

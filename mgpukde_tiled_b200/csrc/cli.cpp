@@ -1,0 +1,363 @@
+// mgkde_tiled: host driver with the reference's command line (main(),
+// kde_cuda_kdtr_tiled.cu:262-1560), running the GPU path on one B200 through
+// the C ABI (libmgk.so).
+//
+//   mode 0: mgkde_tiled 0 #points cellsize_edge_correction cellsize_density h_option
+//           enable_edge_correction enable_sample_weight skip_omp_parallel skip_gpu_parallel
+//           num_cpu_threads num_gpu denfn_seq denfn_cuda serialized_mode [--key=value ...]
+//   mode 1: mgkde_tiled 1 points_file mask_file_edge_correction mask_file_density h_option ...
+//
+// The 14 positional arguments keep their meaning.  h_option: 0 rule of thumb,
+// 1 leave-one-out maximum likelihood (golden section), -1 per-point h from
+// the CSV.  h_option 2 (adaptive) is not part of this build and is rejected.
+// The OpenMP CPU path (skip_omp_parallel = 0) is not part of this build: only
+// the GPU path runs and writes denfn_cuda and pntsCUDA.csv.  num_gpu > 1 runs
+// on one GPU (this build is single-GPU; tiles need no exchange).
+// serialized_mode must be 0 (the reference's author advises 0).
+// Extras: --device=D  --tile=N (tile side, cells)  --bin=S (index bin side)
+//         --h=H (fixed bandwidth, overrides h_option 0)  --budget=BYTES
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "mgk.h"
+#include "tiff_io.hpp"
+
+namespace {
+
+using Clock = std::chrono::high_resolution_clock;
+double ms_since(Clock::time_point t) {
+    return std::chrono::duration<double, std::milli>(Clock::now() - t).count();
+}
+
+struct Args {
+    int mode = 0;
+    int npts = 100;
+    float cs_edge = 1.0f, cs_density = 0.5f;
+    std::string pnt_fn, mask_fn, mask_density_fn;
+    int hoption = 0;
+    bool edge = false, sample_weights = false;
+    int skip_omp = 0, skip_gpu = 0, threads = 1, ngpu = 1;
+    std::string den_omp_fn, den_cuda_fn;
+    int serialized = 0;
+    int device = 0;
+    int64_t tile = 0;
+    float bin = 0.0f;
+    float h_fixed = 0.0f;
+    uint64_t budget = 0;
+};
+
+void usage() {
+    std::printf(
+        "Run in mode 0:\n mgkde_tiled 0 #points cellsize_edge_correction cellsize_density h_option "
+        "enable_edge_corection enable_sample_weight skip_omp_parallel skip_gpu_parallel num_cpu_threads num_gpu "
+        "denfn_omp denfn_cuda serialized_mode\n"
+        "Run in mode 1:\n mgkde_tiled 1 points_file mask_file_edge_correction mask_file_density h_option "
+        "enable_edge_corection enable_sample_weight skip_omp_parallel skip_gpu_parallel num_cpu_threads num_gpu "
+        "denfn_omp denfn_cuda serialized_mode\n");
+}
+
+bool parse(int argc, char** argv, Args& a) {
+    std::vector<std::string> pos;
+    for (int i = 1; i < argc; i++) {
+        std::string s = argv[i];
+        if (s.rfind("--", 0) == 0) {
+            auto eq = s.find('=');
+            std::string k = s.substr(2, eq == std::string::npos ? std::string::npos : eq - 2);
+            std::string v = eq == std::string::npos ? "" : s.substr(eq + 1);
+            if (k == "device") a.device = std::atoi(v.c_str());
+            else if (k == "tile") a.tile = std::atoll(v.c_str());
+            else if (k == "bin") a.bin = (float)std::atof(v.c_str());
+            else if (k == "h") a.h_fixed = (float)std::atof(v.c_str());
+            else if (k == "budget") a.budget = std::strtoull(v.c_str(), nullptr, 10);
+            else { std::printf("***Unknown option %s\n", s.c_str()); return false; }
+        } else {
+            pos.push_back(s);
+        }
+    }
+    if (pos.size() != 14) return false;
+    a.mode = std::atoi(pos[0].c_str());
+    if (a.mode == 0) {
+        a.npts = std::atoi(pos[1].c_str());
+        a.cs_edge = (float)std::atof(pos[2].c_str());
+        a.cs_density = (float)std::atof(pos[3].c_str());
+    } else if (a.mode == 1) {
+        a.pnt_fn = pos[1];
+        a.mask_fn = pos[2];
+        a.mask_density_fn = pos[3];
+    } else {
+        return false;
+    }
+    a.hoption = std::atoi(pos[4].c_str());
+    a.edge = std::atoi(pos[5].c_str()) != 0;
+    a.sample_weights = std::atoi(pos[6].c_str()) != 0;
+    a.skip_omp = std::atoi(pos[7].c_str());
+    a.skip_gpu = std::atoi(pos[8].c_str());
+    a.threads = std::atoi(pos[9].c_str());
+    a.ngpu = std::atoi(pos[10].c_str());
+    a.den_omp_fn = pos[11];
+    a.den_cuda_fn = pos[12];
+    a.serialized = std::atoi(pos[13].c_str());
+    return true;
+}
+
+// ReadSamplePoints (kde_cuda_kdtr_tiled.cu:1623-1711): header skipped,
+// x,y[,h],w; weights used only with enable_sample_weight.
+bool read_points(const Args& a, std::vector<float>& x, std::vector<float>& y, std::vector<float>& w,
+                 std::vector<float>& h) {
+    FILE* f = std::fopen(a.pnt_fn.c_str(), "rt");
+    if (!f) {
+        std::printf("***Error opening file %s\n", a.pnt_fn.c_str());
+        return false;
+    }
+    char line[4096];
+    if (!std::fgets(line, sizeof(line), f)) {
+        std::fclose(f);
+        std::printf("***No point in file!\n");
+        return false;
+    }
+    while (std::fgets(line, sizeof(line), f)) {
+        std::vector<float> v;
+        for (char* t = std::strtok(line, ",\n\r"); t; t = std::strtok(nullptr, ",\n\r")) v.push_back((float)std::atof(t));
+        if (v.empty()) continue;
+        const size_t need = a.hoption == -1 ? 4 : 3;
+        if (v.size() < need - (a.hoption == -1 ? 0 : 1)) {
+            std::printf("***Error - malformed line in %s\n", a.pnt_fn.c_str());
+            std::fclose(f);
+            return false;
+        }
+        x.push_back(v[0]);
+        y.push_back(v[1]);
+        if (a.hoption == -1) {
+            if (v.size() < 4) {
+                std::printf("***Error - No bandwidth provided in the file\n");
+                std::fclose(f);
+                return false;
+            }
+            h.push_back(v[2]);
+            w.push_back(a.sample_weights ? v[3] : 1.0f);
+        } else {
+            w.push_back(a.sample_weights && v.size() > 2 ? v[2] : 1.0f);
+        }
+    }
+    std::fclose(f);
+    if (x.empty()) {
+        std::printf("***No point in file!\n");
+        return false;
+    }
+    return true;
+}
+
+int check(mgk_ctx* ctx, int st, const char* what) {
+    if (st != MGK_OK) std::printf("***%s failed: %s (%s)\n", what, mgk_status_string(st), mgk_ctx_last_error(ctx));
+    return st;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    const auto T1 = Clock::now();
+    Args a;
+    if (!parse(argc, argv, a)) {
+        std::printf("Incorrect arguments provided. Exiting...\n");
+        usage();
+        return 1;
+    }
+    if (a.mode == 0 && a.hoption == -1) {
+        std::printf("***Error - should never use bandwidth option -1 in mode 0 (i.e., randomly generately points). Exiting...");
+        return 1;
+    }
+    if (a.hoption == 2) {
+        std::printf("***Error - h_option 2 (adaptive bandwidth) is not part of this build. Exiting...\n");
+        return 1;
+    }
+    if (a.hoption < -1 || a.hoption > 2) {
+        std::printf("***Error - unknown h_option %d\n", a.hoption);
+        return 1;
+    }
+    if (a.serialized != 0) std::printf("===serialized_mode is ignored (always 0 in this build)\n");
+    if (a.skip_omp == 0) std::printf("===The OpenMP CPU path is not part of this build; running the GPU path only\n");
+    if (a.skip_gpu != 0) {
+        std::printf("===skip_gpu_parallel=1: nothing to run\n");
+        return 0;
+    }
+    if (a.ngpu > 1) std::printf("===This build runs on one GPU (device %d)\n", a.device);
+
+    // ---- inputs ---------------------------------------------------------
+    std::vector<float> x, y, w, hpp;
+    mgk_grid eg{}, dg{};
+    std::vector<float> emask, dmask;
+    double dens_gt[6];
+    bool dmask_all_valid = false;
+    auto t1 = Clock::now();
+    if (a.mode == 1) {
+        if (!read_points(a, x, y, w, hpp)) return 1;
+        mgk_tiff::Raster r, rd;
+        std::string err;
+        if (!mgk_tiff::read_tiff(a.mask_fn, r, err)) { std::printf("***%s\n", err.c_str()); return 1; }
+        if (!mgk_tiff::read_tiff(a.mask_density_fn, rd, err)) { std::printf("***%s\n", err.c_str()); return 1; }
+        // ReadGeoTIFFRaster (kde_cuda_kdtr_tiled.cu:2040-2080)
+        eg = {r.ncols, r.nrows, (float)r.gt[0], (float)(r.gt[3] + r.nrows * r.gt[5]), (float)r.gt[1],
+              (float)(r.has_nodata ? r.nodata : -1e10)};
+        emask.swap(r.data);
+        dg = {rd.ncols, rd.nrows, (float)rd.gt[0], (float)(rd.gt[3] + rd.nrows * rd.gt[5]), (float)rd.gt[1],
+              (float)(rd.has_nodata ? rd.nodata : -1e10)};
+        dmask.swap(rd.data);
+        std::memcpy(dens_gt, rd.gt, sizeof(dens_gt));
+    } else {
+        // AllocateSamplePoints (:1598-1620) with srand(100) (:407)
+        std::srand(100);
+        for (int i = 0; i < a.npts; i++) {
+            x.push_back(std::rand() * 100.0f / RAND_MAX);
+            y.push_back(std::rand() * 100.0f / RAND_MAX);
+            w.push_back(1.0f);
+        }
+        const int n_e = int(100 / a.cs_edge);
+        eg = {n_e, n_e, 0.0f, 0.0f, a.cs_edge, -9999.0f};
+        emask.assign((size_t)n_e * n_e, 0.0f);
+        const int n_d = int(std::ceil(100.0 / a.cs_density));
+        dg = {n_d, n_d, 0.0f, 100.0f - n_d * a.cs_density, a.cs_density, -9999.0f};
+        dmask_all_valid = true;
+        const double gt[6] = {0, a.cs_density, 0, 100.0, 0, -1.0 * a.cs_density};
+        std::memcpy(dens_gt, gt, sizeof(gt));
+    }
+    const int64_t n = (int64_t)x.size();
+    std::printf("...reading in data took %.0f ms\n", ms_since(t1));
+    std::printf("===Number of points: %lld\n", (long long)n);
+    std::printf("===Cell size (edge correction): %f\n", eg.cs);
+    std::printf("===Number of cells (edge correction): %lld\n", (long long)(eg.ncols * eg.nrows));
+    std::printf("===Cell size (density estimation): %f\n", dg.cs);
+    std::printf("===Number of cells (density estimation): %lld\n", (long long)(dg.ncols * dg.nrows));
+    std::printf("===Bandwidth option: %d\n===Enable edge correction: %d\n===Enable sample weight: %d\n", a.hoption,
+                (int)a.edge, (int)a.sample_weights);
+
+    float h = mgk_rule_of_thumb(n, x.data(), y.data(), w.data());
+    std::printf("===Rule of thumb bandwidth h0: %.5f\n", h);
+    if (a.h_fixed > 0.0f) h = a.h_fixed;
+
+    mgk_ctx* ctx = nullptr;
+    int st = mgk_ctx_create(a.device, a.budget, &ctx);
+    if (st != MGK_OK) {
+        std::printf("***No usable B200 device (%s)\n", mgk_status_string(st));
+        return 1;
+    }
+    const auto t_gpu = Clock::now();
+    mgk_points* pts = nullptr;
+    mgk_raster* em = nullptr;
+    mgk_index* idx = nullptr;
+    int rc = 1;
+    do {
+        if (check(ctx, mgk_points_upload(ctx, n, x.data(), y.data(), w.data(), hpp.empty() ? nullptr : hpp.data(), &pts),
+                  "points upload")) break;
+        const float hcall = a.hoption == -1 ? 0.0f : h;
+        if (a.edge) {
+            if (check(ctx, mgk_raster_upload(ctx, &eg, emask.data(), &em), "mask upload")) break;
+            t1 = Clock::now();
+            if (check(ctx, mgk_boundary_dist(ctx, pts, em), "boundary distance")) break;
+            mgk_ctx_synchronize(ctx);
+            std::printf("...MarkBoundary + CalcDist2Boundary took %.0f ms\n", ms_since(t1));
+        }
+        if (a.hoption == 1) {
+            float hopt = h;
+            int it = 0;
+            t1 = Clock::now();
+            if (check(ctx, mgk_mle_fixed_bandwidth(ctx, pts, em, h, &hopt, &it), "bandwidth search")) break;
+            std::printf("cross validated optimal fixed bandwidth hopt: %.5f (%d iterations, %.0f ms)\n", hopt, it,
+                        ms_since(t1));
+            h = hopt;
+        }
+        const float hfinal = a.hoption == -1 ? 0.0f : h;
+        (void)hcall;
+        t1 = Clock::now();
+        if (a.edge) {
+            if (check(ctx, mgk_edge_weights(ctx, pts, em, hfinal, nullptr), "edge weights")) break;
+        } else {
+            if (check(ctx, mgk_edge_weights_unit(ctx, pts), "unit weights")) break;
+        }
+        mgk_ctx_synchronize(ctx);
+        std::printf("...CalcEdgeCorrectionWeights took %.0f ms\n", ms_since(t1));
+        if (check(ctx, mgk_index_build(ctx, pts, hfinal, a.bin, &idx), "index build")) break;
+
+        // ---- tiled density (kde_cuda_kdtr_tiled.cu:1146-1517) ----------
+        size_t fr = 0, tot = 0;
+        cudaMemGetInfo(&fr, &tot);
+        int64_t T = a.tile;
+        if (T <= 0) {  // largest square tile whose mask + output fit in 20% of free memory
+            const double cells = 0.2 * (double)fr / 8.0;
+            T = (int64_t)std::sqrt(cells);
+            T = std::max<int64_t>(256, T / 256 * 256);
+        }
+        const int64_t tr = std::min<int64_t>(T, dg.nrows), tc = std::min<int64_t>(T, dg.ncols);
+        std::printf("...TILE_XSIZE=%lld, TILE_YSIZE=%lld\n", (long long)tc, (long long)tr);
+        mgk_tiff::TiledWriter wr;
+        if (!wr.open(a.den_cuda_fn, dg.ncols, dg.nrows, dens_gt, true, dg.nodata, 256)) {
+            std::printf("***Cannot create %s\n", a.den_cuda_fn.c_str());
+            break;
+        }
+        float *d_out = nullptr, *d_mask = nullptr;
+        std::vector<float> hbuf((size_t)tr * tc), hmask;
+        cudaMalloc(&d_out, sizeof(float) * tr * tc);
+        if (!dmask_all_valid) cudaMalloc(&d_mask, sizeof(float) * tr * tc);
+        t1 = Clock::now();
+        int64_t evals_total = 0;
+        bool ok = d_out && (dmask_all_valid || d_mask);
+        int tile_no = 0;
+        for (int64_t r0 = 0; ok && r0 < dg.nrows; r0 += tr) {
+            for (int64_t c0 = 0; ok && c0 < dg.ncols; c0 += tc) {
+                const int64_t nr = std::min<int64_t>(tr, dg.nrows - r0), nc = std::min<int64_t>(tc, dg.ncols - c0);
+                if (!dmask_all_valid) {
+                    hmask.resize((size_t)nr * nc);
+                    for (int64_t r = 0; r < nr; r++)
+                        std::memcpy(&hmask[r * nc], &dmask[(r0 + r) * dg.ncols + c0], sizeof(float) * nc);
+                    cudaMemcpy(d_mask, hmask.data(), sizeof(float) * nr * nc, cudaMemcpyHostToDevice);
+                }
+                int64_t ev = 0;
+                if (check(ctx, mgk_density_tile(ctx, idx, &dg, r0, c0, nr, nc, d_mask, d_out, &ev), "density")) {
+                    ok = false;
+                    break;
+                }
+                evals_total += ev;
+                cudaMemcpy(hbuf.data(), d_out, sizeof(float) * nr * nc, cudaMemcpyDeviceToHost);
+                if (!wr.write_region(c0, r0, nc, nr, hbuf.data())) {
+                    std::printf("***Unable to write tile in GeoTIFF!\n");
+                    ok = false;
+                    break;
+                }
+                wr.flush();
+                std::printf("...working on tile %d: rows %lld+%lld cols %lld+%lld, %lld kernel evaluations\n",
+                            ++tile_no, (long long)r0, (long long)nr, (long long)c0, (long long)nc, (long long)ev);
+            }
+        }
+        cudaFree(d_out);
+        if (d_mask) cudaFree(d_mask);
+        wr.close();
+        if (!ok) break;
+        std::printf("KernelDensityEstimation took %.0f ms (%lld kernel evaluations)\n", ms_since(t1),
+                    (long long)evals_total);
+
+        // WriteSamplePoints (kde_cuda_kdtr_tiled.cu:1857-1870): x, y, h, edge weight (input order)
+        std::vector<float> ew(n);
+        if (check(ctx, mgk_points_download(pts, nullptr, ew.data()), "download")) break;
+        FILE* f = std::fopen("pntsCUDA.csv", "w");
+        if (f) {
+            std::fprintf(f, "x, y, h, w\n");
+            for (int64_t i = 0; i < n; i++)
+                std::fprintf(f, "%f, %f, %f, %f\n", x[i], y[i], hpp.empty() ? h : hpp[i], ew[i]);
+            std::fclose(f);
+        }
+        std::printf("\n>>>>>>Computation on GPU took %.0f ms in total\n\n", ms_since(t_gpu));
+        rc = 0;
+    } while (0);
+    mgk_index_destroy(idx);
+    mgk_raster_destroy(em);
+    mgk_points_destroy(pts);
+    mgk_ctx_destroy(ctx);
+    std::printf("Done...\n\n+++In total it took %.0f ms\n", ms_since(T1));
+    return rc;
+}

@@ -8,27 +8,31 @@
 //   den(c) = sum_p [d^2 < 9 h_p^2] exp(-d^2 / 2 h_p^2) / (h_p^2 TWO_PI) w_p e_p
 //
 // Layout: a CTA (256 threads) owns a 64 x 64 block of cells; warp w owns a
-// 16 x 32 sub-block, lane l a 4 x 4 micro-tile.  The CTA stages the points of
-// the bins within 3h of its block into shared memory, one contiguous range per
-// bin row.  For each staged point a warp first tests its sub-block's
-// rectangle against the 3h disc (exact, FP64) and skips the point if it
-// cannot contribute.  Otherwise the Gaussian factorises over the grid:
-//   exp2(-(a_j + b_i)) = E_j * F_i,  a_j = dx_j^2 k2, b_i = dy_i^2 k2,
-//   k2 = log2(e) / (2 h^2)
-// Each lane computes one column factor E (32 columns) and one row factor F
-// (16 rows) with an FP64 exponent split into float hi+lo, the warp exchanges
-// them through shared memory, and each lane forms its 16 products with one
-// FMUL each.  The cutoff d^2 < 9h^2 is decided in FP32 as a_j < cut - b_i;
-// pairs within a narrow band of the cutoff (|a_j + b_i - cut| < 4e-6, log2
-// units) are re-decided with the exact FP64 test the oracle uses, so the set
-// of summed pairs equals the reference's.
+// 16 x 32 sub-block, lane l a 4 x 4 micro-tile.  Candidates (points of the
+// bins within 3h of the block, one contiguous range per bin row) arrive in
+// mini-batches of 32 through a double-buffered TMA bulk copy
+// (cp.async.bulk + mbarrier) into shared memory.  Per mini-batch:
 //
-// Accumulation: per cell, FP32 partial sums over 8 points are added into a
-// Kahan-compensated FP32 accumulator; the result is formed in FP64
-// (sum - compensation) times the kernel normalisation.  Blocks with many
-// candidates are split across CTAs (work items); their partial sums are
-// written in FP64 to scratch and merged in a fixed order, so results are
-// bitwise reproducible.
+//  phase A (all 256 threads, 8 per point): the Gaussian factorises over the
+//    grid, exp2(-(a_j + b_i)) = E_j F_i with a_j = dx_j^2 k2, b_i = dy_i^2 k2,
+//    k2 = log2(e) / (2 h^2).  The 64 column factors and 64 row factors of the
+//    block are computed once per point.  Coordinates are hi/lo float pairs on
+//    a common quantum, so dx = (xh - cxh) + (xl - cxl) is exact as a pair and
+//    a = dx^2 k2 is formed with error-free float products (no FP64, no
+//    conversions); E = ex2(-a_hi) (1 - a_lo ln2).  Row entries also carry the
+//    cutoff threshold T_i = cut - b_i, a flag marking rows where some column
+//    lies within a 4e-6 (log2 units) band of the cutoff, and each warp's
+//    sub-block gets an exact-enough rectangle-vs-disc test.
+//  phase B (each warp, its processed points): per cell one compare
+//    a_j < T_i and a predicated FFMA part += E_j F_i.  Rows flagged as
+//    ambiguous are re-decided with the exact FP64 test of the oracle, so the
+//    summed pair set is exactly the reference's.
+//
+// Accumulation: FP32 partial sums over 8 points per cell, added into a
+// Kahan-compensated FP32 accumulator; the epilogue forms (s - c) times the
+// kernel normalisation in FP64.  Heavy blocks are split into work items whose
+// FP64 partials are merged in a fixed order, so results are bitwise
+// reproducible.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -38,9 +42,11 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kBlk = 64;       // cells per CTA block side
-constexpr int kChunk = 512;    // points staged per batch
+constexpr int kBlk = 64;        // cells per CTA block side
+constexpr int kMB = 32;         // points per mini-batch
+constexpr int kStage64 = 512;   // points staged per batch by the FP64 form
 constexpr float kAmbEps = 4e-6f;
+constexpr long long kSpinLimit = 1ll << 24;
 
 struct Item {
     int32_t bx, by;       // block coordinates within the tile
@@ -59,14 +65,16 @@ struct DParams {
     double* scratch;  // [slot][kBlk*kBlk]
     const Item* items;
     // index
-    const float4* pts;
-    const double2* hk;
+    const MgkPt* pts;
     const int32_t* bin_start;
     double ox, oy, inv_side;
     int64_t nbx, nby;
+    int qexp;
     // fixed-h constants
-    double h2, k2, k0, cut_d2, cutl, reach;
+    double h2, k0, cut_d2, reach;
+    float k2h, k2l, cutlh, cutll, cutf;
     unsigned long long* evals;
+    unsigned long long* err;
 };
 
 // Bin range covering [lo, hi] (coordinates), clamped; returns false if empty.
@@ -119,29 +127,139 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t;
 }
 
+// ---- TMA bulk copy + mbarrier (sm_90+ PTX) ---------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait on an mbarrier phase; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+    for (long long i = 0; i < kSpinLimit; i++)
+        if (mbar_try_wait(b, parity)) return true;
+    return false;
+}
+
+// Exponent a = (t + lo)^2 (k2h + k2l) as a float pair ah + al.  t is exact
+// (difference of two multiples of the quantum), |lo| <= quantum; the pair
+// (dh, de) is dx exactly and the products are error-free, so ah + al is a
+// to about 2^-44 relative.
+__device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, float k2l, float& ah, float& al) {
+    const float dh = __fadd_rn(t, lo);
+    const float de = __fsub_rn(lo, __fsub_rn(dh, t));
+    const float p = __fmul_rn(dh, dh);
+    float pe = __fmaf_rn(dh, dh, -p);
+    pe = __fmaf_rn(__fmul_rn(2.0f, dh), de, pe);
+    ah = __fmul_rn(p, k2h);
+    const float ae = __fmaf_rn(p, k2h, -ah);
+    al = __fmaf_rn(pe, k2h, __fmaf_rn(p, k2l, ae));
+}
+
+__device__ __forceinline__ float exp2_pair(float ah, float al) {
+    const float e = mgk_ex2(-ah);
+    return __fmaf_rn(__fmul_rn(-al, MGK_LN2F), e, e);
+}
+
+// Does some column of a regular 64-column block lie within the ambiguity
+// band of row threshold T?  The row's exponent a(x) = k2 (x - px)^2 crosses T
+// at x = px +- s, s = sqrt(T / k2); a column within w = eps / (k2 s) (plus a
+// margin for the float error of the crossing position) of a crossing may be
+// classified differently in FP32 than in FP64.  prel0 = px - cx_0.
+__device__ __forceinline__ bool amb_row(float T, float k2h, float prel0, float cs, float inv_cs) {
+    if (T < -2.0f * kAmbEps) return false;
+    const float s2 = fmaxf(T, 0.0f) / k2h;
+    const float s = sqrtf(s2);
+    const float w = (2.0f * kAmbEps) / (k2h * 2.0f * s + 1e-30f) + 4e-7f * (s + fabsf(prel0)) + 1e-6f * cs;
+    if (w * inv_cs > 0.25f) return true;
+    const float fp = (prel0 + s) * inv_cs, fm = (prel0 - s) * inv_cs;
+    const float np = rintf(fp), nm = rintf(fm);
+    const bool hp = np >= -1.0f && np <= (float)kBlk && fabsf(fp - np) * cs < w;
+    const bool hm = nm >= -1.0f && nm <= (float)kBlk && fabsf(fm - nm) * cs < w;
+    return hp || hm;
+}
+
+struct BatchIt {
+    int64_t by, seq, pos;
+};
+
+// Next mini-batch of the block's candidate sequence (never spans two bin
+// rows): returns its size (0 at the end) and its first global index.
+__device__ __forceinline__ int next_batch(const DParams& P, const BlockGeom& G, const Item& it, BatchIt& s,
+                                          int64_t& src) {
+    if (!G.any) return 0;
+    while (s.by <= G.by1 && s.pos < it.k1) {
+        const int64_t sb = P.bin_start[s.by * P.nbx + G.bx0];
+        const int64_t len = (int64_t)P.bin_start[s.by * P.nbx + G.bx1 + 1] - sb;
+        const int64_t lo = mgk_max64(s.pos, s.seq), hi = mgk_min64(s.seq + len, (int64_t)it.k1);
+        if (lo < hi) {
+            const int m = (int)mgk_min64(kMB, hi - lo);
+            src = sb + (lo - s.seq);
+            s.pos = lo + m;
+            return m;
+        }
+        s.seq += len;
+        s.by++;
+    }
+    return 0;
+}
+
 template <bool VARH, bool COUNT>
 __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
-    __shared__ float4 sp[kChunk];
-    __shared__ double2 shk[VARH ? kChunk : 1];
-    __shared__ double scx[kBlk], scy[kBlk];
-    __shared__ float2 colbuf[kThreads / 32][2][32];
-    __shared__ float2 rowbuf[kThreads / 32][2][16];
+    __shared__ __align__(16) MgkPt stage[2][kMB];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ __align__(16) float2 colf[kMB][kBlk];  // (a_hi, E) per point and column
+    __shared__ __align__(16) float2 rowf[kMB][kBlk];  // (T, F) per point and row
+    __shared__ unsigned long long rowflag[kMB];
+    __shared__ unsigned char procmask[kMB];
+    __shared__ float s_cxh[kBlk], s_cxl[kBlk], s_cyh[kBlk], s_cyl[kBlk], s_cxg[kBlk], s_cyg[kBlk];
+    __shared__ int s_abort;
 
     const Item it = P.items[blockIdx.x];
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wr = warp >> 1, wc = warp & 1;      // warp sub-block: rows wr*16.., cols wc*32..
-    const int tr = lane >> 3, tc = lane & 7;      // lane micro-tile: rows tr*4.., cols tc*4..
-    if (tid < kBlk) scx[tid] = (double)mgk_cell_x(P.xll, P.cs, G.c0 + tid);
-    else if (tid < 2 * kBlk) scy[tid - kBlk] = (double)mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + tid - kBlk);
-    __syncthreads();
+    const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*32..
+    const int tr = lane >> 3, tc = lane & 7;  // lane micro-tile: rows tr*4.., cols tc*4..
 
-    const bool warp_on = (wr * 16 < G.nrow) && (wc * 32 < G.ncol);
-    // warp rectangle (cell centres), clamped to cells inside the tile
-    const double wx0 = scx[wc * 32], wx1 = scx[min(wc * 32 + 31, G.ncol - 1)];
-    const double wy1 = scy[wr * 16], wy0 = scy[min(wr * 16 + 15, G.nrow - 1)];
-    const double my_cx = scx[wc * 32 + lane];
-    const double my_cy = scy[wr * 16 + (lane & 15)];
+    // cell centres of the block: global floats and their quantum split
+    bool regular = true;
+    if (tid < kBlk) {
+        const float cx = mgk_cell_x(P.xll, P.cs, G.c0 + tid);
+        s_cxg[tid] = cx;
+        mgk_qsplit(cx, P.qexp, s_cxh[tid], s_cxl[tid]);
+        const float cx0 = mgk_cell_x(P.xll, P.cs, G.c0);
+        regular = ((double)cx - (double)cx0) == (double)tid * P.cs;
+    } else if (tid < 2 * kBlk) {
+        const float cy = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + tid - kBlk);
+        s_cyg[tid - kBlk] = cy;
+        mgk_qsplit(cy, P.qexp, s_cyh[tid - kBlk], s_cyl[tid - kBlk]);
+    }
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+        s_abort = 0;
+    }
+    regular = __syncthreads_and(regular);
+    const float cs_f = (float)P.cs, inv_cs = 1.0f / (float)P.cs;
 
     // validity of the lane's 16 cells (inside the tile and not NoData)
     unsigned valid = 0;
@@ -161,117 +279,174 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
     unsigned long long cnt = 0;
     unsigned pc = 0;  // points processed by this warp (warp-uniform)
 
-    if (G.any) {
-        int64_t seq = 0;  // position in the block's candidate sequence
-        for (int64_t by = G.by0; by <= G.by1 && seq < it.k1; by++) {
-            const int64_t sb = P.bin_start[by * P.nbx + G.bx0];
-            const int64_t se = P.bin_start[by * P.nbx + G.bx1 + 1];
-            const int64_t len = se - sb;
-            // intersect [seq, seq+len) with [k0, k1)
-            const int64_t lo = mgk_max64(seq, it.k0), hi = mgk_min64(seq + len, it.k1);
-            for (int64_t base = lo; base < hi; base += kChunk) {
-                const int m = (int)mgk_min64(kChunk, hi - base);
-                const int64_t src = sb + (base - seq);
-                __syncthreads();
-                for (int k = tid; k < m; k += kThreads) {
-                    sp[k] = P.pts[src + k];
-                    if (VARH) shk[k] = P.hk[src + k];
+    // phase A roles: point q = tid / 8, part k = tid % 8 (columns/rows k*8.., skip test of warp k)
+    const int qa = tid >> 3, ka = tid & 7;
+    // warp k's sub-block rectangle (cells inside the tile), for the skip test
+    const int sk_wr = ka >> 1, sk_wc = ka & 1;
+    const bool sk_on = (sk_wr * 16 < G.nrow) && (sk_wc * 32 < G.ncol);
+    const int sk_c0 = sk_wc * 32, sk_c1 = min(sk_wc * 32 + 31, G.ncol - 1);
+    const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
+
+    BatchIt bit{G.by0, 0, (int64_t)it.k0};
+    int64_t src = 0;
+    int m = next_batch(P, G, it, bit, src);
+    if (m > 0 && tid == 0) {
+        mbar_arrive_tx(&mbar[0], (unsigned)(m * sizeof(MgkPt)));
+        bulk_g2s(&stage[0][0], P.pts + src, (unsigned)(m * sizeof(MgkPt)), &mbar[0]);
+    }
+    unsigned phase0 = 0, phase1 = 0;
+    int buf = 0;
+    // outstanding copies at an abort: (buffer, parity) pairs to drain
+    int drain_n = 0, drain_b[2] = {0, 0};
+    unsigned drain_p[2] = {0, 0};
+    while (m > 0) {
+        int64_t nsrc = 0;
+        const int nm = next_batch(P, G, it, bit, nsrc);
+        if (nm > 0 && tid == 0) {
+            mbar_arrive_tx(&mbar[buf ^ 1], (unsigned)(nm * sizeof(MgkPt)));
+            bulk_g2s(&stage[buf ^ 1][0], P.pts + nsrc, (unsigned)(nm * sizeof(MgkPt)), &mbar[buf ^ 1]);
+        }
+        const unsigned par = buf ? phase1 : phase0;
+        if (!mbar_wait(&mbar[buf], par)) {
+            atomicExch(P.err, 1ull);
+            s_abort = 1;
+        }
+        if (__syncthreads_or(s_abort)) {
+            drain_b[drain_n] = buf;
+            drain_p[drain_n++] = par;
+            if (nm > 0) {
+                drain_b[drain_n] = buf ^ 1;
+                drain_p[drain_n++] = buf ? phase0 : phase1;
+            }
+            break;
+        }
+        if (buf) phase1 ^= 1u;
+        else phase0 ^= 1u;
+
+        // ---------------- phase A ----------------
+        {
+            bool proc = false;
+            unsigned fl = 0;
+            if (qa < m) {
+                const MgkPt r = stage[buf][qa];
+                float k2h, k2l, cutf;
+                if (VARH) {
+                    k2h = r.k2h;
+                    k2l = r.k2l;
+                    cutf = 9.0f * r.hh;
+                } else {
+                    k2h = P.k2h;
+                    k2l = P.k2l;
+                    cutf = P.cutf;
                 }
-                __syncthreads();
-                if (!warp_on) continue;
-                for (int q = 0; q < m; q++) {
-                    const float4 p = sp[q];
-                    double h2, k2, cut_d2;
-                    if (VARH) {
-                        const double2 hk = shk[q];
-                        h2 = hk.x;
-                        k2 = hk.y;
-                        cut_d2 = MGK_CUT * h2;
-                    } else {
-                        h2 = P.h2;
-                        k2 = P.k2;
-                        cut_d2 = P.cut_d2;
-                    }
-                    (void)h2;
-                    // exact rectangle test: skip if no cell centre of the sub-block is within 3h
-                    {
-                        const double px = p.x, py = p.y;
-                        const double ddx = fmax(0.0, fmax(__dsub_rn(wx0, px), __dsub_rn(px, wx1)));
-                        const double ddy = fmax(0.0, fmax(__dsub_rn(wy0, py), __dsub_rn(py, wy1)));
-                        if (__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)) >= cut_d2) continue;
-                    }
-                    const int b = pc & 1;
-                    {
-                        const double dx = (double)p.x - my_cx;
-                        const double a = dx * dx * k2;
-                        colbuf[warp][b][lane] = make_float2(__double2float_rn(a), mgk_exp2_neg(a));
-                    }
-                    if (lane < 16) {
-                        const double dy = (double)p.y - my_cy;
-                        const double bb = dy * dy * k2;
-                        const double cutl = VARH ? MGK_CUT * 0.5 * MGK_LOG2E : P.cutl;
-                        rowbuf[warp][b][lane] = make_float2(__double2float_rn(cutl - bb), p.z * mgk_exp2_neg(bb));
-                    }
-                    __syncwarp();
-                    float ca[4], ce[4], rt[4], re[4];
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const float2 v = colbuf[warp][b][tc * 4 + j];
-                        ca[j] = v.x;
-                        ce[j] = v.y;
-                    }
+                for (int c = 0; c < 8; c++) {
+                    const int j = ka * 8 + c;
+                    float ah, al;
+                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al);
+                    colf[qa][j] = make_float2(ah, exp2_pair(ah, al));
+                }
+                const float prel0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0]));
+#pragma unroll
+                for (int c = 0; c < 8; c++) {
+                    const int i = ka * 8 + c;
+                    float bh, bl;
+                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl);
+                    const float T = __fadd_rn(__fsub_rn(P.cutlh, bh), __fsub_rn(P.cutll, bl));
+                    rowf[qa][i] = make_float2(T, __fmul_rn(r.wk, exp2_pair(bh, bl)));
+                    const bool a = regular ? amb_row(T, k2h, prel0, cs_f, inv_cs) : (T > -2.0f * kAmbEps);
+                    fl |= (unsigned)a << c;
+                }
+                if (sk_on) {
+                    // distance from the point to the sub-block rectangle of cell centres
+                    const float dxl = __fadd_rn(__fsub_rn(s_cxh[sk_c0], r.xh), __fsub_rn(s_cxl[sk_c0], r.xl));
+                    const float dxr = __fadd_rn(__fsub_rn(r.xh, s_cxh[sk_c1]), __fsub_rn(r.xl, s_cxl[sk_c1]));
+                    const float dyt = __fadd_rn(__fsub_rn(r.yh, s_cyh[sk_r0]), __fsub_rn(r.yl, s_cyl[sk_r0]));
+                    const float dyb = __fadd_rn(__fsub_rn(s_cyh[sk_r1], r.yh), __fsub_rn(s_cyl[sk_r1], r.yl));
+                    const float ddx = fmaxf(0.0f, fmaxf(dxl, dxr));
+                    const float ddy = fmaxf(0.0f, fmaxf(dyt, dyb));
+                    proc = ddx * ddx + ddy * ddy < cutf * 1.0001f;
+                }
+            }
+            // 64 row flags of point qa: 8 bits from each of its 8 threads (same warp)
+            unsigned lo32 = ka < 4 ? fl << (8 * ka) : 0u;
+            unsigned hi32 = ka >= 4 ? fl << (8 * (ka - 4)) : 0u;
+#pragma unroll
+            for (int o = 1; o < 8; o <<= 1) {
+                lo32 |= __shfl_xor_sync(0xffffffffu, lo32, o);
+                hi32 |= __shfl_xor_sync(0xffffffffu, hi32, o);
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, proc);
+            if (ka == 0) {
+                rowflag[qa] = ((unsigned long long)hi32 << 32) | lo32;
+                procmask[qa] = (unsigned char)((bal >> (8 * (qa & 3))) & 0xffu);
+            }
+        }
+        __syncthreads();
+
+        // ---------------- phase B ----------------
+        for (int q = 0; q < m; q++) {
+            if (!((procmask[q] >> warp) & 1u)) continue;
+            const float4 c01 = *reinterpret_cast<const float4*>(&colf[q][wc * 32 + tc * 4]);
+            const float4 c23 = *reinterpret_cast<const float4*>(&colf[q][wc * 32 + tc * 4 + 2]);
+            const float4 r01 = *reinterpret_cast<const float4*>(&rowf[q][wr * 16 + tr * 4]);
+            const float4 r23 = *reinterpret_cast<const float4*>(&rowf[q][wr * 16 + tr * 4 + 2]);
+            const float ca[4] = {c01.x, c01.z, c23.x, c23.z}, ce[4] = {c01.y, c01.w, c23.y, c23.w};
+            const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rf[4] = {r01.y, r01.w, r23.y, r23.w};
+            unsigned inm = 0;
+#pragma unroll
+            for (int i = 0; i < 4; i++)
+#pragma unroll
+                for (int j = 0; j < 4; j++) {
+                    const bool in = ca[j] < rt[i];
+                    if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rf[i], part[i * 4 + j]);
+                    if (COUNT) inm |= (unsigned)in << (i * 4 + j);
+                }
+            const unsigned fl = (unsigned)(rowflag[q] >> (wr * 16 + tr * 4)) & 0xfu;
+            if (__any_sync(0xffffffffu, fl != 0u)) {
+                if (fl) {
+                    const MgkPt r = stage[buf][q];
+                    const float px = r.xh + r.xl, py = r.yh + r.yl;
+                    const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
 #pragma unroll
                     for (int i = 0; i < 4; i++) {
-                        const float2 v = rowbuf[warp][b][tr * 4 + i];
-                        rt[i] = v.x;
-                        re[i] = v.y;
-                    }
-                    bool amb = false;
-                    unsigned inm = 0;
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
+                        if (!((fl >> i) & 1u)) continue;
 #pragma unroll
                         for (int j = 0; j < 4; j++) {
-                            const float u = ca[j] - rt[i];
-                            const bool in = u < 0.0f;
-                            amb |= fabsf(u) < kAmbEps;
-                            if (in) part[i * 4 + j] += ce[j] * re[i];
-                            if (COUNT) inm |= (unsigned)in << (i * 4 + j);
-                        }
-                    if (__any_sync(0xffffffffu, amb)) {
-                        if (amb) {
-#pragma unroll
-                            for (int i = 0; i < 4; i++)
-#pragma unroll
-                                for (int j = 0; j < 4; j++) {
-                                    const float u = ca[j] - rt[i];
-                                    if (fabsf(u) < kAmbEps) {
-                                        const float cxf = (float)scx[wc * 32 + tc * 4 + j];
-                                        const float cyf = (float)scy[wr * 16 + tr * 4 + i];
-                                        const bool ex = mgk_d2_exact(p.x, p.y, cxf, cyf) < cut_d2;
-                                        const bool fl = u < 0.0f;
-                                        if (ex != fl) {
-                                            const float t = ce[j] * re[i];
-                                            part[i * 4 + j] += ex ? t : -t;
-                                            if (COUNT) inm ^= 1u << (i * 4 + j);
-                                        }
-                                    }
-                                }
-                        }
-                    }
-                    if (COUNT) cnt += __popc(inm & valid);
-                    pc++;
-                    if ((pc & 7u) == 0) {
-#pragma unroll
-                        for (int k = 0; k < 16; k++) {
-                            kahan_add(acc_s[k], acc_c[k], part[k]);
-                            part[k] = 0.0f;
+                            const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 32 + tc * 4 + j],
+                                                         s_cyg[wr * 16 + tr * 4 + i]) < cut;
+                            const bool fi = ca[j] < rt[i];
+                            if (ex != fi) {
+                                const float t = __fmul_rn(ce[j], rf[i]);
+                                part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
+                                if (COUNT) inm ^= 1u << (i * 4 + j);
+                            }
                         }
                     }
                 }
             }
-            seq += len;
+            if (COUNT) cnt += __popc(inm & valid);
+            pc++;
+            if ((pc & 7u) == 0) {
+#pragma unroll
+                for (int k = 0; k < 16; k++) {
+                    kahan_add(acc_s[k], acc_c[k], part[k]);
+                    part[k] = 0.0f;
+                }
+            }
         }
+        __syncthreads();  // colf/rowf and stage[buf] are reused next
+        m = nm;
+        src = nsrc;
+        buf ^= 1;
+    }
+    if (drain_n) {
+        // a staging wait ran out: give the outstanding copies a second bounded
+        // wait before the CTA (and its shared memory) goes away
+        if (tid == 0)
+            for (int d = 0; d < drain_n; d++) mbar_wait(&mbar[drain_b[d]], drain_p[d]);
+        __syncthreads();
+        return;
     }
 #pragma unroll
     for (int k = 0; k < 16; k++) kahan_add(acc_s[k], acc_c[k], part[k]);
@@ -299,12 +474,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
     }
 }
 
-// Plain FP64 form: same blocks, staging and candidate lists; per pair an
+// Plain FP64 form: same blocks, work items and candidate lists; per pair an
 // exact FP64 distance, the cutoff, a double exp and a double accumulate.
 template <bool VARH>
 __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
-    __shared__ float4 sp[kChunk];
-    __shared__ double2 shk[VARH ? kChunk : 1];
+    __shared__ MgkPt sp[kStage64];
     const Item it = P.items[blockIdx.x];
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -317,7 +491,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
     double acc[16];
 #pragma unroll
     for (int k = 0; k < 16; k++) acc[k] = 0.0;
-    unsigned long long cnt = 0;
     if (G.any) {
         int64_t seq = 0;
         for (int64_t by = G.by0; by <= G.by1 && seq < it.k1; by++) {
@@ -325,29 +498,24 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
             const int64_t se = P.bin_start[by * P.nbx + G.bx1 + 1];
             const int64_t len = se - sb;
             const int64_t lo = mgk_max64(seq, it.k0), hi = mgk_min64(seq + len, it.k1);
-            for (int64_t base = lo; base < hi; base += kChunk) {
-                const int m = (int)mgk_min64(kChunk, hi - base);
+            for (int64_t base = lo; base < hi; base += kStage64) {
+                const int m = (int)mgk_min64(kStage64, hi - base);
                 const int64_t src = sb + (base - seq);
                 __syncthreads();
-                for (int k = tid; k < m; k += kThreads) {
-                    sp[k] = P.pts[src + k];
-                    if (VARH) shk[k] = P.hk[src + k];
-                }
+                for (int k = tid; k < m; k += kThreads) sp[k] = P.pts[src + k];
                 __syncthreads();
                 for (int q = 0; q < m; q++) {
-                    const float4 p = sp[q];
-                    const double h2 = VARH ? shk[q].x : P.h2;
+                    const MgkPt p = sp[q];
+                    const float px = p.xh + p.xl, py = p.yh + p.yl;
+                    const double h2 = VARH ? (double)p.hh : P.h2;
                     const double cut = MGK_CUT * h2;
                     const double m2h = -1.0 / (2.0 * h2);
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
                         for (int j = 0; j < 4; j++) {
-                            const double d2 = mgk_d2_exact(p.x, p.y, cx[j], cy[i]);
-                            if (d2 < cut) {
-                                acc[i * 4 + j] += exp(d2 * m2h) * (double)p.z;
-                                cnt++;
-                            }
+                            const double d2 = mgk_d2_exact(px, py, cx[j], cy[i]);
+                            if (d2 < cut) acc[i * 4 + j] += exp(d2 * m2h) * (double)p.wk;
                         }
                 }
             }
@@ -355,7 +523,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
         }
     }
     const double norm = VARH ? 1.0 : P.k0;
-    unsigned long long vcnt = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -371,8 +538,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
                 P.out[o] = valid ? (float)v : P.nodata;
             }
         }
-    (void)vcnt;
-    (void)cnt;
 }
 
 // Merge of split blocks: cell value = sum over the block's slots in order.
@@ -416,20 +581,29 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     P.mask = d_mask;
     P.out = d_out;
     P.pts = idx->pts;
-    P.hk = idx->hk;
     P.bin_start = idx->bin_start;
     P.ox = idx->ox;
     P.oy = idx->oy;
     P.inv_side = 1.0 / idx->side;
     P.nbx = idx->nbx;
     P.nby = idx->nby;
+    P.qexp = idx->qexp;
     P.h2 = idx->h2;
-    P.k2 = idx->k2;
     P.k0 = idx->k0;
     P.cut_d2 = idx->cut_d2;
-    P.cutl = idx->cut_d2 * idx->k2;
     P.reach = idx->reach;
+    {
+        const double k2 = idx->k2;
+        P.k2h = (float)k2;
+        P.k2l = (float)(k2 - (double)P.k2h);
+        // log2-unit cutoff: 9 h^2 k2 for fixed h; 4.5 log2(e) for per-point h
+        const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
+        P.cutlh = (float)cutl;
+        P.cutll = (float)(cutl - (double)P.cutlh);
+        P.cutf = (float)idx->cut_d2;
+    }
     P.evals = d_evals;
+    P.err = ctx->d_counter + 7;
 
     const int nbx_t = (int)((nc + kBlk - 1) / kBlk), nby_t = (int)((nr + kBlk - 1) / kBlk);
     const int nblk = nbx_t * nby_t;
@@ -439,20 +613,19 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     if ((st = mgk_alloc(ctx, (void**)&d_counts, sizeof(int64_t) * nblk))) return st;
     k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, d_counts);
     std::vector<int64_t> counts(nblk);
-    cudaError_t ce = cudaMemcpyAsync(counts.data(), d_counts, sizeof(int64_t) * nblk, cudaMemcpyDeviceToHost, s);
+    cudaError_t ce = cudaMemsetAsync(P.err, 0, sizeof(unsigned long long), s);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(counts.data(), d_counts, sizeof(int64_t) * nblk, cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
     mgk_free(ctx, d_counts, sizeof(int64_t) * nblk);
     if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
 
-    int64_t total = 0, maxc = 0;
-    for (int64_t c : counts) {
-        total += c;
-        maxc = std::max(maxc, c);
-    }
+    int64_t total = 0;
+    for (int64_t c : counts) total += c;
     // Items of at most K candidates: about 8 waves of the resident CTAs.
     const int64_t slots_resident = (int64_t)ctx->sm_count * 2;
     int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
-    K = (K + kChunk - 1) / kChunk * kChunk;
+    K = (K + kMB - 1) / kMB * kMB;
     std::vector<Item> items;
     std::vector<int32_t> split_blocks, split_begin;
     int32_t nslots = 0;
@@ -491,6 +664,7 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         mgk_free(ctx, d_items, b_items); mgk_free(ctx, P.scratch, b_scr); mgk_free(ctx, d_sb, b_sb); return st;
     }
     int rc = MGK_OK;
+    unsigned long long err = 0;
     do {
         if ((ce = cudaMemcpyAsync(d_items, items.data(), b_items, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
         if (nslots) {
@@ -520,10 +694,12 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
             MGK_COUNT_LAUNCH(ctx, 1);
         }
         // the work list and scratch are freed below: wait for the kernels
+        if ((ce = cudaMemcpyAsync(&err, P.err, sizeof(err), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
         ce = cudaStreamSynchronize(s);
         if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
     } while (0);
     if (ce != cudaSuccess) rc = mgk_cuda_fail(ctx, ce, "density");
+    else if (err) rc = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
     mgk_free(ctx, d_items, b_items);
     if (nslots) {
         mgk_free(ctx, P.scratch, b_scr);

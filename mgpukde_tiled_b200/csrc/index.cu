@@ -177,19 +177,27 @@ __global__ void k_bin_starts(int64_t n, const unsigned* __restrict__ keys, int64
 
 __global__ void k_gather(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ x,
                          const float* __restrict__ y, const float* __restrict__ w,
-                         const float* __restrict__ ew, const float* __restrict__ hpp, float4* __restrict__ out,
-                         double2* __restrict__ hk) {
+                         const float* __restrict__ ew, const float* __restrict__ hpp, int qexp,
+                         MgkPt* __restrict__ out) {
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int32_t j = perm[i];
-    float wk = (w ? w[j] : 1.0f) * (ew ? ew[j] : 1.0f);
+    MgkPt r;
+    mgk_qsplit(x[j], qexp, r.xh, r.xl);
+    mgk_qsplit(y[j], qexp, r.yh, r.yl);
+    r.wk = (w ? w[j] : 1.0f) * (ew ? ew[j] : 1.0f);
+    r.k2h = r.k2l = r.hh = 0.0f;
     if (hpp) {
-        const double h2 = mgk_h2(hpp[j]);
+        const float hh = hpp[j] * hpp[j];
+        const double h2 = (double)hh;
         // w * e / (h^2 TWO_PI): the per-point normalisation of the kernel
-        wk = (float)((double)wk / (h2 * (double)MGK_TWO_PI_F));
-        hk[i] = make_double2(h2, MGK_LOG2E / (2.0 * h2));
+        r.wk = (float)((double)r.wk / (h2 * (double)MGK_TWO_PI_F));
+        const double k2 = MGK_LOG2E / (2.0 * h2);
+        r.k2h = (float)k2;
+        r.k2l = (float)(k2 - (double)r.k2h);
+        r.hh = hh;
     }
-    out[i] = make_float4(x[j], y[j], wk, 0.0f);
+    out[i] = r;
 }
 
 __global__ void k_hmax(int64_t n, const float* __restrict__ h, unsigned* out) {
@@ -259,18 +267,22 @@ int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float b
     idx->nbx = (int64_t)std::floor((xmax - xmin) / side) + 1;
     idx->nby = (int64_t)std::floor((ymax - ymin) / side) + 1;
     const int64_t nbins = idx->nbx * idx->nby;
+    // coordinate quantum: every coordinate within 3h (+ a bin) of a point is
+    // below 2^(22 - qexp) in magnitude, so hi parts are exact floats and
+    // differences of hi parts within the cutoff are exact
+    const double maxabs = std::max(std::max(std::fabs(xmin), std::fabs(xmax)),
+                                   std::max(std::fabs(ymin), std::fabs(ymax))) + 4.0 * idx->reach + 2.0 * side + 1.0;
+    idx->qexp = 22 - (int)std::ceil(std::log2(maxabs));
 
     // allocations (persistent)
     const size_t b_start = sizeof(int32_t) * (size_t)(nbins + 1);
-    const size_t b_pts = sizeof(float4) * (size_t)std::max<int64_t>(n, 1);
-    const size_t b_hk = idx->varh ? sizeof(double2) * (size_t)std::max<int64_t>(n, 1) : 0;
+    const size_t b_pts = sizeof(MgkPt) * (size_t)std::max<int64_t>(n, 1);
     const size_t b_perm = sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1);
     int st;
     if ((st = mgk_alloc(ctx, (void**)&idx->bin_start, b_start))) return st;
     if ((st = mgk_alloc(ctx, (void**)&idx->pts, b_pts))) return st;
-    if (b_hk && (st = mgk_alloc(ctx, (void**)&idx->hk, b_hk))) return st;
     if ((st = mgk_alloc(ctx, (void**)&idx->perm, b_perm))) return st;
-    idx->bytes = b_start + b_pts + b_hk + b_perm;
+    idx->bytes = b_start + b_pts + b_perm;
 
     // scratch: keys x2, vals x1 (+ perm as second value buffer), counts
     const int ntiles = (int)std::max<int64_t>(1, (n + kSortTile - 1) / kSortTile);
@@ -315,7 +327,7 @@ int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float b
             k_bin_starts<<<(unsigned)((n + 1 + 255) / 256), 256, 0, s>>>(n, kin, nbins, idx->bin_start);
             k_gather<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, idx->perm, pts->x, pts->y, pts->w,
                                                                  pts->has_ew ? pts->ew : nullptr,
-                                                                 idx->varh ? pts->h : nullptr, idx->pts, idx->hk);
+                                                                 idx->varh ? pts->h : nullptr, idx->qexp, idx->pts);
             if ((rc = cudaGetLastError()) != cudaSuccess) { rc = mgk_cuda_fail(ctx, (cudaError_t)rc, "index gather"); break; }
             MGK_COUNT_LAUNCH(ctx, (idx->varh ? 2 : 1) + 1 + 3 * passes + 2);
         } else {

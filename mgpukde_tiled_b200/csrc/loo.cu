@@ -26,7 +26,7 @@ __global__ void k_gather_ew(int64_t n, const int32_t* __restrict__ perm, const f
     if (i < n) sew[i] = ew ? ew[perm[i]] : 1.0f;
 }
 
-__global__ void __launch_bounds__(kLooThreads) k_loo(int64_t n, const float4* __restrict__ pts,
+__global__ void __launch_bounds__(kLooThreads) k_loo(int64_t n, const MgkPt* __restrict__ pts,
                                                      const float* __restrict__ sew,
                                                      const int32_t* __restrict__ bin_start, double ox, double oy,
                                                      double inv_side, int64_t nbx, int64_t nby, float h,
@@ -39,7 +39,8 @@ __global__ void __launch_bounds__(kLooThreads) k_loo(int64_t n, const float4* __
     const double cut = MGK_CUT * h2;
     const double k2 = MGK_LOG2E / (2.0 * h2);
     const double reach = 3.0 * (double)h;
-    const float4 q = pts[j];
+    const MgkPt qr = pts[j];
+    const float2 q = make_float2(qr.xh + qr.xl, qr.yh + qr.yl);
     int64_t bx0 = (int64_t)floor(((double)q.x - reach - ox) * inv_side);
     int64_t bx1 = (int64_t)floor(((double)q.x + reach - ox) * inv_side);
     int64_t by0 = (int64_t)floor(((double)q.y - reach - oy) * inv_side);
@@ -54,12 +55,12 @@ __global__ void __launch_bounds__(kLooThreads) k_loo(int64_t n, const float4* __
         const int64_t sb = bin_start[by * nbx + bx0], se = bin_start[by * nbx + bx1 + 1];
         for (int64_t i = sb + lane; i < se; i += 32) {
             if (i == j) continue;
-            const float4 p = pts[i];
-            const double dx = __dsub_rn((double)p.x, (double)q.x);
-            const double dy = __dsub_rn((double)p.y, (double)q.y);
+            const MgkPt p = pts[i];
+            const double dx = __dsub_rn((double)(p.xh + p.xl), (double)q.x);
+            const double dy = __dsub_rn((double)(p.yh + p.yl), (double)q.y);
             const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
             if (d2 < cut) {
-                const float t = mgk_exp2_neg(d2 * k2) * (p.z * sew[i]);
+                const float t = mgk_exp2_neg(d2 * k2) * (p.wk * sew[i]);
                 const float yk = t - c;
                 const float tk = s + yk;
                 c = (tk - s) - yk;

@@ -62,10 +62,23 @@ struct mgk_raster {
     bool marked = false;
 };
 
+// One point of the bin-major index (32 B, one bulk copy moves whole records).
+// Coordinates are split on a global quantum q = 2^-qexp: x = xh + xl exactly,
+// xh a multiple of q, |xl| <= q/2.  Cell centres are split on the same
+// quantum, so xh - cxh is exact in FP32 and the distance is recovered
+// exactly as a float pair.  wk = w * e (fixed h) or w * e / (h^2 TWO_PI)
+// (per-point h); k2h + k2l = log2(e) / (2 h^2) and hh = h*h (float product)
+// for per-point h, zero otherwise.
+struct __align__(16) MgkPt {
+    float xh, yh, xl, yl;
+    float wk, k2h, k2l, hh;
+};
+
 struct mgk_index {
     mgk_ctx* ctx = nullptr;
     int64_t n = 0;
     bool varh = false;
+    int qexp = 0;  // coordinate quantum 2^-qexp
     // fixed-h constants (double): h^2 as the reference forms it, 9 h^2,
     // log2(e)/(2 h^2), 1/(h^2 TWO_PI), 3 h
     float h = 0.0f;
@@ -75,8 +88,7 @@ struct mgk_index {
     int64_t nbx = 1, nby = 1;
     int32_t* bin_start = nullptr;  // nbx*nby + 1
     // bin-major point data
-    float4* pts = nullptr;   // x, y, w*e (fixed h) or w*e/(h^2 TWO_PI) (per-point h), unused
-    double2* hk = nullptr;   // per-point h: (h^2, log2(e)/(2 h^2)); NULL for fixed h
+    MgkPt* pts = nullptr;
     int32_t* perm = nullptr; // sorted position -> input index
     uint64_t bytes = 0;
 };
@@ -134,6 +146,14 @@ __device__ __forceinline__ double mgk_d2_exact(float x0, float y0, float x1, flo
     const double dx = __dsub_rn((double)x1, (double)x0);
     const double dy = __dsub_rn((double)y1, (double)y0);
     return __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
+}
+
+// Splits a float coordinate on the quantum 2^-qexp: hi = nearest multiple,
+// lo = remainder, both exact floats (|v| < 2^(22 - qexp) assumed).
+__device__ __host__ __forceinline__ void mgk_qsplit(float v, int qexp, float& hi, float& lo) {
+    const double s = ldexp(1.0, qexp);
+    hi = (float)(rint((double)v * s) / s);
+    lo = (float)((double)v - (double)hi);
 }
 
 // h^2 exactly as the reference's CPU path forms it: float product widened.

@@ -68,7 +68,8 @@ def test_golden_case_components(ctx, case):
     nd = d["density_mask"] == d["dg"].nodata
     assert np.array_equal(r["density"][nd], d["density_mask"][nd])
     assert rel_err(r["density"][~nd], ref["density"][~nd]).max() <= RTOL
-    assert rel_err(r["density_fp64"][~nd], ref["density"][~nd]).max() <= 1e-7  # float rounding of an FP64 result
+    # FP64 form: FP64 sums of float-stored w*e, rounded to float once
+    assert rel_err(r["density_fp64"][~nd], ref["density"][~nd]).max() <= 3e-7
     assert r["density_evals"] == ref["density_evals"]
     if int(d["edge"]):
         assert np.array_equal(r["boundary"], ref["boundary"])
