@@ -72,7 +72,7 @@ struct DParams {
     int qexp;
     // fixed-h constants
     double h2, k0, cut_d2, reach;
-    float k2h, k2l, cutlh, cutll, cutf;
+    float k2h, k2l, cutlh, cutll, cutf, epsd2;
     unsigned long long* evals;
     unsigned long long* err;
 };
@@ -163,10 +163,12 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
 // (difference of two multiples of the quantum), |lo| <= quantum; the pair
 // (dh, de) is dx exactly and the products are error-free, so ah + al is a
 // to about 2^-44 relative.
-__device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, float k2l, float& ah, float& al) {
+__device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, float k2l, float& ah, float& al,
+                                              float& d2) {
     const float dh = __fadd_rn(t, lo);
     const float de = __fsub_rn(lo, __fsub_rn(dh, t));
     const float p = __fmul_rn(dh, dh);
+    d2 = p;
     float pe = __fmaf_rn(dh, dh, -p);
     pe = __fmaf_rn(__fmul_rn(2.0f, dh), de, pe);
     ah = __fmul_rn(p, k2h);
@@ -179,22 +181,33 @@ __device__ __forceinline__ float exp2_pair(float ah, float al) {
     return __fmaf_rn(__fmul_rn(-al, MGK_LN2F), e, e);
 }
 
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// acc += e * f when a < t: one compare and one predicated FFMA.
+__device__ __forceinline__ void fma_if_less(float& acc, float a, float t, float e, float f) {
+    asm("{\n .reg .pred p;\n setp.lt.f32 p, %1, %2;\n @p fma.rn.f32 %0, %3, %4, %0;\n}\n"
+        : "+f"(acc)
+        : "f"(a), "f"(t), "f"(e), "f"(f));
+}
+
 // Does some column of a regular 64-column block lie within the ambiguity
-// band of row threshold T?  The row's exponent a(x) = k2 (x - px)^2 crosses T
-// at x = px +- s, s = sqrt(T / k2); a column within w = eps / (k2 s) (plus a
-// margin for the float error of the crossing position) of a crossing may be
-// classified differently in FP32 than in FP64.  prel0 = px - cx_0.
-__device__ __forceinline__ bool amb_row(float T, float k2h, float prel0, float cs, float inv_cs) {
-    if (T < -2.0f * kAmbEps) return false;
-    const float s2 = fmaxf(T, 0.0f) / k2h;
-    const float s = sqrtf(s2);
-    const float w = (2.0f * kAmbEps) / (k2h * 2.0f * s + 1e-30f) + 4e-7f * (s + fabsf(prel0)) + 1e-6f * cs;
-    if (w * inv_cs > 0.25f) return true;
-    const float fp = (prel0 + s) * inv_cs, fm = (prel0 - s) * inv_cs;
-    const float np = rintf(fp), nm = rintf(fm);
-    const bool hp = np >= -1.0f && np <= (float)kBlk && fabsf(fp - np) * cs < w;
-    const bool hm = nm >= -1.0f && nm <= (float)kBlk && fabsf(fm - nm) * cs < w;
-    return hp || hm;
+// band of a row?  For the row, in-disc columns satisfy dx^2 < s2 with
+// s2 = 9h^2 - dy^2 (squared half-chord); the FP32 decision a_j < T_i can
+// differ from the exact one only for columns with |dx^2 - s2| < eps_d2, i.e.
+// within eps_d2 / (2 s) of a crossing x = px +- s.  pc0 = (px - cx_0) / cs in
+// columns; margins cover the float error of the crossing positions.
+__device__ __forceinline__ bool amb_row(float s2, float eps_d2, float pc0, float inv_cs) {
+    const float r = rsqrt_approx(fmaxf(s2, 1e-30f));
+    const float sc = s2 * r * inv_cs;  // half-chord in columns (0 when s2 <= 0)
+    const float wc = __fmaf_rn(eps_d2 * 0.5f * inv_cs, r, __fmaf_rn(4e-7f, sc + fabsf(pc0), 1e-6f));
+    const float fp = pc0 + sc, fm = pc0 - sc;
+    const bool hp = fabsf(fp - 31.5f) <= 33.0f && fabsf(fp - rintf(fp)) < wc;
+    const bool hm = fabsf(fm - 31.5f) <= 33.0f && fabsf(fm - rintf(fm)) < wc;
+    return s2 >= -eps_d2 && (wc > 0.25f || hp || hm);
 }
 
 struct BatchIt {
@@ -222,13 +235,23 @@ __device__ __forceinline__ int next_batch(const DParams& P, const BlockGeom& G, 
     return 0;
 }
 
+// Dynamic shared memory of k_density (bytes); factor tables are padded to a
+// row stride of 72 float2 so that phase-A stores of 4 points hit distinct banks.
+constexpr int kFStride = 72;
+constexpr size_t kSmemStage = 2 * kMB * sizeof(MgkPt);
+constexpr size_t kSmemTab = (size_t)kMB * kFStride * sizeof(float2);
+constexpr size_t kSmemKahan = 16 * kThreads * sizeof(float2);
+constexpr size_t kDensitySmem = kSmemStage + 2 * kSmemTab + kSmemKahan;
+
 template <bool VARH, bool COUNT>
-__global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
-    __shared__ __align__(16) MgkPt stage[2][kMB];
+__global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
+    extern __shared__ __align__(128) unsigned char dsm[];
+    MgkPt* stage = reinterpret_cast<MgkPt*>(dsm);                                  // [2][kMB]
+    float2* colf = reinterpret_cast<float2*>(dsm + kSmemStage);                    // [kMB][kFStride] (a_hi, E)
+    float2* rowf = reinterpret_cast<float2*>(dsm + kSmemStage + kSmemTab);         // [kMB][kFStride] (T, F)
+    float2* kah = reinterpret_cast<float2*>(dsm + kSmemStage + 2 * kSmemTab);     // [16][kThreads] Kahan (s, c)
     __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ __align__(16) float2 colf[kMB][kBlk];  // (a_hi, E) per point and column
-    __shared__ __align__(16) float2 rowf[kMB][kBlk];  // (T, F) per point and row
-    __shared__ unsigned long long rowflag[kMB];
+    __shared__ __align__(8) unsigned long long rowflag[kMB];
     __shared__ unsigned char procmask[kMB];
     __shared__ float s_cxh[kBlk], s_cxl[kBlk], s_cyh[kBlk], s_cyl[kBlk], s_cxg[kBlk], s_cyg[kBlk];
     __shared__ int s_abort;
@@ -258,8 +281,10 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         fence_mbar_init();
         s_abort = 0;
     }
+#pragma unroll
+    for (int k = 0; k < 16; k++) kah[k * kThreads + tid] = make_float2(0.0f, 0.0f);
     regular = __syncthreads_and(regular);
-    const float cs_f = (float)P.cs, inv_cs = 1.0f / (float)P.cs;
+    const float inv_cs = 1.0f / (float)P.cs;
 
     // validity of the lane's 16 cells (inside the tile and not NoData)
     unsigned valid = 0;
@@ -273,15 +298,15 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
             valid |= (unsigned)v << (i * 4 + j);
         }
 
-    float acc_s[16], acc_c[16], part[16];
+    float part[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) acc_s[k] = acc_c[k] = part[k] = 0.0f;
+    for (int k = 0; k < 16; k++) part[k] = 0.0f;
     unsigned long long cnt = 0;
     unsigned pc = 0;  // points processed by this warp (warp-uniform)
 
-    // phase A roles: point q = tid / 8, part k = tid % 8 (columns/rows k*8.., skip test of warp k)
+    // phase A roles: point q = tid / 8, part k = tid % 8: columns and rows
+    // k, k+8, ..., k+56, and the skip test of warp k
     const int qa = tid >> 3, ka = tid & 7;
-    // warp k's sub-block rectangle (cells inside the tile), for the skip test
     const int sk_wr = ka >> 1, sk_wc = ka & 1;
     const bool sk_on = (sk_wr * 16 < G.nrow) && (sk_wc * 32 < G.ncol);
     const int sk_c0 = sk_wc * 32, sk_c1 = min(sk_wc * 32 + 31, G.ncol - 1);
@@ -292,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
     int m = next_batch(P, G, it, bit, src);
     if (m > 0 && tid == 0) {
         mbar_arrive_tx(&mbar[0], (unsigned)(m * sizeof(MgkPt)));
-        bulk_g2s(&stage[0][0], P.pts + src, (unsigned)(m * sizeof(MgkPt)), &mbar[0]);
+        bulk_g2s(&stage[0], P.pts + src, (unsigned)(m * sizeof(MgkPt)), &mbar[0]);
     }
     unsigned phase0 = 0, phase1 = 0;
     int buf = 0;
@@ -304,7 +329,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         const int nm = next_batch(P, G, it, bit, nsrc);
         if (nm > 0 && tid == 0) {
             mbar_arrive_tx(&mbar[buf ^ 1], (unsigned)(nm * sizeof(MgkPt)));
-            bulk_g2s(&stage[buf ^ 1][0], P.pts + nsrc, (unsigned)(nm * sizeof(MgkPt)), &mbar[buf ^ 1]);
+            bulk_g2s(&stage[(buf ^ 1) * kMB], P.pts + nsrc, (unsigned)(nm * sizeof(MgkPt)), &mbar[buf ^ 1]);
         }
         const unsigned par = buf ? phase1 : phase0;
         if (!mbar_wait(&mbar[buf], par)) {
@@ -322,40 +347,47 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         }
         if (buf) phase1 ^= 1u;
         else phase0 ^= 1u;
+        const MgkPt* st = stage + buf * kMB;
 
         // ---------------- phase A ----------------
         {
             bool proc = false;
-            unsigned fl = 0;
+            unsigned lo32 = 0, hi32 = 0;
             if (qa < m) {
-                const MgkPt r = stage[buf][qa];
-                float k2h, k2l, cutf;
+                const MgkPt r = st[qa];
+                float k2h, k2l, cutf, epsd2;
                 if (VARH) {
                     k2h = r.k2h;
                     k2l = r.k2l;
                     cutf = 9.0f * r.hh;
+                    epsd2 = r.hh * (4.0f * kAmbEps / (float)MGK_LOG2E);
                 } else {
                     k2h = P.k2h;
                     k2l = P.k2l;
                     cutf = P.cutf;
+                    epsd2 = P.epsd2;
                 }
+                float2* crow = colf + qa * kFStride;
+                float2* rrow = rowf + qa * kFStride;
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
-                    const int j = ka * 8 + c;
-                    float ah, al;
-                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al);
-                    colf[qa][j] = make_float2(ah, exp2_pair(ah, al));
+                    const int j = ka + 8 * c;
+                    float ah, al, d2;
+                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
+                    crow[j] = make_float2(ah, exp2_pair(ah, al));
                 }
-                const float prel0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0]));
+                const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
-                    const int i = ka * 8 + c;
-                    float bh, bl;
-                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl);
+                    const int i = ka + 8 * c;
+                    float bh, bl, d2;
+                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
                     const float T = __fadd_rn(__fsub_rn(P.cutlh, bh), __fsub_rn(P.cutll, bl));
-                    rowf[qa][i] = make_float2(T, __fmul_rn(r.wk, exp2_pair(bh, bl)));
-                    const bool a = regular ? amb_row(T, k2h, prel0, cs_f, inv_cs) : (T > -2.0f * kAmbEps);
-                    fl |= (unsigned)a << c;
+                    rrow[i] = make_float2(T, __fmul_rn(r.wk, exp2_pair(bh, bl)));
+                    const float s2 = cutf - d2;
+                    const bool a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2);
+                    if (c < 4) lo32 |= (unsigned)a << (ka + 8 * c);
+                    else hi32 |= (unsigned)a << (ka + 8 * (c - 4));
                 }
                 if (sk_on) {
                     // distance from the point to the sub-block rectangle of cell centres
@@ -368,9 +400,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
                     proc = ddx * ddx + ddy * ddy < cutf * 1.0001f;
                 }
             }
-            // 64 row flags of point qa: 8 bits from each of its 8 threads (same warp)
-            unsigned lo32 = ka < 4 ? fl << (8 * ka) : 0u;
-            unsigned hi32 = ka >= 4 ? fl << (8 * (ka - 4)) : 0u;
+            // the 64 row flags of point qa come from its 8 threads (same warp)
 #pragma unroll
             for (int o = 1; o < 8; o <<= 1) {
                 lo32 |= __shfl_xor_sync(0xffffffffu, lo32, o);
@@ -385,27 +415,37 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         __syncthreads();
 
         // ---------------- phase B ----------------
+        const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(rowflag);
         for (int q = 0; q < m; q++) {
             if (!((procmask[q] >> warp) & 1u)) continue;
-            const float4 c01 = *reinterpret_cast<const float4*>(&colf[q][wc * 32 + tc * 4]);
-            const float4 c23 = *reinterpret_cast<const float4*>(&colf[q][wc * 32 + tc * 4 + 2]);
-            const float4 r01 = *reinterpret_cast<const float4*>(&rowf[q][wr * 16 + tr * 4]);
-            const float4 r23 = *reinterpret_cast<const float4*>(&rowf[q][wr * 16 + tr * 4 + 2]);
+            const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
+            const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
+            const float4 c01 = *reinterpret_cast<const float4*>(crow);
+            const float4 c23 = *reinterpret_cast<const float4*>(crow + 2);
+            const float4 r01 = *reinterpret_cast<const float4*>(rrow);
+            const float4 r23 = *reinterpret_cast<const float4*>(rrow + 2);
             const float ca[4] = {c01.x, c01.z, c23.x, c23.z}, ce[4] = {c01.y, c01.w, c23.y, c23.w};
-            const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rf[4] = {r01.y, r01.w, r23.y, r23.w};
+            const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rv[4] = {r01.y, r01.w, r23.y, r23.w};
             unsigned inm = 0;
+            if (COUNT) {
 #pragma unroll
-            for (int i = 0; i < 4; i++)
+                for (int i = 0; i < 4; i++)
 #pragma unroll
-                for (int j = 0; j < 4; j++) {
-                    const bool in = ca[j] < rt[i];
-                    if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rf[i], part[i * 4 + j]);
-                    if (COUNT) inm |= (unsigned)in << (i * 4 + j);
-                }
-            const unsigned fl = (unsigned)(rowflag[q] >> (wr * 16 + tr * 4)) & 0xfu;
+                    for (int j = 0; j < 4; j++) {
+                        const bool in = ca[j] < rt[i];
+                        if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
+                        inm |= (unsigned)in << (i * 4 + j);
+                    }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], ca[j], rt[i], ce[j], rv[i]);
+            }
+            const unsigned fl = ((unsigned)rf16[q * 4 + wr] >> (tr * 4)) & 0xfu;
             if (__any_sync(0xffffffffu, fl != 0u)) {
                 if (fl) {
-                    const MgkPt r = stage[buf][q];
+                    const MgkPt r = st[q];
                     const float px = r.xh + r.xl, py = r.yh + r.yl;
                     const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
 #pragma unroll
@@ -417,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
                                                          s_cyg[wr * 16 + tr * 4 + i]) < cut;
                             const bool fi = ca[j] < rt[i];
                             if (ex != fi) {
-                                const float t = __fmul_rn(ce[j], rf[i]);
+                                const float t = __fmul_rn(ce[j], rv[i]);
                                 part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
                                 if (COUNT) inm ^= 1u << (i * 4 + j);
                             }
@@ -430,12 +470,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
             if ((pc & 7u) == 0) {
 #pragma unroll
                 for (int k = 0; k < 16; k++) {
-                    kahan_add(acc_s[k], acc_c[k], part[k]);
+                    float2 a = kah[k * kThreads + tid];
+                    kahan_add(a.x, a.y, part[k]);
+                    kah[k * kThreads + tid] = a;
                     part[k] = 0.0f;
                 }
             }
         }
-        __syncthreads();  // colf/rowf and stage[buf] are reused next
+        __syncthreads();  // factor tables and stage[buf] are reused next
         m = nm;
         src = nsrc;
         buf ^= 1;
@@ -448,8 +490,6 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         __syncthreads();
         return;
     }
-#pragma unroll
-    for (int k = 0; k < 16; k++) kahan_add(acc_s[k], acc_c[k], part[k]);
 
     // epilogue: FP64 result = (s - c) * normalisation
     const double norm = VARH ? 1.0 : P.k0;
@@ -458,9 +498,11 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int k = i * 4 + j;
+            float2 a = kah[k * kThreads + tid];
+            kahan_add(a.x, a.y, part[k]);
             const int r = wr * 16 + tr * 4 + i, c = wc * 32 + tc * 4 + j;
             if (r >= G.nrow || c >= G.ncol) continue;
-            const double v = ((double)acc_s[k] - (double)acc_c[k]) * norm;
+            const double v = ((double)a.x - (double)a.y) * norm;
             if (it.slot >= 0) {
                 P.scratch[(size_t)it.slot * (kBlk * kBlk) + r * kBlk + c] = v;
             } else {
@@ -473,6 +515,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density(DParams P) {
         if (lane == 0 && cnt) atomicAdd(P.evals, cnt);
     }
 }
+
 
 // Plain FP64 form: same blocks, work items and candidate lists; per pair an
 // exact FP64 distance, the cutoff, a double exp and a double accumulate.
@@ -561,6 +604,12 @@ __global__ void k_merge(DParams P, const int32_t* __restrict__ blocks, const int
     }
 }
 
+template <bool VARH, bool COUNT>
+void launch_density(unsigned grid, cudaStream_t s, const DParams& P) {
+    cudaFuncSetAttribute(k_density<VARH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+    k_density<VARH, COUNT><<<grid, kThreads, kDensitySmem, s>>>(P);
+}
+
 }  // namespace
 
 int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
@@ -601,6 +650,8 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         P.cutlh = (float)cutl;
         P.cutll = (float)(cutl - (double)P.cutlh);
         P.cutf = (float)idx->cut_d2;
+        // ambiguity band in d^2 units: |a - T| < kAmbEps  <=>  |dx^2 - s^2| < kAmbEps / k2 (x2 margin)
+        P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
     }
     P.evals = d_evals;
     P.err = ctx->d_counter + 7;
@@ -679,11 +730,11 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
             if (idx->varh) k_density_fp64<true><<<grid, kThreads, 0, s>>>(P);
             else k_density_fp64<false><<<grid, kThreads, 0, s>>>(P);
         } else if (d_evals) {
-            if (idx->varh) k_density<true, true><<<grid, kThreads, 0, s>>>(P);
-            else k_density<false, true><<<grid, kThreads, 0, s>>>(P);
+            if (idx->varh) launch_density<true, true>(grid, s, P);
+            else launch_density<false, true>(grid, s, P);
         } else {
-            if (idx->varh) k_density<true, false><<<grid, kThreads, 0, s>>>(P);
-            else k_density<false, false><<<grid, kThreads, 0, s>>>(P);
+            if (idx->varh) launch_density<true, false>(grid, s, P);
+            else launch_density<false, false>(grid, s, P);
         }
         cudaEventRecord(ctx->ev_b, s);
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
