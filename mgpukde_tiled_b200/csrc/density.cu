@@ -160,17 +160,15 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
 }
 
 // Exponent a = (t + lo)^2 (k2h + k2l) as a float pair ah + al.  t is exact
-// (difference of two multiples of the quantum), |lo| <= quantum; the pair
-// (dh, de) is dx exactly and the products are error-free, so ah + al is a
-// to about 2^-44 relative.
+// (difference of two multiples of the quantum), |lo| <= quantum (a few
+// ulps of t at most): (t + lo)^2 = t^2 + (2t + lo) lo, t^2 is split
+// error-free into p + pe, and the products with k2 are error-free, so ah + al
+// is a to about 2^-40 relative.  d2 = p approximates dx^2.
 __device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, float k2l, float& ah, float& al,
                                               float& d2) {
-    const float dh = __fadd_rn(t, lo);
-    const float de = __fsub_rn(lo, __fsub_rn(dh, t));
-    const float p = __fmul_rn(dh, dh);
-    d2 = p;
-    float pe = __fmaf_rn(dh, dh, -p);
-    pe = __fmaf_rn(__fmul_rn(2.0f, dh), de, pe);
+    const float p = __fmul_rn(t, t);
+    const float pe = __fmaf_rn(__fadd_rn(t, __fadd_rn(t, lo)), lo, __fmaf_rn(t, t, -p));
+    d2 = __fadd_rn(p, pe);
     ah = __fmul_rn(p, k2h);
     const float ae = __fmaf_rn(p, k2h, -ah);
     al = __fmaf_rn(pe, k2h, __fmaf_rn(p, k2l, ae));
@@ -199,15 +197,20 @@ __device__ __forceinline__ void fma_if_less(float& acc, float a, float t, float 
 // s2 = 9h^2 - dy^2 (squared half-chord); the FP32 decision a_j < T_i can
 // differ from the exact one only for columns with |dx^2 - s2| < eps_d2, i.e.
 // within eps_d2 / (2 s) of a crossing x = px +- s.  pc0 = (px - cx_0) / cs in
-// columns; margins cover the float error of the crossing positions.
-__device__ __forceinline__ bool amb_row(float s2, float eps_d2, float pc0, float inv_cs) {
+// columns; margins cover the float error of the crossing positions.  Returns
+// two bits: bit 0 for columns 0-31 (warp column half 0), bit 1 for 32-63.
+__device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, float inv_cs) {
     const float r = rsqrt_approx(fmaxf(s2, 1e-30f));
     const float sc = s2 * r * inv_cs;  // half-chord in columns (0 when s2 <= 0)
     const float wc = __fmaf_rn(eps_d2 * 0.5f * inv_cs, r, __fmaf_rn(4e-7f, sc + fabsf(pc0), 1e-6f));
+    if (s2 < -eps_d2) return 0u;
+    if (wc > 0.25f) return 3u;
     const float fp = pc0 + sc, fm = pc0 - sc;
-    const bool hp = fabsf(fp - 31.5f) <= 33.0f && fabsf(fp - rintf(fp)) < wc;
-    const bool hm = fabsf(fm - 31.5f) <= 33.0f && fabsf(fm - rintf(fm)) < wc;
-    return s2 >= -eps_d2 && (wc > 0.25f || hp || hm);
+    const bool np = fabsf(fp - rintf(fp)) < wc, nm = fabsf(fm - rintf(fm)) < wc;
+    // a crossing near column position f concerns half 0 if f <= 32, half 1 if f >= 31
+    const unsigned b0 = (np && fp >= -1.0f && fp <= 32.0f) || (nm && fm >= -1.0f && fm <= 32.0f);
+    const unsigned b1 = (np && fp >= 31.0f && fp <= 64.0f) || (nm && fm >= 31.0f && fm <= 64.0f);
+    return b0 | (b1 << 1);
 }
 
 struct BatchIt {
@@ -251,8 +254,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
     float2* rowf = reinterpret_cast<float2*>(dsm + kSmemStage + kSmemTab);         // [kMB][kFStride] (T, F)
     float2* kah = reinterpret_cast<float2*>(dsm + kSmemStage + 2 * kSmemTab);     // [16][kThreads] Kahan (s, c)
     __shared__ __align__(8) uint64_t mbar[2];
-    __shared__ __align__(8) unsigned long long rowflag[kMB];
-    __shared__ unsigned char procmask[kMB];
+    __shared__ __align__(16) unsigned long long rowflag[kMB][2];  // per column half: 64 row bits
+    __shared__ unsigned char procmask[kMB];  // warp w processes the point
+    __shared__ unsigned char fullmask[kMB];  // every cell of warp w's sub-block is inside the cutoff
     __shared__ float s_cxh[kBlk], s_cxl[kBlk], s_cyh[kBlk], s_cyl[kBlk], s_cxg[kBlk], s_cyg[kBlk];
     __shared__ int s_abort;
 
@@ -351,8 +355,8 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
 
         // ---------------- phase A ----------------
         {
-            bool proc = false;
-            unsigned lo32 = 0, hi32 = 0;
+            bool proc = false, full = false;
+            unsigned lo32 = 0, hi32 = 0, lo32h = 0, hi32h = 0;
             if (qa < m) {
                 const MgkPt r = st[qa];
                 float k2h, k2l, cutf, epsd2;
@@ -385,9 +389,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                     const float T = __fadd_rn(__fsub_rn(P.cutlh, bh), __fsub_rn(P.cutll, bl));
                     rrow[i] = make_float2(T, __fmul_rn(r.wk, exp2_pair(bh, bl)));
                     const float s2 = cutf - d2;
-                    const bool a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2);
-                    if (c < 4) lo32 |= (unsigned)a << (ka + 8 * c);
-                    else hi32 |= (unsigned)a << (ka + 8 * (c - 4));
+                    const unsigned a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2 ? 3u : 0u);
+                    const unsigned sh = (ka + 8 * c) & 31;
+                    if (c < 4) {
+                        lo32 |= (a & 1u) << sh;
+                        lo32h |= (a >> 1) << sh;
+                    } else {
+                        hi32 |= (a & 1u) << sh;
+                        hi32h |= (a >> 1) << sh;
+                    }
                 }
                 if (sk_on) {
                     // distance from the point to the sub-block rectangle of cell centres
@@ -398,26 +408,49 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                     const float ddx = fmaxf(0.0f, fmaxf(dxl, dxr));
                     const float ddy = fmaxf(0.0f, fmaxf(dyt, dyb));
                     proc = ddx * ddx + ddy * ddy < cutf * 1.0001f;
+                    // farthest corner well inside the cutoff: no cell of the sub-block needs the test
+                    const float fx = fmaxf(fabsf(dxl), fabsf(dxr)), fy = fmaxf(fabsf(dyt), fabsf(dyb));
+                    full = fx * fx + fy * fy < cutf * 0.9999f;
                 }
             }
-            // the 64 row flags of point qa come from its 8 threads (same warp)
+            // the row flags of point qa come from its 8 threads (same warp)
 #pragma unroll
             for (int o = 1; o < 8; o <<= 1) {
                 lo32 |= __shfl_xor_sync(0xffffffffu, lo32, o);
                 hi32 |= __shfl_xor_sync(0xffffffffu, hi32, o);
+                lo32h |= __shfl_xor_sync(0xffffffffu, lo32h, o);
+                hi32h |= __shfl_xor_sync(0xffffffffu, hi32h, o);
             }
             const unsigned bal = __ballot_sync(0xffffffffu, proc);
+            const unsigned balf = __ballot_sync(0xffffffffu, full);
             if (ka == 0) {
-                rowflag[qa] = ((unsigned long long)hi32 << 32) | lo32;
+                rowflag[qa][0] = ((unsigned long long)hi32 << 32) | lo32;
+                rowflag[qa][1] = ((unsigned long long)hi32h << 32) | lo32h;
                 procmask[qa] = (unsigned char)((bal >> (8 * (qa & 3))) & 0xffu);
+                fullmask[qa] = (unsigned char)((balf >> (8 * (qa & 3))) & 0xffu);
             }
         }
         __syncthreads();
 
         // ---------------- phase B ----------------
-        const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(rowflag);
+        const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
         for (int q = 0; q < m; q++) {
             if (!((procmask[q] >> warp) & 1u)) continue;
+            if (!COUNT && ((fullmask[q] >> warp) & 1u)) {
+                // the whole sub-block is inside the cutoff: one FFMA per cell
+                const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
+                const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
+                const float4 c01 = *reinterpret_cast<const float4*>(crow);
+                const float4 c23 = *reinterpret_cast<const float4*>(crow + 2);
+                const float4 r01 = *reinterpret_cast<const float4*>(rrow);
+                const float4 r23 = *reinterpret_cast<const float4*>(rrow + 2);
+                const float ce[4] = {c01.y, c01.w, c23.y, c23.w};
+                const float rv[4] = {r01.y, r01.w, r23.y, r23.w};
+#pragma unroll
+                for (int i = 0; i < 4; i++)
+#pragma unroll
+                    for (int j = 0; j < 4; j++) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
+            } else {
             const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
             const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
             const float4 c01 = *reinterpret_cast<const float4*>(crow);
@@ -442,7 +475,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
 #pragma unroll
                     for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], ca[j], rt[i], ce[j], rv[i]);
             }
-            const unsigned fl = ((unsigned)rf16[q * 4 + wr] >> (tr * 4)) & 0xfu;
+            const unsigned fl = ((unsigned)rf16[q * 8 + wc * 4 + wr] >> (tr * 4)) & 0xfu;
             if (__any_sync(0xffffffffu, fl != 0u)) {
                 if (fl) {
                     const MgkPt r = st[q];
@@ -466,6 +499,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                 }
             }
             if (COUNT) cnt += __popc(inm & valid);
+            }
             pc++;
             if ((pc & 7u) == 0) {
 #pragma unroll
