@@ -160,14 +160,17 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
 }
 
 // Exponent a = (t + lo)^2 (k2h + k2l) as a float pair ah + al.  t is exact
-// (difference of two multiples of the quantum), |lo| <= quantum (a few
-// ulps of t at most): (t + lo)^2 = t^2 + (2t + lo) lo, t^2 is split
-// error-free into p + pe, and the products with k2 are error-free, so ah + al
-// is a to about 2^-40 relative.  d2 = p approximates dx^2.
+// (difference of two multiples of the quantum), |lo| <= quantum.  dx = t + lo
+// is formed as an exact pair (dh, de) first, so p = dh^2 is the rounded
+// square, pe its error-free remainder plus 2 dh de, and the products with k2
+// are error-free: ah is a to within a few ulps (|al| <= ~3 ulp(ah)), and
+// ah + al is a to about 2^-40 relative.  d2 = p + pe approximates dx^2.
 __device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, float k2l, float& ah, float& al,
                                               float& d2) {
-    const float p = __fmul_rn(t, t);
-    const float pe = __fmaf_rn(__fadd_rn(t, __fadd_rn(t, lo)), lo, __fmaf_rn(t, t, -p));
+    const float dh = __fadd_rn(t, lo);
+    const float de = __fsub_rn(lo, __fsub_rn(dh, t));
+    const float p = __fmul_rn(dh, dh);
+    const float pe = __fmaf_rn(__fadd_rn(dh, dh), de, __fmaf_rn(dh, dh, -p));
     d2 = __fadd_rn(p, pe);
     ah = __fmul_rn(p, k2h);
     const float ae = __fmaf_rn(p, k2h, -ah);
