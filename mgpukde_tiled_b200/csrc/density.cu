@@ -436,81 +436,85 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
         __syncthreads();
 
         // ---------------- phase B ----------------
-        const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
-        for (int q = 0; q < m; q++) {
-            if (!((procmask[q] >> warp) & 1u)) continue;
-            if (!COUNT && ((fullmask[q] >> warp) & 1u)) {
-                // the whole sub-block is inside the cutoff: one FFMA per cell
+        {
+            // this warp's processed, fully-inside and flagged points of the batch as bit masks
+            const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
+            const bool lv = lane < m;
+            const bool pm = lv && ((procmask[lane] >> warp) & 1u);
+            const bool fm = lv && ((fullmask[lane] >> warp) & 1u);
+            const unsigned myflag = lv ? (unsigned)rf16[lane * 8 + wc * 4 + wr] : 0u;  // 16 rows, point `lane`
+            unsigned todo = __ballot_sync(0xffffffffu, pm);
+            const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
+            const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
+            while (todo) {
+                const int q = __ffs(todo) - 1;
+                todo &= todo - 1u;
                 const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
                 const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
                 const float4 c01 = *reinterpret_cast<const float4*>(crow);
                 const float4 c23 = *reinterpret_cast<const float4*>(crow + 2);
                 const float4 r01 = *reinterpret_cast<const float4*>(rrow);
                 const float4 r23 = *reinterpret_cast<const float4*>(rrow + 2);
-                const float ce[4] = {c01.y, c01.w, c23.y, c23.w};
-                const float rv[4] = {r01.y, r01.w, r23.y, r23.w};
+                const float ca[4] = {c01.x, c01.z, c23.x, c23.z}, ce[4] = {c01.y, c01.w, c23.y, c23.w};
+                const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rv[4] = {r01.y, r01.w, r23.y, r23.w};
+                if (!COUNT && ((fullb >> q) & 1u)) {
+                    // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
-                for (int i = 0; i < 4; i++)
+                    for (int i = 0; i < 4; i++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
-            } else {
-            const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
-            const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
-            const float4 c01 = *reinterpret_cast<const float4*>(crow);
-            const float4 c23 = *reinterpret_cast<const float4*>(crow + 2);
-            const float4 r01 = *reinterpret_cast<const float4*>(rrow);
-            const float4 r23 = *reinterpret_cast<const float4*>(rrow + 2);
-            const float ca[4] = {c01.x, c01.z, c23.x, c23.z}, ce[4] = {c01.y, c01.w, c23.y, c23.w};
-            const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rv[4] = {r01.y, r01.w, r23.y, r23.w};
-            unsigned inm = 0;
-            if (COUNT) {
+                        for (int j = 0; j < 4; j++) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
+                } else {
+                    unsigned inm = 0;
+                    if (COUNT) {
 #pragma unroll
-                for (int i = 0; i < 4; i++)
+                        for (int i = 0; i < 4; i++)
 #pragma unroll
-                    for (int j = 0; j < 4; j++) {
-                        const bool in = ca[j] < rt[i];
-                        if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
-                        inm |= (unsigned)in << (i * 4 + j);
+                            for (int j = 0; j < 4; j++) {
+                                const bool in = ca[j] < rt[i];
+                                if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
+                                inm |= (unsigned)in << (i * 4 + j);
+                            }
+                    } else {
+#pragma unroll
+                        for (int i = 0; i < 4; i++)
+#pragma unroll
+                            for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], ca[j], rt[i], ce[j], rv[i]);
                     }
-            } else {
+                    if ((ambb >> q) & 1u) {
+                        // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
+                        const unsigned fl = (__shfl_sync(0xffffffffu, myflag, q) >> (tr * 4)) & 0xfu;
+                        if (fl) {
+                            const MgkPt r = st[q];
+                            const float px = r.xh + r.xl, py = r.yh + r.yl;
+                            const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
 #pragma unroll
-                for (int i = 0; i < 4; i++)
+                            for (int i = 0; i < 4; i++) {
+                                if (!((fl >> i) & 1u)) continue;
 #pragma unroll
-                    for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], ca[j], rt[i], ce[j], rv[i]);
-            }
-            const unsigned fl = ((unsigned)rf16[q * 8 + wc * 4 + wr] >> (tr * 4)) & 0xfu;
-            if (__any_sync(0xffffffffu, fl != 0u)) {
-                if (fl) {
-                    const MgkPt r = st[q];
-                    const float px = r.xh + r.xl, py = r.yh + r.yl;
-                    const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
-#pragma unroll
-                    for (int i = 0; i < 4; i++) {
-                        if (!((fl >> i) & 1u)) continue;
-#pragma unroll
-                        for (int j = 0; j < 4; j++) {
-                            const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 32 + tc * 4 + j],
-                                                         s_cyg[wr * 16 + tr * 4 + i]) < cut;
-                            const bool fi = ca[j] < rt[i];
-                            if (ex != fi) {
-                                const float t = __fmul_rn(ce[j], rv[i]);
-                                part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
-                                if (COUNT) inm ^= 1u << (i * 4 + j);
+                                for (int j = 0; j < 4; j++) {
+                                    const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 32 + tc * 4 + j],
+                                                                 s_cyg[wr * 16 + tr * 4 + i]) < cut;
+                                    const bool fi = ca[j] < rt[i];
+                                    if (ex != fi) {
+                                        const float t = __fmul_rn(ce[j], rv[i]);
+                                        part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
+                                        if (COUNT) inm ^= 1u << (i * 4 + j);
+                                    }
+                                }
                             }
                         }
                     }
+                    if (COUNT) cnt += __popc(inm & valid);
                 }
-            }
-            if (COUNT) cnt += __popc(inm & valid);
-            }
-            pc++;
-            if ((pc & 7u) == 0) {
+                pc++;
+                if ((pc & 7u) == 0) {
 #pragma unroll
-                for (int k = 0; k < 16; k++) {
-                    float2 a = kah[k * kThreads + tid];
-                    kahan_add(a.x, a.y, part[k]);
-                    kah[k * kThreads + tid] = a;
-                    part[k] = 0.0f;
+                    for (int k = 0; k < 16; k++) {
+                        float2 a = kah[k * kThreads + tid];
+                        kahan_add(a.x, a.y, part[k]);
+                        kah[k * kThreads + tid] = a;
+                        part[k] = 0.0f;
+                    }
                 }
             }
         }
