@@ -243,19 +243,22 @@ __device__ __forceinline__ int next_batch(const DParams& P, const BlockGeom& G, 
 
 // Dynamic shared memory of k_density (bytes); factor tables are padded to a
 // row stride of 72 float2 so that phase-A stores of 4 points hit distinct banks.
-constexpr int kFStride = 72;
+constexpr int kFStride = 72;  // floats; 72 = 8 (mod 32): phase-A stores of 4 points hit 32 banks
 constexpr size_t kSmemStage = 2 * kMB * sizeof(MgkPt);
-constexpr size_t kSmemTab = (size_t)kMB * kFStride * sizeof(float2);
-constexpr size_t kSmemKahan = 16 * kThreads * sizeof(float2);
-constexpr size_t kDensitySmem = kSmemStage + 2 * kSmemTab + kSmemKahan;
+constexpr size_t kSmemTab = (size_t)kMB * kFStride * sizeof(float);
+constexpr size_t kDensitySmem = kSmemStage + 3 * kSmemTab;
+
+#ifndef MGK_DENSITY_MIN_CTAS
+#define MGK_DENSITY_MIN_CTAS 3  // resident CTAs per SM the register budget is sized for
+#endif
 
 template <bool VARH, bool COUNT>
-__global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
+__global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DParams P) {
     extern __shared__ __align__(128) unsigned char dsm[];
     MgkPt* stage = reinterpret_cast<MgkPt*>(dsm);                                  // [2][kMB]
-    float2* colf = reinterpret_cast<float2*>(dsm + kSmemStage);                    // [kMB][kFStride] (a_hi, E)
-    float2* rowf = reinterpret_cast<float2*>(dsm + kSmemStage + kSmemTab);         // [kMB][kFStride] (T, F)
-    float2* kah = reinterpret_cast<float2*>(dsm + kSmemStage + 2 * kSmemTab);     // [16][kThreads] Kahan (s, c)
+    float* colE = reinterpret_cast<float*>(dsm + kSmemStage);                 // [kMB][kFStride] E_j = 2^-a_j
+    float* rowF = reinterpret_cast<float*>(dsm + kSmemStage + kSmemTab);      // [kMB][kFStride] F_i = w e 2^-b_i
+    float* rowG = reinterpret_cast<float*>(dsm + kSmemStage + 2 * kSmemTab);  // [kMB][kFStride] G_i = 2^-T_i
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ __align__(16) unsigned long long rowflag[kMB][2];  // per column half: 64 row bits
     __shared__ unsigned char procmask[kMB];  // warp w processes the point
@@ -288,8 +291,6 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
         fence_mbar_init();
         s_abort = 0;
     }
-#pragma unroll
-    for (int k = 0; k < 16; k++) kah[k * kThreads + tid] = make_float2(0.0f, 0.0f);
     regular = __syncthreads_and(regular);
     const float inv_cs = 1.0f / (float)P.cs;
 
@@ -305,9 +306,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
             valid |= (unsigned)v << (i * 4 + j);
         }
 
-    float part[16];
+    float part[16], acc_s[16], acc_c[16];
 #pragma unroll
-    for (int k = 0; k < 16; k++) part[k] = 0.0f;
+    for (int k = 0; k < 16; k++) part[k] = acc_s[k] = acc_c[k] = 0.0f;
     unsigned long long cnt = 0;
     unsigned pc = 0;  // points processed by this warp (warp-uniform)
 
@@ -374,14 +375,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                     cutf = P.cutf;
                     epsd2 = P.epsd2;
                 }
-                float2* crow = colf + qa * kFStride;
-                float2* rrow = rowf + qa * kFStride;
+                float* cE = colE + qa * kFStride;
+                float* rF = rowF + qa * kFStride;
+                float* rG = rowG + qa * kFStride;
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
                     const int j = ka + 8 * c;
                     float ah, al, d2;
                     exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                    crow[j] = make_float2(ah, exp2_pair(ah, al));
+                    cE[j] = exp2_pair(ah, al);
                 }
                 const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
 #pragma unroll
@@ -390,7 +392,9 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                     float bh, bl, d2;
                     exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
                     const float T = __fadd_rn(__fsub_rn(P.cutlh, bh), __fsub_rn(P.cutll, bl));
-                    rrow[i] = make_float2(T, __fmul_rn(r.wk, exp2_pair(bh, bl)));
+                    rF[i] = __fmul_rn(r.wk, exp2_pair(bh, bl));
+                    // a_j < T_i  <=>  E_j > G_i (2^-x is decreasing); G = inf for rows off the disc
+                    rG[i] = mgk_ex2(-T);
                     const float s2 = cutf - d2;
                     const unsigned a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2 ? 3u : 0u);
                     const unsigned sh = (ka + 8 * c) & 31;
@@ -449,14 +453,12 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
             while (todo) {
                 const int q = __ffs(todo) - 1;
                 todo &= todo - 1u;
-                const float2* crow = colf + q * kFStride + wc * 32 + tc * 4;
-                const float2* rrow = rowf + q * kFStride + wr * 16 + tr * 4;
-                const float4 c01 = *reinterpret_cast<const float4*>(crow);
-                const float4 c23 = *reinterpret_cast<const float4*>(crow + 2);
-                const float4 r01 = *reinterpret_cast<const float4*>(rrow);
-                const float4 r23 = *reinterpret_cast<const float4*>(rrow + 2);
-                const float ca[4] = {c01.x, c01.z, c23.x, c23.z}, ce[4] = {c01.y, c01.w, c23.y, c23.w};
-                const float rt[4] = {r01.x, r01.z, r23.x, r23.z}, rv[4] = {r01.y, r01.w, r23.y, r23.w};
+                const float* pE = colE + q * kFStride + wc * 32 + tc * 4;
+                const float* pF = rowF + q * kFStride + wr * 16 + tr * 4;
+                const float4 e4 = *reinterpret_cast<const float4*>(pE);
+                const float4 f4 = *reinterpret_cast<const float4*>(pF);
+                const float ce[4] = {e4.x, e4.y, e4.z, e4.w};
+                const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
                 if (!COUNT && ((fullb >> q) & 1u)) {
                     // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
@@ -464,13 +466,15 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
 #pragma unroll
                         for (int j = 0; j < 4; j++) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
                 } else {
+                    const float4 g4 = *reinterpret_cast<const float4*>(rowG + q * kFStride + wr * 16 + tr * 4);
+                    const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
                     unsigned inm = 0;
                     if (COUNT) {
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
                             for (int j = 0; j < 4; j++) {
-                                const bool in = ca[j] < rt[i];
+                                const bool in = rg[i] < ce[j];
                                 if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
                                 inm |= (unsigned)in << (i * 4 + j);
                             }
@@ -478,7 +482,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
-                            for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], ca[j], rt[i], ce[j], rv[i]);
+                            for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], rg[i], ce[j], ce[j], rv[i]);
                     }
                     if ((ambb >> q) & 1u) {
                         // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
@@ -494,7 +498,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                                 for (int j = 0; j < 4; j++) {
                                     const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 32 + tc * 4 + j],
                                                                  s_cyg[wr * 16 + tr * 4 + i]) < cut;
-                                    const bool fi = ca[j] < rt[i];
+                                    const bool fi = rg[i] < ce[j];
                                     if (ex != fi) {
                                         const float t = __fmul_rn(ce[j], rv[i]);
                                         part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
@@ -510,9 +514,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
                 if ((pc & 7u) == 0) {
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
-                        float2 a = kah[k * kThreads + tid];
-                        kahan_add(a.x, a.y, part[k]);
-                        kah[k * kThreads + tid] = a;
+                        kahan_add(acc_s[k], acc_c[k], part[k]);
                         part[k] = 0.0f;
                     }
                 }
@@ -539,11 +541,10 @@ __global__ void __launch_bounds__(kThreads, 3) k_density(DParams P) {
 #pragma unroll
         for (int j = 0; j < 4; j++) {
             const int k = i * 4 + j;
-            float2 a = kah[k * kThreads + tid];
-            kahan_add(a.x, a.y, part[k]);
+            kahan_add(acc_s[k], acc_c[k], part[k]);
             const int r = wr * 16 + tr * 4 + i, c = wc * 32 + tc * 4 + j;
             if (r >= G.nrow || c >= G.ncol) continue;
-            const double v = ((double)a.x - (double)a.y) * norm;
+            const double v = ((double)acc_s[k] - (double)acc_c[k]) * norm;
             if (it.slot >= 0) {
                 P.scratch[(size_t)it.slot * (kBlk * kBlk) + r * kBlk + c] = v;
             } else {
