@@ -23,27 +23,64 @@ int mgk_cuda_fail(mgk_ctx* ctx, cudaError_t e, const char* what) {
                     std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Device memory of a context is cached: a freed block goes back to a pool
+// keyed by its size class and is handed out again to the next request of that
+// class, so a step that allocates and frees the same scratch every call
+// (index build, tile plans) does not pay cudaMalloc/cudaFree each time.  All
+// work of a context is ordered on its stream, so a block reused by a later
+// launch is only touched after the earlier launches that used it.  Pooled
+// bytes count against the HBM budget; when a request would exceed it the pool
+// is released first.
+static size_t size_class(size_t bytes) {
+    if (bytes <= 256) return 256;
+    if (bytes <= (1u << 20)) {
+        size_t c = 256;
+        while (c < bytes) c <<= 1;
+        return c;
+    }
+    const size_t g = 2u << 20;
+    return (bytes + g - 1) / g * g;
+}
+
+static void release_pool(mgk_ctx* ctx) {
+    for (auto& kv : ctx->pool) {
+        cudaFree(kv.second);
+        ctx->in_use -= std::min<uint64_t>(ctx->in_use, kv.first);
+    }
+    ctx->pool.clear();
+}
+
 int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes) {
     *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    if (ctx->in_use + bytes > ctx->budget)
+    const size_t cls = size_class(bytes ? bytes : 16);
+    auto it = ctx->pool.find(cls);
+    if (it != ctx->pool.end()) {
+        *p = it->second;
+        ctx->pool.erase(it);
+        return MGK_OK;
+    }
+    if (ctx->in_use + cls > ctx->budget && !ctx->pool.empty()) release_pool(ctx);
+    if (ctx->in_use + cls > ctx->budget)
         return mgk_fail(ctx, MGK_ERR_BUDGET,
-                        "HBM budget exceeded: need " + std::to_string(bytes) + " B, in use " +
+                        "HBM budget exceeded: need " + std::to_string(cls) + " B, in use " +
                             std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget));
-    cudaError_t e = cudaMalloc(p, bytes);
+    cudaError_t e = cudaMalloc(p, cls);
+    if (e == cudaErrorMemoryAllocation && !ctx->pool.empty()) {
+        (void)cudaGetLastError();
+        release_pool(ctx);
+        e = cudaMalloc(p, cls);
+    }
     if (e != cudaSuccess) {
         *p = nullptr;
         return mgk_cuda_fail(ctx, e, "cudaMalloc");
     }
-    ctx->in_use += bytes;
+    ctx->in_use += cls;
     return MGK_OK;
 }
 
 void mgk_free(mgk_ctx* ctx, void* p, size_t bytes) {
     if (!p) return;
-    if (bytes == 0) bytes = 16;
-    cudaFree(p);
-    ctx->in_use -= std::min<uint64_t>(ctx->in_use, bytes);
+    ctx->pool.emplace(size_class(bytes ? bytes : 16), p);
 }
 
 extern "C" {
@@ -103,6 +140,7 @@ int mgk_ctx_destroy(mgk_ctx* c) {
     if (!c) return MGK_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
+    release_pool(c);
     if (c->d_counter) cudaFree(c->d_counter);
     if (c->d_sum) cudaFree(c->d_sum);
     if (c->h_counter) cudaFreeHost(c->h_counter);
@@ -290,7 +328,8 @@ int mgk_raster_destroy(mgk_raster* r) {
     const size_t ncell = (size_t)r->g.ncols * (size_t)r->g.nrows;
     if (r->owns) mgk_free(c, r->mask, sizeof(float) * ncell);
     mgk_free(c, r->boundary, ncell);
-    mgk_free(c, r->bcells, sizeof(float2) * (size_t)r->nb);
+    mgk_free(c, r->bcells, sizeof(float2) * (size_t)std::max<int64_t>(r->nb, 1));
+    mgk_free(c, r->bstart, sizeof(int) * (size_t)(r->nbins + 1));
     delete r;
     return MGK_OK;
 }

@@ -6,74 +6,144 @@
 // dCalcDist2Boundary (kde_kernel_kdtr.cu:1285-1353) takes, per point, the
 // minimum squared distance to every boundary-cell centre; the CPU twin
 // (kde_cuda_kdtr_tiled.cu:4092-4133) keeps it in double, DBL_MAX when there is
-// no boundary cell.  The distance only gates the edge-correction short-circuit
+// no boundary cell.  The distance gates the edge-correction short-circuit
 // (weight 1 when dist2 >= 9 h^2), so it is computed exactly as the FP64 CPU
 // path does: the minimum of exactly rounded double d^2 values.
 //
 // Here the mask is read once: the boundary test and the compaction of the
-// boundary-cell centres happen in one pass; the distance kernel streams the
-// compacted centres through shared memory (one thread per point, FP64 math).
+// boundary-cell centres happen in one pass.  The centres are then binned on a
+// coarse grid (32 x 32 cells per bin) and each point searches rings of bins
+// outward from its own, stopping once the nearest ring not yet searched
+// cannot hold anything closer than the best distance found.  The minimum is
+// order independent, so the result is the brute-force minimum bit for bit.
+#include <algorithm>
 #include <cfloat>
 
 #include "mgk_internal.cuh"
 
 namespace {
 
+constexpr int kBinCells = 32;  // boundary bins are kBinCells x kBinCells mask cells
+
 __global__ void k_mark_boundary(mgk_grid g, const float* __restrict__ mask, uint8_t* __restrict__ out,
                                 float2* __restrict__ cells, unsigned long long* __restrict__ count) {
     const int64_t ncell = g.ncols * g.nrows;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell;
          i += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r = i / g.ncols, c = i - r * g.ncols;
-    const float nd = g.nodata;
-    uint8_t b = 0;
-    if (mask[i] != nd) {
-        if (r == 0 || r == g.nrows - 1 || c == 0 || c == g.ncols - 1) {
-            b = 1;
-        } else {
-            const float* up = mask + i - g.ncols;
-            const float* dn = mask + i + g.ncols;
-            b = (up[-1] == nd) | (up[0] == nd) | (up[1] == nd) | (mask[i - 1] == nd) | (mask[i + 1] == nd) |
-                (dn[-1] == nd) | (dn[0] == nd) | (dn[1] == nd);
+        const int64_t r = i / g.ncols, c = i - r * g.ncols;
+        const float nd = g.nodata;
+        uint8_t b = 0;
+        if (mask[i] != nd) {
+            if (r == 0 || r == g.nrows - 1 || c == 0 || c == g.ncols - 1) {
+                b = 1;
+            } else {
+                const float* up = mask + i - g.ncols;
+                const float* dn = mask + i + g.ncols;
+                b = (up[-1] == nd) | (up[0] == nd) | (up[1] == nd) | (mask[i - 1] == nd) | (mask[i + 1] == nd) |
+                    (dn[-1] == nd) | (dn[0] == nd) | (dn[1] == nd);
+            }
         }
-    }
-    out[i] = b;
-    if (b) {
-        const unsigned long long k = atomicAdd(count, 1ull);
-        cells[k] = make_float2(mgk_cell_x(g.xll, g.cs, c), mgk_cell_y(g.yll, g.cs, g.nrows, r));
-    }
+        out[i] = b;
+        if (b) {
+            const unsigned long long k = atomicAdd(count, 1ull);
+            cells[k] = make_float2(mgk_cell_x(g.xll, g.cs, c), mgk_cell_y(g.yll, g.cs, g.nrows, r));
+        }
     }
 }
 
-constexpr int kDistThreads = 256;
-constexpr int kDistChunk = 2048;
+struct BinGrid {
+    double x0, y0, side;  // lower-left corner of bin (0, 0), bin side in coordinates
+    int nbx, nby;
+};
 
-__global__ void __launch_bounds__(kDistThreads) k_dist2(int64_t n, const float* __restrict__ x,
-                                                        const float* __restrict__ y,
-                                                        const float2* __restrict__ cells, int64_t nb,
-                                                        double* __restrict__ out) {
-    __shared__ float2 sc[kDistChunk];
-    const int64_t i = blockIdx.x * (int64_t)kDistThreads + threadIdx.x;
-    const bool live = i < n;
-    const double px = live ? (double)x[i] : 0.0, py = live ? (double)y[i] : 0.0;
-    double best = DBL_MAX;
-    for (int64_t base = 0; base < nb; base += kDistChunk) {
-        const int m = (int)mgk_min64(kDistChunk, nb - base);
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+
+__device__ __forceinline__ void bin_of(const BinGrid& B, double x, double y, int& bx, int& by) {
+    const double fx = floor((x - B.x0) / B.side), fy = floor((y - B.y0) / B.side);
+    bx = clampi((int)fmax(fmin(fx, 1e9), -1e9), 0, B.nbx - 1);
+    by = clampi((int)fmax(fmin(fy, 1e9), -1e9), 0, B.nby - 1);
+}
+
+__global__ void k_bin_count(int64_t nb, const float2* __restrict__ cells, BinGrid B, int* __restrict__ cnt) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    int bx, by;
+    bin_of(B, cells[i].x, cells[i].y, bx, by);
+    atomicAdd(&cnt[by * B.nbx + bx], 1);
+}
+
+// exclusive scan of n ints in one CTA (n is the boundary-bin count, small)
+__global__ void __launch_bounds__(1024) k_scan_small(int* __restrict__ a, int n) {
+    __shared__ int part[1024];
+    const int t = threadIdx.x;
+    const int chunk = (n + 1023) / 1024;
+    const int b = t * chunk, e = min(n, b + chunk);
+    int s = 0;
+    for (int i = b; i < e; i++) s += a[i];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int v = t >= off ? part[t - off] : 0;
         __syncthreads();
-        for (int k = threadIdx.x; k < m; k += kDistThreads) sc[k] = cells[base + k];
+        part[t] += v;
         __syncthreads();
-        if (live) {
-#pragma unroll 4
-            for (int k = 0; k < m; k++) {
-                const float2 c = sc[k];
-                const double dx = __dsub_rn((double)c.x, px);
-                const double dy = __dsub_rn((double)c.y, py);
-                const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-                best = fmin(best, d2);
-            }
-        }
     }
-    if (live) out[i] = best;
+    int run = t ? part[t - 1] : 0;
+    for (int i = b; i < e; i++) {
+        const int v = a[i];
+        a[i] = run;
+        run += v;
+    }
+    if (t == 1023) a[n] = part[1023];
+}
+
+__global__ void k_bin_fill(int64_t nb, const float2* __restrict__ cells, BinGrid B, const int* __restrict__ start,
+                           int* __restrict__ cursor, float2* __restrict__ binned) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= nb) return;
+    int bx, by;
+    bin_of(B, cells[i].x, cells[i].y, bx, by);
+    const int k = by * B.nbx + bx;
+    binned[start[k] + atomicAdd(&cursor[k], 1)] = cells[i];
+}
+
+__device__ __forceinline__ void scan_bin(const float2* __restrict__ cells, const int* __restrict__ start, int k,
+                                         double px, double py, double& best) {
+    for (int j = start[k]; j < start[k + 1]; j++) {
+        const float2 c = cells[j];
+        const double dx = __dsub_rn((double)c.x, px);
+        const double dy = __dsub_rn((double)c.y, py);
+        best = fmin(best, __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+    }
+}
+
+__global__ void k_dist2_binned(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
+                               const float2* __restrict__ cells, const int* __restrict__ start, BinGrid B,
+                               double* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double px = x[i], py = y[i];
+    int bx0, by0;
+    bin_of(B, px, py, bx0, by0);
+    double best = DBL_MAX;
+    const int rmax = max(B.nbx, B.nby);
+    for (int r = 0; r <= rmax; r++) {
+        // ring r: bins at Chebyshev distance r from (bx0, by0)
+        const int ylo = by0 - r, yhi = by0 + r, xlo = bx0 - r, xhi = bx0 + r;
+        for (int bx = max(xlo, 0); bx <= min(xhi, B.nbx - 1); bx++) {
+            if (ylo >= 0) scan_bin(cells, start, ylo * B.nbx + bx, px, py, best);
+            if (r > 0 && yhi < B.nby) scan_bin(cells, start, yhi * B.nbx + bx, px, py, best);
+        }
+        for (int by = max(ylo + 1, 0); by <= min(yhi - 1, B.nby - 1); by++) {
+            if (r > 0 && xlo >= 0) scan_bin(cells, start, by * B.nbx + xlo, px, py, best);
+            if (r > 0 && xhi < B.nbx) scan_bin(cells, start, by * B.nbx + xhi, px, py, best);
+        }
+        // every bin beyond ring r is at least r full bins away from the point
+        // (the margin covers rounding in the bin assignment)
+        const double lb = (double)r * B.side * (1.0 - 1e-9);
+        if (best <= lb * lb) break;
+    }
+    out[i] = best;
 }
 
 }  // namespace
@@ -84,7 +154,6 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     const size_t ncell = (size_t)g.ncols * (size_t)g.nrows;
     int st;
     if (!r->boundary && (st = mgk_alloc(ctx, (void**)&r->boundary, ncell))) return st;
-    // Worst-case list size, trimmed after counting.
     float2* cells = nullptr;
     if ((st = mgk_alloc(ctx, (void**)&cells, sizeof(float2) * ncell))) return st;
     MGK_CHECK_CUDA(ctx, cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned long long), s));
@@ -95,17 +164,36 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     unsigned long long nb = 0;
     MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&nb, ctx->d_counter, sizeof(nb), cudaMemcpyDeviceToHost, s));
     MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-    if (r->bcells) mgk_free(ctx, r->bcells, sizeof(float2) * (size_t)r->nb);
+    if (r->bcells) mgk_free(ctx, r->bcells, sizeof(float2) * (size_t)std::max<int64_t>(r->nb, 1));
+    if (r->bstart) mgk_free(ctx, r->bstart, sizeof(int) * (size_t)(r->nbins + 1));
     r->bcells = nullptr;
+    r->bstart = nullptr;
     r->nb = (int64_t)nb;
-    if (nb > 0) {
-        if ((st = mgk_alloc(ctx, (void**)&r->bcells, sizeof(float2) * nb))) {
-            mgk_free(ctx, cells, sizeof(float2) * ncell);
-            return st;
-        }
-        MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(r->bcells, cells, sizeof(float2) * nb, cudaMemcpyDeviceToDevice, s));
-        MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    // bins of kBinCells x kBinCells mask cells over the mask extent
+    r->bnx = (int)((g.ncols + kBinCells - 1) / kBinCells);
+    r->bny = (int)((g.nrows + kBinCells - 1) / kBinCells);
+    r->nbins = (int64_t)r->bnx * r->bny;
+    const size_t b_cells = sizeof(float2) * (size_t)std::max<uint64_t>(nb, 1);
+    const size_t b_start = sizeof(int) * (size_t)(r->nbins + 1);
+    int* cursor = nullptr;
+    if ((st = mgk_alloc(ctx, (void**)&r->bcells, b_cells)) || (st = mgk_alloc(ctx, (void**)&r->bstart, b_start)) ||
+        (st = mgk_alloc(ctx, (void**)&cursor, b_start))) {
+        mgk_free(ctx, cells, sizeof(float2) * ncell);
+        return st;
     }
+    BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->bstart, 0, b_start, s));
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(cursor, 0, b_start, s));
+    if (nb > 0) {
+        const unsigned gb = (unsigned)((nb + 255) / 256);
+        k_bin_count<<<gb, 256, 0, s>>>((int64_t)nb, cells, B, r->bstart);
+        k_scan_small<<<1, 1024, 0, s>>>(r->bstart, (int)r->nbins);
+        k_bin_fill<<<gb, 256, 0, s>>>((int64_t)nb, cells, B, r->bstart, cursor, r->bcells);
+        MGK_CHECK_LAUNCH(ctx, "boundary bins");
+        MGK_COUNT_LAUNCH(ctx, 3);
+    }
+    MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    mgk_free(ctx, cursor, b_start);
     mgk_free(ctx, cells, sizeof(float2) * ncell);
     r->marked = true;
     return MGK_OK;
@@ -113,9 +201,11 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
 
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {
     if (p->n == 0) return MGK_OK;
-    k_dist2<<<(unsigned)((p->n + kDistThreads - 1) / kDistThreads), kDistThreads, 0, ctx->stream>>>(
-        p->n, p->x, p->y, r->bcells, r->nb, p->dist2);
-    MGK_CHECK_LAUNCH(ctx, "k_dist2");
+    const mgk_grid& g = r->g;
+    BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};
+    k_dist2_binned<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(p->n, p->x, p->y, r->bcells, r->bstart,
+                                                                          B, p->dist2);
+    MGK_CHECK_LAUNCH(ctx, "k_dist2_binned");
     MGK_COUNT_LAUNCH(ctx, 1);
     return MGK_OK;
 }

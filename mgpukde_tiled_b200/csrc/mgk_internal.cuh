@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <string>
 
 #include "../../include/mgk.h"
@@ -33,6 +34,7 @@ struct mgk_ctx {
     unsigned long long* h_counter = nullptr;  // pinned mirror
     double* d_sum = nullptr;                  // 256 doubles
     double* h_sum = nullptr;                  // pinned mirror
+    std::multimap<size_t, void*> pool;        // cached device blocks by size class
     uint64_t launches = 0;                    // kernels launched by this context
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     float last_density_ms = 0.0f;
@@ -57,7 +59,10 @@ struct mgk_raster {
     float* mask = nullptr;
     bool owns = false;
     uint8_t* boundary = nullptr;  // per cell
-    float2* bcells = nullptr;     // boundary-cell centres (compacted)
+    float2* bcells = nullptr;     // boundary-cell centres, binned
+    int* bstart = nullptr;        // bin offsets into bcells (nbins + 1)
+    int bnx = 0, bny = 0;         // boundary bins per row / column
+    int64_t nbins = 0;
     int64_t nb = 0;
     bool marked = false;
 };

@@ -142,9 +142,10 @@ class Points:
         return d, e
 
     def close(self):
-        if self._h:
+        # objects are destroyed before their context (the context owns the memory pool)
+        if self._h and self.ctx.handle:
             lib().mgk_points_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -180,9 +181,9 @@ class Raster:
         return out
 
     def close(self):
-        if self._h:
+        if self._h and self.ctx.handle:
             lib().mgk_raster_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -200,9 +201,9 @@ class Index:
         ctx.check(lib().mgk_index_build(ctx.handle, points._h, float(h), float(bin_size), C.byref(self._h)))
 
     def close(self):
-        if self._h:
+        if self._h and self.ctx.handle:
             lib().mgk_index_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
