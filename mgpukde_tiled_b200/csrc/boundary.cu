@@ -117,9 +117,33 @@ __device__ __forceinline__ void scan_bin(const float2* __restrict__ cells, const
     }
 }
 
+// Per bin: the smallest ring index (Chebyshev distance in bins) holding a
+// non-empty bin; rings inside it are empty and are skipped by the search.
+__global__ void k_bin_near(const int* __restrict__ start, BinGrid B, int* __restrict__ near) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B.nbx * B.nby) return;
+    const int bx0 = k % B.nbx, by0 = k / B.nbx;
+    const int rmax = max(B.nbx, B.nby);
+    int found = rmax + 1;
+    for (int r = 0; r <= rmax && found > rmax; r++) {
+        for (int by = max(by0 - r, 0); by <= min(by0 + r, B.nby - 1) && found > rmax; by++) {
+            const bool edge_row = (by == by0 - r) || (by == by0 + r);
+            for (int bx = max(bx0 - r, 0); bx <= min(bx0 + r, B.nbx - 1); bx++) {
+                if (!edge_row && bx != bx0 - r && bx != bx0 + r) continue;
+                const int kk = by * B.nbx + bx;
+                if (start[kk + 1] > start[kk]) {
+                    found = r;
+                    break;
+                }
+            }
+        }
+    }
+    near[k] = found;
+}
+
 __global__ void k_dist2_binned(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
-                               const float2* __restrict__ cells, const int* __restrict__ start, BinGrid B,
-                               double* __restrict__ out) {
+                               const float2* __restrict__ cells, const int* __restrict__ start,
+                               const int* __restrict__ near, BinGrid B, double* __restrict__ out) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
     const double px = x[i], py = y[i];
@@ -127,7 +151,7 @@ __global__ void k_dist2_binned(int64_t n, const float* __restrict__ x, const flo
     bin_of(B, px, py, bx0, by0);
     double best = DBL_MAX;
     const int rmax = max(B.nbx, B.nby);
-    for (int r = 0; r <= rmax; r++) {
+    for (int r = near[by0 * B.nbx + bx0]; r <= rmax; r++) {
         // ring r: bins at Chebyshev distance r from (bx0, by0)
         const int ylo = by0 - r, yhi = by0 + r, xlo = bx0 - r, xhi = bx0 + r;
         for (int bx = max(xlo, 0); bx <= min(xhi, B.nbx - 1); bx++) {
@@ -192,8 +216,14 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
         MGK_CHECK_LAUNCH(ctx, "boundary bins");
         MGK_COUNT_LAUNCH(ctx, 3);
     }
+    // cursor (nbins + 1 ints) is reused as the nearest-ring table
+    k_bin_near<<<(unsigned)((r->nbins + 255) / 256), 256, 0, s>>>(r->bstart, B, cursor);
+    MGK_CHECK_LAUNCH(ctx, "k_bin_near");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    if (r->bnear) mgk_free(ctx, r->bnear, b_start);
+    r->bnear = cursor;
+    cursor = nullptr;
     MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-    mgk_free(ctx, cursor, b_start);
     mgk_free(ctx, cells, sizeof(float2) * ncell);
     r->marked = true;
     return MGK_OK;
@@ -204,7 +234,7 @@ int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {
     const mgk_grid& g = r->g;
     BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};
     k_dist2_binned<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(p->n, p->x, p->y, r->bcells, r->bstart,
-                                                                          B, p->dist2);
+                                                                          r->bnear, B, p->dist2);
     MGK_CHECK_LAUNCH(ctx, "k_dist2_binned");
     MGK_COUNT_LAUNCH(ctx, 1);
     return MGK_OK;

@@ -61,6 +61,7 @@ struct mgk_raster {
     uint8_t* boundary = nullptr;  // per cell
     float2* bcells = nullptr;     // boundary-cell centres, binned
     int* bstart = nullptr;        // bin offsets into bcells (nbins + 1)
+    int* bnear = nullptr;         // per bin: first ring index holding a non-empty bin
     int bnx = 0, bny = 0;         // boundary bins per row / column
     int64_t nbins = 0;
     int64_t nb = 0;
