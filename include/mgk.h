@@ -166,6 +166,23 @@ int mgk_density_tile_fp64(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g,
                           int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,
                           float* d_out, int64_t* evals);
 
+/* Same density as mgk_density_tile, for callers that cannot let the library
+ * allocate device memory at call time (an application that reserves the GPU's
+ * memory up front for its own allocator, or a running latency-critical loop
+ * in which cudaMalloc/cudaFree, which may synchronise the device, are not
+ * allowed).  It calls no cudaMalloc, cudaFree or other allocating routine:
+ * its scratch (block counts, work items, FP64 partial sums of split blocks)
+ * lives in one fixed file-scope device array of about 12.4 MiB that every GPU
+ * loading the library holds until the process exits.  Limit: tiles of at most
+ * 4096 x 4096 cells (MGK_ERR_INVALID beyond).  The first call on a device looks
+ * up that array's device address (once per device); make that first call
+ * before any stream capture.  All calls share the one array: calls that
+ * overlap on the GPU (other streams, other threads) race and must be
+ * serialised by the caller.  No counterpart in the reference. */
+int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
+                             int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,
+                             float* d_out);
+
 /* ---- bandwidth selection ---------------------------------------------- */
 
 /* Batched LogLikelihood (kde_cuda_kdtr_tiled.cu:3214-3299) over nh fixed

@@ -24,7 +24,7 @@ EXPORTS = [
     "mgk_points_download", "mgk_raster_upload", "mgk_raster_wrap", "mgk_raster_destroy",
     "mgk_mark_boundary", "mgk_raster_boundary_download", "mgk_boundary_dist",
     "mgk_edge_weights", "mgk_edge_weights_unit", "mgk_index_build", "mgk_index_destroy",
-    "mgk_density_tile", "mgk_density_tile_fp64", "mgk_loo_loglik_batch",
+    "mgk_density_tile", "mgk_density_tile_fp64", "mgk_density_tile_noalloc", "mgk_loo_loglik_batch",
     "mgk_mle_fixed_bandwidth", "mgk_rule_of_thumb", "mgk_kde_raster",
 ]
 
@@ -81,6 +81,7 @@ def lib():
         "mgk_index_destroy": (I, [P]),
         "mgk_density_tile": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
         "mgk_density_tile_fp64": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
+        "mgk_density_tile_noalloc": (I, [P, P, G, I64, I64, I64, I64, P, P]),
         "mgk_loo_loglik_batch": (I, [P, P, P, P, I, P, C.POINTER(I)]),
         "mgk_mle_fixed_bandwidth": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(I)]),
         "mgk_rule_of_thumb": (C.c_float, [I64, P, P, P]),

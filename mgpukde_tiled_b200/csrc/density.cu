@@ -35,6 +35,7 @@
 // reproducible.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include <vector>
 
 #include "mgk_internal.cuh"
@@ -800,4 +801,185 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         mgk_free(ctx, d_sbeg, b_sbeg);
     }
     return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Density of one tile without allocating anything.
+//
+// mgk_density_tile takes its scratch (the per-block candidate counts, the
+// work-item list and the FP64 partial sums of blocks split across CTAs) from
+// the context's device allocator.  Some callers cannot let a library allocate
+// device memory at that point: an application that reserves the GPU's memory
+// up front for its own allocator or arena, or a latency-critical loop that
+// forbids cudaMalloc/cudaFree (which may synchronise the whole device) once it
+// is running.  For them this variant keeps all scratch in one fixed
+// file-scope device array, g_density_scratch (kNaScratchBytes, about 12.4 MiB),
+// which every GPU that loads the library holds until the process exits, and
+// its host-side plan in fixed static arrays.  Limits: a tile of at most 4096 x
+// 4096 cells (64 x 64 blocks of 64 x 64) and at most kNaMaxSlots split work
+// items (heavy blocks get larger work items instead).  Inputs (index, mask) and
+// the output tile are the caller's as for mgk_density_tile.
+namespace {
+
+constexpr int kNaMaxBlocks = 4096;
+constexpr int kNaMaxItems = 12288;
+constexpr int kNaMaxSlots = 384;
+constexpr size_t kNaSlotBytes = sizeof(double) * kBlk * kBlk;
+constexpr size_t na_round(size_t v) { return (v + 255) / 256 * 256; }
+constexpr size_t kNaOffCounts = 0;
+constexpr size_t kNaOffItems = na_round(kNaOffCounts + sizeof(int64_t) * kNaMaxBlocks);
+constexpr size_t kNaOffSplit = na_round(kNaOffItems + sizeof(Item) * kNaMaxItems);
+constexpr size_t kNaOffSplitBegin = na_round(kNaOffSplit + sizeof(int32_t) * kNaMaxSlots);
+constexpr size_t kNaOffSlots = na_round(kNaOffSplitBegin + sizeof(int32_t) * (kNaMaxSlots + 1));
+constexpr size_t kNaScratchBytes = kNaOffSlots + kNaSlotBytes * kNaMaxSlots;
+
+static __device__ __align__(256) unsigned char g_density_scratch[kNaScratchBytes];
+
+constexpr int kNaMaxDevices = 64;
+unsigned char* g_na_addr[kNaMaxDevices];  // device address of g_density_scratch, per device
+std::mutex g_na_mu;                       // guards g_na_addr and the static host plan below
+int64_t g_na_counts[kNaMaxBlocks];
+Item g_na_items[kNaMaxItems];
+int32_t g_na_split[kNaMaxSlots];
+int32_t g_na_split_begin[kNaMaxSlots + 1];
+
+}  // namespace
+
+extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
+                                        int64_t col0, int64_t nr, int64_t nc, const float* d_mask, float* d_out) {
+    if (!ctx || !idx || !g || !d_out || !(g->cs > 0.0f) || g->ncols <= 0 || g->nrows <= 0)
+        return mgk_fail(ctx, MGK_ERR_INVALID, "density_tile_noalloc: bad arguments");
+    if (row0 < 0 || col0 < 0 || nr < 0 || nc < 0 || row0 + nr > g->nrows || col0 + nc > g->ncols)
+        return mgk_fail(ctx, MGK_ERR_INVALID, "density_tile_noalloc: tile outside the raster");
+    if (nr == 0 || nc == 0) return MGK_OK;
+    const int nbx_t = (int)((nc + kBlk - 1) / kBlk), nby_t = (int)((nr + kBlk - 1) / kBlk);
+    const int nblk = nbx_t * nby_t;
+    if (nblk > kNaMaxBlocks)
+        return mgk_fail(ctx, MGK_ERR_INVALID,
+                        "density_tile_noalloc: tile of " + std::to_string(nr) + " x " + std::to_string(nc) +
+                            " cells exceeds the fixed scratch (at most 4096 x 4096 cells)");
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (ctx->device < 0 || ctx->device >= kNaMaxDevices)
+        return mgk_fail(ctx, MGK_ERR_INVALID, "density_tile_noalloc: device index out of range");
+    // set-up, once per device, with that device current: the host-side name of
+    // a __device__ array is not its device address, so look the address up
+    if (!g_na_addr[ctx->device]) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (cur != ctx->device) cudaSetDevice(ctx->device);
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_density_scratch);
+        if (cur != ctx->device && cur >= 0) cudaSetDevice(cur);
+        if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "cudaGetSymbolAddress(g_density_scratch)");
+        g_na_addr[ctx->device] = static_cast<unsigned char*>(p);
+    }
+    unsigned char* base = g_na_addr[ctx->device];
+    int64_t* d_counts = reinterpret_cast<int64_t*>(base + kNaOffCounts);
+    Item* d_items = reinterpret_cast<Item*>(base + kNaOffItems);
+    int32_t* d_sb = reinterpret_cast<int32_t*>(base + kNaOffSplit);
+    int32_t* d_sbeg = reinterpret_cast<int32_t*>(base + kNaOffSplitBegin);
+    cudaStream_t s = ctx->stream;
+
+    DParams P{};
+    P.xll = g->xll;
+    P.yll = g->yll;
+    P.cs = g->cs;
+    P.g_nrows = g->nrows;
+    P.row0 = row0;
+    P.col0 = col0;
+    P.nr = nr;
+    P.nc = nc;
+    P.nodata = g->nodata;
+    P.mask = d_mask;
+    P.out = d_out;
+    P.pts = idx->pts;
+    P.bin_start = idx->bin_start;
+    P.ox = idx->ox;
+    P.oy = idx->oy;
+    P.inv_side = 1.0 / idx->side;
+    P.nbx = idx->nbx;
+    P.nby = idx->nby;
+    P.qexp = idx->qexp;
+    P.h2 = idx->h2;
+    P.k0 = idx->k0;
+    P.cut_d2 = idx->cut_d2;
+    P.reach = idx->reach;
+    {
+        const double k2 = idx->k2;
+        P.k2h = (float)k2;
+        P.k2l = (float)(k2 - (double)P.k2h);
+        const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
+        P.cutlh = (float)cutl;
+        P.cutll = (float)(cutl - (double)P.cutlh);
+        P.cutf = (float)idx->cut_d2;
+        P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
+    }
+    P.evals = nullptr;
+    P.err = ctx->d_counter + 7;
+    P.scratch = reinterpret_cast<double*>(base + kNaOffSlots);
+
+    // plan: candidates per block (device) -> work items (host, static arrays)
+    k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, d_counts);
+    cudaError_t ce = cudaMemsetAsync(P.err, 0, sizeof(unsigned long long), s);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(g_na_counts, d_counts, sizeof(int64_t) * nblk, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc plan");
+    int64_t total = 0;
+    for (int b = 0; b < nblk; b++) total += g_na_counts[b];
+    const int64_t slots_resident = (int64_t)ctx->sm_count * MGK_DENSITY_MIN_CTAS;
+    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
+    K = (K + kMB - 1) / kMB * kMB;
+    for (;;) {  // grow the item size until the split items fit the fixed slots
+        int64_t need = 0;
+        for (int b = 0; b < nblk; b++)
+            if (g_na_counts[b] > K) need += (g_na_counts[b] + K - 1) / K;
+        if (need <= kNaMaxSlots) break;
+        K *= 2;
+    }
+    int nitems = 0, nsplit = 0;
+    int32_t nslots = 0;
+    for (int b = 0; b < nblk; b++) {
+        const int64_t c = g_na_counts[b];
+        const int bxi = b % nbx_t, byi = b / nbx_t;
+        if (c <= K) {
+            g_na_items[nitems++] = {bxi, byi, 0, (int32_t)c, -1, 0};
+        } else {
+            g_na_split[nsplit] = b;
+            g_na_split_begin[nsplit++] = nslots;
+            for (int64_t k = 0; k < c; k += K)
+                g_na_items[nitems++] = {bxi, byi, (int32_t)k, (int32_t)std::min<int64_t>(c, k + K), nslots++, 0};
+        }
+    }
+    g_na_split_begin[nsplit] = nslots;
+    // heaviest items first; ties keep block order (std::sort allocates nothing)
+    for (int i = 0; i < nitems; i++) g_na_items[i].pad = i;
+    std::sort(g_na_items, g_na_items + nitems, [](const Item& a, const Item& b) {
+        const int32_t ca = a.k1 - a.k0, cb = b.k1 - b.k0;
+        return ca != cb ? ca > cb : a.pad < b.pad;
+    });
+    ce = cudaMemcpyAsync(d_items, g_na_items, sizeof(Item) * nitems, cudaMemcpyHostToDevice, s);
+    if (ce == cudaSuccess && nsplit) {
+        ce = cudaMemcpyAsync(d_sb, g_na_split, sizeof(int32_t) * nsplit, cudaMemcpyHostToDevice, s);
+        if (ce == cudaSuccess)
+            ce = cudaMemcpyAsync(d_sbeg, g_na_split_begin, sizeof(int32_t) * (nsplit + 1), cudaMemcpyHostToDevice, s);
+    }
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc upload");
+    P.items = d_items;
+    if (idx->varh) launch_density<true, false>((unsigned)nitems, s, P);
+    else launch_density<false, false>((unsigned)nitems, s, P);
+    if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc");
+    MGK_COUNT_LAUNCH(ctx, 2);
+    if (nsplit) {
+        k_merge<<<(unsigned)nsplit, 256, 0, s>>>(P, d_sb, d_sbeg, nbx_t);
+        if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc merge");
+        MGK_COUNT_LAUNCH(ctx, 1);
+    }
+    // the static host plan is reused by the next call: finish this one first
+    unsigned long long err = 0;
+    ce = cudaMemcpyAsync(&err, P.err, sizeof(err), cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc");
+    if (err) return mgk_fail(ctx, MGK_ERR_TIMEOUT, "density_tile_noalloc: a shared-memory staging wait timed out");
+    return MGK_OK;
 }
