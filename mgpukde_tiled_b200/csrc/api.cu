@@ -331,6 +331,9 @@ int mgk_raster_destroy(mgk_raster* r) {
     mgk_free(c, r->bcells, sizeof(float2) * (size_t)std::max<int64_t>(r->nb, 1));
     mgk_free(c, r->bstart, sizeof(int) * (size_t)(r->nbins + 1));
     mgk_free(c, r->bnear, sizeof(int) * (size_t)(r->nbins + 1));
+    mgk_free(c, r->bub, sizeof(double) * (size_t)r->nbins);
+    mgk_free(c, r->cstart, sizeof(int) * (size_t)(r->nbins + 1));
+    mgk_free(c, r->cand, sizeof(float2) * (size_t)std::max<int64_t>(r->ncand, 1));
     delete r;
     return MGK_OK;
 }

@@ -170,6 +170,116 @@ __global__ void k_dist2_binned(int64_t n, const float* __restrict__ x, const flo
     out[i] = best;
 }
 
+// ---- per-bin candidate lists ------------------------------------------------
+// For a point p inside bin b (rectangle R), the nearest boundary cell c* obeys
+// d(p, c*) <= UB_b = min_c maxdist(R, c) (the farthest corner of R from the
+// best cell), so c* is among the cells with mindist(R, c) <= UB_b.  Each bin
+// gets that candidate list once; its points then scan only the list.
+
+__device__ __forceinline__ void bin_rect(const BinGrid& B, int bx, int by, double& x0, double& y0, double& x1,
+                                         double& y1) {
+    x0 = B.x0 + bx * B.side;
+    y0 = B.y0 + by * B.side;
+    x1 = x0 + B.side;
+    y1 = y0 + B.side;
+}
+
+__device__ __forceinline__ double mind2(double x0, double y0, double x1, double y1, double cx, double cy) {
+    const double dx = fmax(0.0, fmax(x0 - cx, cx - x1)), dy = fmax(0.0, fmax(y0 - cy, cy - y1));
+    return dx * dx + dy * dy;
+}
+
+__device__ __forceinline__ double maxd2(double x0, double y0, double x1, double y1, double cx, double cy) {
+    const double dx = fmax(fabs(cx - x0), fabs(cx - x1)), dy = fmax(fabs(cy - y0), fabs(cy - y1));
+    return dx * dx + dy * dy;
+}
+
+// mode 0: UB per bin; mode 1: candidate count per bin; mode 2: fill the lists
+template <int MODE>
+__global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restrict__ start,
+                            const int* __restrict__ near, BinGrid B, double* __restrict__ ub,
+                            int* __restrict__ cnt, const int* __restrict__ cstart, float2* __restrict__ cand) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= B.nbx * B.nby) return;
+    const int bx0 = k % B.nbx, by0 = k / B.nbx;
+    double x0, y0, x1, y1;
+    bin_rect(B, bx0, by0, x0, y0, x1, y1);
+    // widen the rectangle a little: a point assigned to this bin by a rounded
+    // floor() may sit a hair outside it, and the lists must stay supersets
+    const double widen = 1e-6 * B.side;
+    x0 -= widen;
+    y0 -= widen;
+    x1 += widen;
+    y1 += widen;
+    const int rmax = max(B.nbx, B.nby);
+    double lim = MODE == 0 ? DBL_MAX : ub[k] * (1.0 + 1e-9);
+    int n = 0;
+    const int base = MODE == 2 ? cstart[k] : 0;
+    for (int r = near[k]; r <= rmax; r++) {
+        // cells in ring r are at least (r - 1) bins away from the rectangle
+        const double lb = (double)(r > 0 ? r - 1 : 0) * B.side * (1.0 - 1e-9);
+        if (lb * lb > lim) break;
+        for (int by = max(by0 - r, 0); by <= min(by0 + r, B.nby - 1); by++) {
+            const bool edge_row = (by == by0 - r) || (by == by0 + r);
+            for (int bx = max(bx0 - r, 0); bx <= min(bx0 + r, B.nbx - 1); bx++) {
+                if (!edge_row && bx != bx0 - r && bx != bx0 + r) continue;
+                const int kk = by * B.nbx + bx;
+                for (int j = start[kk]; j < start[kk + 1]; j++) {
+                    const double cx = cells[j].x, cy = cells[j].y;
+                    if (MODE == 0) {
+                        lim = fmin(lim, maxd2(x0, y0, x1, y1, cx, cy));
+                    } else if (mind2(x0, y0, x1, y1, cx, cy) <= lim) {
+                        if (MODE == 2) cand[base + n] = cells[j];
+                        n++;
+                    }
+                }
+            }
+        }
+    }
+    if (MODE == 0) ub[k] = lim;
+    if (MODE == 1) cnt[k] = n;
+}
+
+__global__ void k_dist2_cands(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
+                              const float2* __restrict__ cells, const int* __restrict__ start,
+                              const int* __restrict__ near, const float2* __restrict__ cand,
+                              const int* __restrict__ cstart, BinGrid B, double* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double px = x[i], py = y[i];
+    double best = DBL_MAX;
+    const double fx = floor((px - B.x0) / B.side), fy = floor((py - B.y0) / B.side);
+    if (fx >= 0.0 && fy >= 0.0 && fx < (double)B.nbx && fy < (double)B.nby) {
+        const int k = (int)fy * B.nbx + (int)fx;
+        for (int j = cstart[k]; j < cstart[k + 1]; j++) {
+            const float2 c = cand[j];
+            const double dx = __dsub_rn((double)c.x, px);
+            const double dy = __dsub_rn((double)c.y, py);
+            best = fmin(best, __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)));
+        }
+        out[i] = best;
+        return;
+    }
+    // outside the bin grid: ring search from the nearest bin
+    int bx0, by0;
+    bin_of(B, px, py, bx0, by0);
+    const int rmax = max(B.nbx, B.nby);
+    for (int r = near[by0 * B.nbx + bx0]; r <= rmax; r++) {
+        const int ylo = by0 - r, yhi = by0 + r, xlo = bx0 - r, xhi = bx0 + r;
+        for (int bx = max(xlo, 0); bx <= min(xhi, B.nbx - 1); bx++) {
+            if (ylo >= 0) scan_bin(cells, start, ylo * B.nbx + bx, px, py, best);
+            if (r > 0 && yhi < B.nby) scan_bin(cells, start, yhi * B.nbx + bx, px, py, best);
+        }
+        for (int by = max(ylo + 1, 0); by <= min(yhi - 1, B.nby - 1); by++) {
+            if (r > 0 && xlo >= 0) scan_bin(cells, start, by * B.nbx + xlo, px, py, best);
+            if (r > 0 && xhi < B.nbx) scan_bin(cells, start, by * B.nbx + xhi, px, py, best);
+        }
+        const double lb = (double)r * B.side * (1.0 - 1e-9);
+        if (best <= lb * lb) break;
+    }
+    out[i] = best;
+}
+
 }  // namespace
 
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
@@ -223,6 +333,39 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     if (r->bnear) mgk_free(ctx, r->bnear, b_start);
     r->bnear = cursor;
     cursor = nullptr;
+    // per-bin candidate lists
+    if (r->bub) mgk_free(ctx, r->bub, sizeof(double) * (size_t)r->nbins);
+    if (r->cstart) mgk_free(ctx, r->cstart, b_start);
+    if (r->cand) mgk_free(ctx, r->cand, sizeof(float2) * (size_t)std::max<int64_t>(r->ncand, 1));
+    r->bub = nullptr;
+    r->cstart = nullptr;
+    r->cand = nullptr;
+    r->ncand = 0;
+    if ((st = mgk_alloc(ctx, (void**)&r->bub, sizeof(double) * (size_t)r->nbins)) ||
+        (st = mgk_alloc(ctx, (void**)&r->cstart, b_start))) {
+        mgk_free(ctx, cells, sizeof(float2) * ncell);
+        return st;
+    }
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->cstart, 0, b_start, s));
+    if (nb > 0) {
+        const unsigned gbin = (unsigned)((r->nbins + 127) / 128);
+        k_bin_cands<0><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, nullptr, nullptr, nullptr);
+        k_bin_cands<1><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, r->cstart, nullptr, nullptr);
+        k_scan_small<<<1, 1024, 0, s>>>(r->cstart, (int)r->nbins);
+        MGK_CHECK_LAUNCH(ctx, "boundary candidate lists");
+        MGK_COUNT_LAUNCH(ctx, 3);
+        int total = 0;
+        MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&total, r->cstart + r->nbins, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+        r->ncand = total;
+        if ((st = mgk_alloc(ctx, (void**)&r->cand, sizeof(float2) * (size_t)std::max(total, 1)))) {
+            mgk_free(ctx, cells, sizeof(float2) * ncell);
+            return st;
+        }
+        k_bin_cands<2><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, nullptr, r->cstart, r->cand);
+        MGK_CHECK_LAUNCH(ctx, "boundary candidate fill");
+        MGK_COUNT_LAUNCH(ctx, 1);
+    }
     MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
     mgk_free(ctx, cells, sizeof(float2) * ncell);
     r->marked = true;
@@ -233,9 +376,14 @@ int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {
     if (p->n == 0) return MGK_OK;
     const mgk_grid& g = r->g;
     BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};
-    k_dist2_binned<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(p->n, p->x, p->y, r->bcells, r->bstart,
-                                                                          r->bnear, B, p->dist2);
-    MGK_CHECK_LAUNCH(ctx, "k_dist2_binned");
+    if (r->nb == 0) {
+        k_dist2_binned<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(
+            p->n, p->x, p->y, r->bcells, r->bstart, r->bnear, B, p->dist2);
+    } else {
+        k_dist2_cands<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(
+            p->n, p->x, p->y, r->bcells, r->bstart, r->bnear, r->cand, r->cstart, B, p->dist2);
+    }
+    MGK_CHECK_LAUNCH(ctx, "k_dist2");
     MGK_COUNT_LAUNCH(ctx, 1);
     return MGK_OK;
 }

@@ -62,6 +62,10 @@ struct mgk_raster {
     float2* bcells = nullptr;     // boundary-cell centres, binned
     int* bstart = nullptr;        // bin offsets into bcells (nbins + 1)
     int* bnear = nullptr;         // per bin: first ring index holding a non-empty bin
+    double* bub = nullptr;        // per bin: upper bound of the nearest-cell d^2 of its points
+    int* cstart = nullptr;        // per bin: offsets of its candidate list in cand (nbins + 1)
+    float2* cand = nullptr;       // candidate boundary-cell centres, bin by bin
+    int64_t ncand = 0;
     int bnx = 0, bny = 0;         // boundary bins per row / column
     int64_t nbins = 0;
     int64_t nb = 0;

@@ -123,6 +123,23 @@ def test_single_large_crop(ctx):
     assert gev == rev + eev
 
 
+def test_boundary_distance_exact_large(ctx):
+    """Binned candidate-list search vs the oracle's brute force, bit for bit,
+    on a 1000 x 1000 polygon mask with points inside, near the boundary and
+    outside the mask extent."""
+    c = synth.single_large(scale=0.4, seed=5)
+    x = np.concatenate([c["x"][:60000], np.array([-300.0, 4500.0, -50.0, 2000.0, 3999.0], np.float32)])
+    y = np.concatenate([c["y"][:60000], np.array([2000.0, -10.0, -70.0, 4321.0, 0.5], np.float32)])
+    og = o.grid(*c["edge_grid"].astuple())
+    b = o.mark_boundary(og, c["edge_mask"])
+    ref = o.dist2_boundary(x, y, og, b)
+    pts = mk.Points.upload(ctx, x, y)
+    em = mk.Raster.upload(ctx, mk.Grid.of(c["edge_grid"]), c["edge_mask"])
+    mk.calc_dist2_boundary(ctx, pts, em)
+    got, _ = pts.download(dist2=True, ew=False)
+    assert np.array_equal(got, ref)
+
+
 def test_loo_batch_matches_oracle(ctx):
     d = load("loo_h1")
     x, y, w = d["x"], d["y"], d["w"]
