@@ -195,17 +195,40 @@ __device__ __forceinline__ double maxd2(double x0, double y0, double x1, double 
 }
 
 // mode 0: UB per bin; mode 1: candidate count per bin; mode 2: fill the lists
+// (one warp per bin; the lanes share each ring's perimeter bins)
+__device__ __forceinline__ bool ring_bin(int r, int i, int bx0, int by0, const BinGrid& B, int& kk) {
+    int bx, by;
+    if (r == 0) {
+        bx = bx0;
+        by = by0;
+    } else if (i < 2 * r + 1) {
+        bx = bx0 - r + i;
+        by = by0 - r;
+    } else if (i < 4 * r + 2) {
+        bx = bx0 - r + (i - 2 * r - 1);
+        by = by0 + r;
+    } else if (i < 6 * r + 1) {
+        bx = bx0 - r;
+        by = by0 - r + 1 + (i - 4 * r - 2);
+    } else {
+        bx = bx0 + r;
+        by = by0 - r + 1 + (i - 6 * r - 1);
+    }
+    if (bx < 0 || by < 0 || bx >= B.nbx || by >= B.nby) return false;
+    kk = by * B.nbx + bx;
+    return true;
+}
+
 template <int MODE>
 __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restrict__ start,
                             const int* __restrict__ near, BinGrid B, double* __restrict__ ub,
                             int* __restrict__ cnt, const int* __restrict__ cstart, float2* __restrict__ cand) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= B.nbx * B.nby) return;
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= B.nbx * B.nby) return;  // warp-uniform
     const int bx0 = k % B.nbx, by0 = k / B.nbx;
     double x0, y0, x1, y1;
     bin_rect(B, bx0, by0, x0, y0, x1, y1);
-    // widen the rectangle a little: a point assigned to this bin by a rounded
-    // floor() may sit a hair outside it, and the lists must stay supersets
     const double widen = 1e-6 * B.side;
     x0 -= widen;
     y0 -= widen;
@@ -214,31 +237,51 @@ __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restr
     const int rmax = max(B.nbx, B.nby);
     double lim = MODE == 0 ? DBL_MAX : ub[k] * (1.0 + 1e-9);
     int n = 0;
-    const int base = MODE == 2 ? cstart[k] : 0;
+    int base = MODE == 2 ? cstart[k] : 0;
     for (int r = near[k]; r <= rmax; r++) {
-        // cells in ring r are at least (r - 1) bins away from the rectangle
         const double lb = (double)(r > 0 ? r - 1 : 0) * B.side * (1.0 - 1e-9);
-        if (lb * lb > lim) break;
-        for (int by = max(by0 - r, 0); by <= min(by0 + r, B.nby - 1); by++) {
-            const bool edge_row = (by == by0 - r) || (by == by0 + r);
-            for (int bx = max(bx0 - r, 0); bx <= min(bx0 + r, B.nbx - 1); bx++) {
-                if (!edge_row && bx != bx0 - r && bx != bx0 + r) continue;
-                const int kk = by * B.nbx + bx;
-                for (int j = start[kk]; j < start[kk + 1]; j++) {
-                    const double cx = cells[j].x, cy = cells[j].y;
-                    if (MODE == 0) {
-                        lim = fmin(lim, maxd2(x0, y0, x1, y1, cx, cy));
-                    } else if (mind2(x0, y0, x1, y1, cx, cy) <= lim) {
-                        if (MODE == 2) cand[base + n] = cells[j];
-                        n++;
+        if (lb * lb > lim) break;  // lim is warp-uniform
+        const int per = r == 0 ? 1 : 8 * r;
+        int mine = 0;
+        for (int i = lane; i < per; i += 32) {
+            int kk;
+            if (!ring_bin(r, i, bx0, by0, B, kk)) continue;
+            for (int j = start[kk]; j < start[kk + 1]; j++) {
+                const double cx = cells[j].x, cy = cells[j].y;
+                if (MODE == 0) lim = fmin(lim, maxd2(x0, y0, x1, y1, cx, cy));
+                else if (mind2(x0, y0, x1, y1, cx, cy) <= lim) mine++;
+            }
+        }
+        if (MODE == 0) {
+            for (int o = 16; o; o >>= 1) lim = fmin(lim, __shfl_xor_sync(0xffffffffu, lim, o));
+        } else {
+            // lane offsets within the ring, then the matches are written in lane order
+            int incl = mine;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            const int tot = __shfl_sync(0xffffffffu, incl, 31);
+            if (MODE == 2 && mine) {
+                int w = base + n + incl - mine;
+                for (int i = lane; i < per; i += 32) {
+                    int kk;
+                    if (!ring_bin(r, i, bx0, by0, B, kk)) continue;
+                    for (int j = start[kk]; j < start[kk + 1]; j++) {
+                        const double cx = cells[j].x, cy = cells[j].y;
+                        if (mind2(x0, y0, x1, y1, cx, cy) <= lim) cand[w++] = cells[j];
                     }
                 }
             }
+            n += tot;
         }
     }
-    if (MODE == 0) ub[k] = lim;
-    if (MODE == 1) cnt[k] = n;
+    if (lane == 0) {
+        if (MODE == 0) ub[k] = lim;
+        if (MODE == 1) cnt[k] = n;
+    }
 }
+
 
 __global__ void k_dist2_cands(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
                               const float2* __restrict__ cells, const int* __restrict__ start,
@@ -348,7 +391,7 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     }
     MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->cstart, 0, b_start, s));
     if (nb > 0) {
-        const unsigned gbin = (unsigned)((r->nbins + 127) / 128);
+        const unsigned gbin = (unsigned)((r->nbins * 32 + 127) / 128);  // one warp per bin
         k_bin_cands<0><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, nullptr, nullptr, nullptr);
         k_bin_cands<1><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, r->cstart, nullptr, nullptr);
         k_scan_small<<<1, 1024, 0, s>>>(r->cstart, (int)r->nbins);
