@@ -63,53 +63,103 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed
+    region: NVML in a background thread every 10 ms (read-only queries), or
+    nvidia-smi -lms 200 when NVML is not importable."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
     def __init__(self, device):
         self.device = device
         self.proc = None
         self.path = None
+        self.thread = None
+        self.samples = []
+        self.stop_flag = False
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            p = torch.cuda.get_device_properties(self.device)
+            bus = "%08x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        except Exception:
+            return self._start_smi()
+        import threading
+
+        def run():
+            while not self.stop_flag:
+                try:
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, mx, [n for n, b in bits.items() if r & b]))
+                except Exception:
+                    pass
+                time.sleep(0.01)
+
+        self.thread = threading.Thread(target=run, daemon=True)
+        self.thread.start()
+        t0 = time.time()
+        while not self.samples and time.time() - t0 < 2.0:
+            time.sleep(0.005)
+
+    def _start_smi(self):
         if not shutil.which("nvidia-smi"):
             return
+        fields = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                  "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                  "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         fd, self.path = tempfile.mkstemp(suffix=".csv")
         os.close(fd)
-        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+        self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={fields}",
                                       "--format=csv,noheader,nounits", "-lms", "200"],
                                      stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        time.sleep(1.0)
 
     def stop(self):
-        if not self.proc:
-            return None
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], [], set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [t.strip() for t in line.split(",")]
-            if len(f) < 9:
-                continue
+        if self.thread:
+            self.stop_flag = True
+            self.thread.join(timeout=2)
+            rows = self.samples
+            src = "nvml"
+        elif self.proc:
+            self.proc.terminate()
             try:
-                sm.append(float(f[1]))
-                mx.append(float(f[2]))
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower() == "active":
-                    reasons.add(n)
-        os.unlink(self.path)
-        if not sm:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            rows = []
+            for line in open(self.path):
+                f = [t.strip() for t in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    rows.append((float(f[1]), float(f[2]),
+                                 [n for n, v in zip(self.NAMES, f[5:9]) if v.lower() == "active"]))
+                except ValueError:
+                    continue
+            os.unlink(self.path)
+            src = "nvidia-smi"
+        else:
             return None
-        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if not rows:
+            return None
+        reasons = sorted({n for _, _, rs in rows for n in rs})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": float(max(r[1] for r in rows)),
+                "reasons": reasons, "samples": len(rows), "source": src}
 
 
 def build_workload(name, scale, seed):
@@ -341,6 +391,22 @@ def run_mgk(args):
     h2d = 4 * (3 * len(c["x"]) + c["edge_mask"].size + c["density_mask"].size)
     d2h = 4 * dg.nrows * dg.ncols
 
+    # the plain FP64 GPU form of the density gather on the same raster (one launch, after warm-up)
+    fp64_form = None
+    if not args.no_fp64_form:
+        idx = mk.Index(ctx, pts, h)
+        mk.density_tile(ctx, idx, dg, 0, 0, dg.nrows, dg.ncols, ddmask, dout, fp64=True)
+        f64_ms = []
+        for _ in range(2):
+            mk.density_tile(ctx, idx, dg, 0, 0, dg.nrows, dg.ncols, ddmask, dout, fp64=True)
+            f64_ms.append(ctx.last_density_ms)
+        idx.close()
+        f64 = float(np.mean(f64_ms))
+        dens_ms_mean = float(np.mean(dens_ms))
+        fp64_form = {"value": ev_d / (f64 / 1e3), "unit": UNIT, "kernel": "k_density_fp64", "kernel_ms": f64,
+                     "fp32c_kernel_value": ev_d / (dens_ms_mean / 1e3),
+                     "fp32c_over_fp64": f64 / dens_ms_mean}
+
     # roofline of the density kernel (FP32-issue bound; no measured FP32 peak exists, nominal used)
     peaks, peak_kind = load_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
@@ -349,11 +415,12 @@ def run_mgk(args):
     dens_s = float(np.mean(dens_ms)) / 1e3
     achieved = ev_d * FLOP_PER_EVAL / dens_s / 1e12
     traffic = None
-    tp = os.path.join(REPO, "profiles", "density_traffic.json")
-    if os.path.exists(tp):
+    tp = os.path.join(REPO, "profiles", "k_density_traffic.txt")
+    if os.path.exists(tp) and args.scale == 1.0:
         with open(tp) as f:
-            tj = json.load(f)
-        traffic = tj.get("bytes_per_launch_scaled")
+            for line in f:
+                if line.startswith("bytes_per_launch_scaled:"):
+                    traffic = int(line.split(":", 1)[1].split()[0])
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
@@ -368,6 +435,7 @@ def run_mgk(args):
                      "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
                                   f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"},
         "clocks": clocks,
+        "fp64_form": fp64_form,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -393,6 +461,7 @@ def main():
     ap.add_argument("--workload", default="single_large")
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp64-form", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -117,28 +117,54 @@ __device__ __forceinline__ void scan_bin(const float2* __restrict__ cells, const
     }
 }
 
+// Bin index of perimeter position i (0 <= i < 8r; i = 0 for r = 0) of the
+// square ring r around (bx0, by0); false when that bin is off the grid.
+__device__ __forceinline__ bool ring_bin(int r, int i, int bx0, int by0, const BinGrid& B, int& kk) {
+    int bx, by;
+    if (r == 0) {
+        bx = bx0;
+        by = by0;
+    } else if (i < 2 * r + 1) {
+        bx = bx0 - r + i;
+        by = by0 - r;
+    } else if (i < 4 * r + 2) {
+        bx = bx0 - r + (i - 2 * r - 1);
+        by = by0 + r;
+    } else if (i < 6 * r + 1) {
+        bx = bx0 - r;
+        by = by0 - r + 1 + (i - 4 * r - 2);
+    } else {
+        bx = bx0 + r;
+        by = by0 - r + 1 + (i - 6 * r - 1);
+    }
+    if (bx < 0 || by < 0 || bx >= B.nbx || by >= B.nby) return false;
+    kk = by * B.nbx + bx;
+    return true;
+}
+
 // Per bin: the smallest ring index (Chebyshev distance in bins) holding a
 // non-empty bin; rings inside it are empty and are skipped by the search.
+// One warp per bin, the lanes sharing each ring's perimeter.
 __global__ void k_bin_near(const int* __restrict__ start, BinGrid B, int* __restrict__ near) {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= B.nbx * B.nby) return;
+    const int lane = threadIdx.x & 31;
+    const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (k >= B.nbx * B.nby) return;  // warp-uniform
     const int bx0 = k % B.nbx, by0 = k / B.nbx;
     const int rmax = max(B.nbx, B.nby);
     int found = rmax + 1;
-    for (int r = 0; r <= rmax && found > rmax; r++) {
-        for (int by = max(by0 - r, 0); by <= min(by0 + r, B.nby - 1) && found > rmax; by++) {
-            const bool edge_row = (by == by0 - r) || (by == by0 + r);
-            for (int bx = max(bx0 - r, 0); bx <= min(bx0 + r, B.nbx - 1); bx++) {
-                if (!edge_row && bx != bx0 - r && bx != bx0 + r) continue;
-                const int kk = by * B.nbx + bx;
-                if (start[kk + 1] > start[kk]) {
-                    found = r;
-                    break;
-                }
-            }
+    for (int r = 0; r <= rmax; r++) {
+        const int per = r == 0 ? 1 : 8 * r;
+        bool hit = false;
+        for (int i = lane; i < per && !hit; i += 32) {
+            int kk;
+            hit = ring_bin(r, i, bx0, by0, B, kk) && start[kk + 1] > start[kk];
+        }
+        if (__any_sync(0xffffffffu, hit)) {
+            found = r;
+            break;
         }
     }
-    near[k] = found;
+    if (lane == 0) near[k] = found;
 }
 
 __global__ void k_dist2_binned(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
@@ -196,29 +222,6 @@ __device__ __forceinline__ double maxd2(double x0, double y0, double x1, double 
 
 // mode 0: UB per bin; mode 1: candidate count per bin; mode 2: fill the lists
 // (one warp per bin; the lanes share each ring's perimeter bins)
-__device__ __forceinline__ bool ring_bin(int r, int i, int bx0, int by0, const BinGrid& B, int& kk) {
-    int bx, by;
-    if (r == 0) {
-        bx = bx0;
-        by = by0;
-    } else if (i < 2 * r + 1) {
-        bx = bx0 - r + i;
-        by = by0 - r;
-    } else if (i < 4 * r + 2) {
-        bx = bx0 - r + (i - 2 * r - 1);
-        by = by0 + r;
-    } else if (i < 6 * r + 1) {
-        bx = bx0 - r;
-        by = by0 - r + 1 + (i - 4 * r - 2);
-    } else {
-        bx = bx0 + r;
-        by = by0 - r + 1 + (i - 6 * r - 1);
-    }
-    if (bx < 0 || by < 0 || bx >= B.nbx || by >= B.nby) return false;
-    kk = by * B.nbx + bx;
-    return true;
-}
-
 template <int MODE>
 __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restrict__ start,
                             const int* __restrict__ near, BinGrid B, double* __restrict__ ub,
@@ -370,7 +373,7 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
         MGK_COUNT_LAUNCH(ctx, 3);
     }
     // cursor (nbins + 1 ints) is reused as the nearest-ring table
-    k_bin_near<<<(unsigned)((r->nbins + 255) / 256), 256, 0, s>>>(r->bstart, B, cursor);
+    k_bin_near<<<(unsigned)((r->nbins * 32 + 255) / 256), 256, 0, s>>>(r->bstart, B, cursor);
     MGK_CHECK_LAUNCH(ctx, "k_bin_near");
     MGK_COUNT_LAUNCH(ctx, 1);
     if (r->bnear) mgk_free(ctx, r->bnear, b_start);
