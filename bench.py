@@ -452,6 +452,73 @@ def run_mgk(args):
     return 0
 
 
+# ------------------------------------------------- bandwidth selection (C2) --
+def run_bandwidth_select(args):
+    """One step = one batched bandwidth selection: point-to-boundary distances,
+    then edge weights and the leave-one-out log likelihood for 64 log-spaced
+    h in [5, 500] and the argmax, in one graph launch.  Evals = edge-mask
+    cells plus point pairs inside the cutoff, summed over the 64 h."""
+    import torch
+
+    import mgpukde_tiled_b200 as mk
+
+    rank, world, local = env_rank()
+    if world > 1:
+        raise SystemExit("bandwidth_select runs on one GPU (replicas only)")
+    torch.cuda.set_device(local)
+    c = synth.bandwidth_select(scale=args.scale, seed=2, nh=64)
+    eg = mk.Grid.of(c["edge_grid"])
+    stream = torch.cuda.current_stream()
+    ctx = mk.Context(local, stream=stream)
+    dx = torch.from_numpy(c["x"]).cuda()
+    dy = torch.from_numpy(c["y"]).cuda()
+    dw = torch.from_numpy(c["w"]).cuda()
+    demask = torch.from_numpy(c["edge_mask"]).cuda()
+    pts = mk.Points.wrap(ctx, dx, dy, dw)
+    em = mk.Raster.wrap(ctx, eg, demask)
+    hgrid = c["hgrid"]
+
+    def step():
+        mk.calc_dist2_boundary(ctx, pts, em)
+        return mk.log_likelihood_batch(ctx, pts, em, hgrid)
+
+    logl, best = step()
+    ev_edge, ev_loo = ctx.last_loo_evals
+    evals = ev_edge + ev_loo
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    loo_ms, batch_ms = [], []
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+        loo_ms.append(ctx.last_loo_ms)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (ctx.kernel_launches - l0) / args.steps
+    out = {"metric": METRIC, "value": evals / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
+           "config": {"workload": f"bandwidth_select: {len(c['x'])} mixture points (20 comps) in "
+                                  f"{c['edge_grid'].ncols * 4}^2, unit weights, edge mask "
+                                  f"{c['edge_grid'].ncols}^2 @ cell 4, 64 log-spaced h in [5, 500]",
+                      "scale": args.scale, "l2": "per-h edge weights and point records stay L2-resident"},
+           "evals_per_step": evals, "edge_evals": ev_edge, "loo_evals": ev_loo,
+           "batch_ms": float(np.mean(loo_ms)), "argmax": best, "h_best": float(hgrid[best]),
+           "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(out))
+    pts.close()
+    em.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -465,6 +532,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    if args.workload == "bandwidth_select":
+        return run_bandwidth_select(args)
     return run_mgk(args)
 
 

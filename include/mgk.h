@@ -75,6 +75,13 @@ const char* mgk_status_string(int status);
  * kernel (CUDA events on the context stream around that one launch). */
 uint64_t mgk_ctx_kernel_launches(const mgk_ctx* ctx);
 float mgk_ctx_last_density_ms(const mgk_ctx* ctx);
+/* Instrumentation of the last mgk_loo_loglik_batch / golden-section step: the
+ * device time in ms of the batch (CUDA events on the context stream around
+ * the edge weights, the gather, the sums and the argmax) and its algorithmic
+ * eval counts (edge-mask cells in the cutoff, point pairs in the cutoff).
+ * No reference counterpart. */
+float mgk_ctx_last_loo_ms(const mgk_ctx* ctx);
+int mgk_ctx_last_loo_evals(const mgk_ctx* ctx, int64_t* edge_evals, int64_t* loo_evals);
 
 /* ---- points (SamplePoints) --------------------------------------------- */
 
@@ -183,6 +190,22 @@ int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid*
                              int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,
                              float* d_out);
 
+/* Several density tiles in one launch (continuous batching of small jobs):
+ * each job is one tile of one index over its own raster, as for
+ * mgk_density_tile.  The tiles are planned independently, so each result is
+ * bitwise the result of mgk_density_tile on that tile alone.  evals
+ * (optional, host, njobs entries): algorithmic pair counts per job (the
+ * counting kernel variant runs when given).  No reference counterpart (the
+ * reference runs one tile at a time, kde_cuda_kdtr_tiled.cu:1233-1517). */
+typedef struct mgk_tile_job {
+    const mgk_index* index;
+    mgk_grid grid;                 /* the raster the tile belongs to */
+    int64_t row0, col0, nrows, ncols;
+    const float* d_mask;           /* device, nrows x ncols row-major, or NULL */
+    float* d_out;                  /* device, nrows x ncols row-major */
+} mgk_tile_job;
+int mgk_density_tiles(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, int64_t* evals);
+
 /* ---- bandwidth selection ---------------------------------------------- */
 
 /* Batched LogLikelihood (kde_cuda_kdtr_tiled.cu:3214-3299) over nh fixed
@@ -201,6 +224,48 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mas
 /* Rule-of-thumb bandwidth (kde_cuda_kdtr_tiled.cu:64-68, 1563-1595), host
  * arithmetic identical to the reference's. */
 float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w);
+
+/* ---- serving loop ------------------------------------------------------ */
+/* A worker thread with its own context on `device` (HBM budget as for
+ * mgk_ctx_create) serves whole fixed-h KDE requests: admission by free slots
+ * (max_active) and the estimated device footprint within the budget, points
+ * and index resident while a request is active, and each tick one density
+ * launch over the next tile (tile_side^2 cells) of every active request, so
+ * requests that arrive while others run join the next tick (continuous
+ * batching).  A request's raster is bitwise the same alone or in a mix.  No
+ * reference counterpart (the reference runs one study per process). */
+typedef struct mgk_server mgk_server;
+typedef struct mgk_request {
+    int64_t n;
+    const float *x, *y, *w;      /* host, n each; w may be NULL */
+    float h;                     /* fixed bandwidth */
+    mgk_grid grid;               /* density raster */
+    const float* mask;           /* host density mask (NoData passthrough) or NULL */
+    int edge;                    /* edge correction on the edge mask below */
+    mgk_grid edge_grid;
+    const float* edge_mask;      /* host */
+    float* out;                  /* host, grid.nrows x grid.ncols */
+} mgk_request;
+typedef struct mgk_result {
+    int status;                  /* MGK_OK or the failing call's status */
+    int64_t evals;               /* density + edge-correction pairs in the cutoff */
+    double queue_ms, run_ms, total_ms;
+} mgk_result;
+typedef struct mgk_serve_info {
+    uint64_t ticks, tiles, max_batch, completed, queued, active, reserved_bytes, device_bytes;
+} mgk_serve_info;
+int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, int max_active,
+                     mgk_server** out);
+/* Queues a request (its host buffers must stay valid until it completes). */
+int mgk_serve_submit(mgk_server* srv, const mgk_request* req, uint64_t* ticket);
+/* done = 1 and the result once finished (the ticket is then released). */
+int mgk_serve_poll(mgk_server* srv, uint64_t ticket, int* done, mgk_result* res);
+/* Blocks until the request finishes (its status is returned) or timeout_s
+ * passes (MGK_ERR_TIMEOUT, the ticket stays valid). */
+int mgk_serve_wait(mgk_server* srv, uint64_t ticket, double timeout_s, mgk_result* res);
+int mgk_serve_stats(mgk_server* srv, mgk_serve_info* out);
+/* Finishes the queued and active requests, then stops the worker. */
+int mgk_serve_destroy(mgk_server* srv);
 
 /* ---- whole path from host buffers ------------------------------------- */
 

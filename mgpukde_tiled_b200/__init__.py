@@ -8,11 +8,13 @@ command line is `_lib/mgkde_tiled`.
 """
 from ._native import EXPORTS, LIB_PATH, MgkError, MgkGrid, lib  # noqa: F401
 from .kde import (Context, Grid, Index, Points, Raster, calc_dist2_boundary, density_tile,  # noqa: F401
-                  edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
+                  density_tiles, edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
                   mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights)
+from .serve import Server  # noqa: F401
 
 __all__ = [
-    "Context", "Grid", "Index", "Points", "Raster", "MgkError", "calc_dist2_boundary", "density_tile",
+    "Context", "Grid", "Index", "Points", "Raster", "MgkError", "Server", "calc_dist2_boundary", "density_tile",
+    "density_tiles",
     "edge_correction_weights", "kde_raster", "log_likelihood_batch", "mark_boundary",
     "mle_fixed_bandwidth", "rule_of_thumb", "unit_edge_weights", "lib",
 ]

@@ -19,19 +19,42 @@ STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "HBM budget exc
 EXPORTS = [
     "mgk_ctx_create", "mgk_ctx_destroy", "mgk_ctx_set_stream", "mgk_ctx_synchronize",
     "mgk_ctx_last_error", "mgk_ctx_bytes_in_use", "mgk_status_string",
-    "mgk_ctx_kernel_launches", "mgk_ctx_last_density_ms",
+    "mgk_ctx_kernel_launches", "mgk_ctx_last_density_ms", "mgk_ctx_last_loo_ms", "mgk_ctx_last_loo_evals",
     "mgk_points_upload", "mgk_points_wrap", "mgk_points_destroy", "mgk_points_device_arrays",
     "mgk_points_download", "mgk_raster_upload", "mgk_raster_wrap", "mgk_raster_destroy",
     "mgk_mark_boundary", "mgk_raster_boundary_download", "mgk_boundary_dist",
     "mgk_edge_weights", "mgk_edge_weights_unit", "mgk_index_build", "mgk_index_destroy",
-    "mgk_density_tile", "mgk_density_tile_fp64", "mgk_density_tile_noalloc", "mgk_loo_loglik_batch",
+    "mgk_density_tile", "mgk_density_tile_fp64", "mgk_density_tile_noalloc", "mgk_density_tiles", "mgk_loo_loglik_batch",
     "mgk_mle_fixed_bandwidth", "mgk_rule_of_thumb", "mgk_kde_raster",
+    "mgk_serve_create", "mgk_serve_submit", "mgk_serve_poll", "mgk_serve_wait", "mgk_serve_stats",
+    "mgk_serve_destroy",
 ]
 
 
 class MgkGrid(C.Structure):
     _fields_ = [("ncols", C.c_int64), ("nrows", C.c_int64), ("xll", C.c_float),
                 ("yll", C.c_float), ("cs", C.c_float), ("nodata", C.c_float)]
+
+
+class MgkTileJob(C.Structure):
+    _fields_ = [("index", C.c_void_p), ("grid", MgkGrid), ("row0", C.c_int64), ("col0", C.c_int64),
+                ("nrows", C.c_int64), ("ncols", C.c_int64), ("d_mask", C.c_void_p), ("d_out", C.c_void_p)]
+
+
+class MgkRequest(C.Structure):
+    _fields_ = [("n", C.c_int64), ("x", C.c_void_p), ("y", C.c_void_p), ("w", C.c_void_p), ("h", C.c_float),
+                ("grid", MgkGrid), ("mask", C.c_void_p), ("edge", C.c_int), ("edge_grid", MgkGrid),
+                ("edge_mask", C.c_void_p), ("out", C.c_void_p)]
+
+
+class MgkResult(C.Structure):
+    _fields_ = [("status", C.c_int), ("evals", C.c_int64), ("queue_ms", C.c_double), ("run_ms", C.c_double),
+                ("total_ms", C.c_double)]
+
+
+class MgkServeInfo(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("ticks", "tiles", "max_batch", "completed", "queued", "active",
+                                          "reserved_bytes", "device_bytes")]
 
 
 class MgkError(RuntimeError):
@@ -64,6 +87,8 @@ def lib():
         "mgk_status_string": (C.c_char_p, [I]),
         "mgk_ctx_kernel_launches": (C.c_uint64, [P]),
         "mgk_ctx_last_density_ms": (C.c_float, [P]),
+        "mgk_ctx_last_loo_ms": (C.c_float, [P]),
+        "mgk_ctx_last_loo_evals": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "mgk_points_upload": (I, [P, I64, P, P, P, P, PP]),
         "mgk_points_wrap": (I, [P, I64, P, P, P, P, PP]),
         "mgk_points_destroy": (I, [P]),
@@ -82,7 +107,14 @@ def lib():
         "mgk_density_tile": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
         "mgk_density_tile_fp64": (I, [P, P, G, I64, I64, I64, I64, P, P, C.POINTER(I64)]),
         "mgk_density_tile_noalloc": (I, [P, P, G, I64, I64, I64, I64, P, P]),
+        "mgk_density_tiles": (I, [P, I, C.POINTER(MgkTileJob), C.POINTER(I64)]),
         "mgk_loo_loglik_batch": (I, [P, P, P, P, I, P, C.POINTER(I)]),
+        "mgk_serve_create": (I, [I, C.c_uint64, I64, I, C.POINTER(P)]),
+        "mgk_serve_submit": (I, [P, C.POINTER(MgkRequest), C.POINTER(C.c_uint64)]),
+        "mgk_serve_poll": (I, [P, C.c_uint64, C.POINTER(I), C.POINTER(MgkResult)]),
+        "mgk_serve_wait": (I, [P, C.c_uint64, C.c_double, C.POINTER(MgkResult)]),
+        "mgk_serve_stats": (I, [P, C.POINTER(MgkServeInfo)]),
+        "mgk_serve_destroy": (I, [P]),
         "mgk_mle_fixed_bandwidth": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(I)]),
         "mgk_rule_of_thumb": (C.c_float, [I64, P, P, P]),
         "mgk_kde_raster": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, P, I64, P, P, C.POINTER(I64)]),

@@ -20,7 +20,7 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "_lib")
 OBJ = os.path.join(PKG, "_build")
-CU_SOURCES = ["api.cu", "index.cu", "density.cu", "boundary.cu", "edge.cu", "loo.cu"]
+CU_SOURCES = ["api.cu", "index.cu", "density.cu", "boundary.cu", "edge.cu", "loo.cu", "serve.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -66,7 +66,7 @@ def build(verbose_ptxas: bool = False, force: bool = False) -> str:
     objs = [o for o, _ in results]
     so = os.path.join(LIB, "libmgk.so")
     if force or not _newer(so, objs):
-        subprocess.run([nvcc(), *ARCH, "-shared", "-o", so, *objs, "-lcudart"], check=True)
+        subprocess.run([nvcc(), *ARCH, "-shared", "-o", so, *objs, "-lcudart", "-lpthread"], check=True)
     cli_src = os.path.join(CSRC, "cli.cpp")
     cli = os.path.join(LIB, "mgkde_tiled")
     if os.path.exists(cli_src) and (force or not _newer(cli, [cli_src, so, *headers])):

@@ -171,6 +171,13 @@ uint64_t mgk_ctx_bytes_in_use(const mgk_ctx* c) { return c ? c->in_use : 0; }
 uint64_t mgk_ctx_kernel_launches(const mgk_ctx* c) { return c ? c->launches : 0; }
 
 float mgk_ctx_last_density_ms(const mgk_ctx* c) { return c ? c->last_density_ms : 0.0f; }
+float mgk_ctx_last_loo_ms(const mgk_ctx* c) { return c ? c->last_loo_ms : 0.0f; }
+int mgk_ctx_last_loo_evals(const mgk_ctx* c, int64_t* edge_evals, int64_t* loo_evals) {
+    if (!c) return MGK_ERR_INVALID;
+    if (edge_evals) *edge_evals = c->last_loo_evals[0];
+    if (loo_evals) *loo_evals = c->last_loo_evals[1];
+    return MGK_OK;
+}
 
 // ----------------------------------------------------------------- points --
 static int points_alloc_results(mgk_ctx* c, mgk_points* p) {
@@ -334,6 +341,8 @@ int mgk_raster_destroy(mgk_raster* r) {
     mgk_free(c, r->bub, sizeof(double) * (size_t)r->nbins);
     mgk_free(c, r->cstart, sizeof(int) * (size_t)(r->nbins + 1));
     mgk_free(c, r->cand, sizeof(float2) * (size_t)std::max<int64_t>(r->ncand, 1));
+    mgk_free(c, r->run_start, sizeof(int64_t) * (size_t)(r->g.nrows + 1));
+    mgk_free(c, r->runs, sizeof(int2) * (size_t)std::max<int64_t>(r->nruns, 1));
     delete r;
     return MGK_OK;
 }
@@ -452,6 +461,35 @@ int mgk_density_tile_fp64(mgk_ctx* c, const mgk_index* idx, const mgk_grid* g, i
     return density_common(c, idx, g, row0, col0, nr, nc, d_mask, d_out, nullptr, true);
 }
 
+int mgk_density_tiles(mgk_ctx* c, int njobs, const mgk_tile_job* jobs, int64_t* evals) {
+    if (!c || njobs < 0 || (njobs > 0 && !jobs)) return mgk_fail(c, MGK_ERR_INVALID, "density_tiles: bad arguments");
+    for (int j = 0; j < njobs; j++) {
+        const mgk_tile_job& J = jobs[j];
+        if (!J.index || !grid_ok(&J.grid) || !J.d_out) return mgk_fail(c, MGK_ERR_INVALID, "density_tiles: bad job");
+        if (J.row0 < 0 || J.col0 < 0 || J.nrows < 0 || J.ncols < 0 || J.row0 + J.nrows > J.grid.nrows ||
+            J.col0 + J.ncols > J.grid.ncols)
+            return mgk_fail(c, MGK_ERR_INVALID, "density_tiles: tile outside its raster");
+    }
+    unsigned long long* d_ev = nullptr;
+    const size_t bev = sizeof(unsigned long long) * (size_t)std::max(njobs, 1);
+    int st;
+    if (evals) {
+        if ((st = mgk_alloc(c, (void**)&d_ev, bev))) return st;
+        MGK_CHECK_CUDA(c, cudaMemsetAsync(d_ev, 0, bev, c->stream));
+    }
+    st = mgk_launch_density_jobs(c, njobs, jobs, d_ev);
+    if (st == MGK_OK && evals) {
+        std::vector<unsigned long long> h(njobs);
+        cudaError_t e = cudaMemcpyAsync(h.data(), d_ev, sizeof(unsigned long long) * njobs, cudaMemcpyDeviceToHost,
+                                        c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "density_tiles evals");
+        for (int j = 0; j < njobs && st == MGK_OK; j++) evals[j] = (int64_t)h[j];
+    }
+    mgk_free(c, d_ev, bev);
+    return st;
+}
+
 // ------------------------------------------------------------ bandwidths --
 float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w) {
     // MeanCenter (float accumulators), StandardDistance2 (double), BandWidth2,
@@ -481,72 +519,57 @@ float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* 
 }
 
 // evaluates logL at each h; the index over the points (unit edge weights) is shared
-static int loglik_many(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const float* hs, int nh, double* logl) {
-    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
-    float hmin = FLT_MAX;
+static int check_bandwidths(mgk_ctx* c, const float* hs, int nh, float* lo, float* hi) {
+    *lo = FLT_MAX;
+    *hi = 0.0f;
     for (int k = 0; k < nh; k++) {
         if (!(hs[k] > 0.0f) || !std::isfinite(hs[k])) return mgk_fail(c, MGK_ERR_INVALID, "loo: bandwidths must be positive");
-        hmin = std::min(hmin, hs[k]);
+        *lo = std::min(*lo, hs[k]);
+        *hi = std::max(*hi, hs[k]);
     }
-    mgk_points view = *p;  // index over w only; e(h) is applied per h
-    view.has_ew = false;
-    view.h = nullptr;
-    mgk_index* idx = nullptr;
-    int st = mgk_index_build(c, &view, hmin, 1.5f * hmin, &idx);
-    if (st) return st;
-    float* ew = nullptr;
-    if (r && (st = mgk_alloc(c, (void**)&ew, sizeof(float) * std::max<int64_t>(p->n, 1)))) {
-        mgk_index_destroy(idx);
-        return st;
-    }
-    for (int k = 0; k < nh && st == MGK_OK; k++) {
-        if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, hs[k], p->dist2, r, ew, nullptr);
-        if (st == MGK_OK) st = mgk_launch_loo(c, idx, r ? ew : nullptr, hs[k], c->d_sum, nullptr);
-        if (st == MGK_OK) {
-            cudaError_t e = cudaMemcpy(&logl[k], c->d_sum, sizeof(double), cudaMemcpyDeviceToHost);
-            if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "loo result");
-        }
-    }
-    if (ew) mgk_free(c, ew, sizeof(float) * std::max<int64_t>(p->n, 1));
-    mgk_index_destroy(idx);
-    return st;
+    return MGK_OK;
 }
 
 int mgk_loo_loglik_batch(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const float* h_grid, int nh, double* logl,
                          int* argmax) {
     if (!c || !p || !h_grid || nh <= 0 || !logl) return mgk_fail(c, MGK_ERR_INVALID, "loo_loglik_batch: bad arguments");
-    int st = loglik_many(c, p, r, h_grid, nh, logl);
+    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
+    float lo, hi;
+    int st = check_bandwidths(c, h_grid, nh, &lo, &hi);
     if (st) return st;
-    if (argmax) {
-        int best = 0;
-        for (int k = 1; k < nh; k++)
-            if (logl[k] > logl[best]) best = k;
-        *argmax = best;
-    }
-    return MGK_OK;
+    mgk_loo_batch* B = nullptr;
+    if ((st = mgk_loo_batch_create(c, p, r, lo, hi, nh, &B))) return st;
+    st = mgk_loo_batch_run(B, h_grid, logl, argmax, nullptr, nullptr);
+    mgk_loo_batch_destroy(B);
+    return st;
 }
 
 int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h0, float* h_opt, int* iterations) {
     if (!c || !p || !h_opt || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "mle_fixed_bandwidth: bad arguments");
+    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
     // MLE_FixedBandWidth, kde_cuda_kdtr_tiled.cu:3044-3093 (float bracket arithmetic)
     float hA = h0 / 20;
     float hD = 2 * h0;
     float width = hD - hA;
     const float epsilon = width / 100;
     const float factor = 1 + sqrtf(5.0f);
+    mgk_loo_batch* B = nullptr;
+    int st = mgk_loo_batch_create(c, p, r, hA, hD, 2, &B);  // every probe lies in [h0/20, 2 h0]
+    if (st) return st;
     int it = 0;
     while (width > epsilon && it < 30) {
         const float hB = hA + width / factor;
         const float hC = hD - width / factor;
         const float hh[2] = {hB, hC};
         double l[2];
-        int st = loglik_many(c, p, r, hh, 2, l);
-        if (st) return st;
+        if ((st = mgk_loo_batch_run(B, hh, l, nullptr, nullptr, nullptr))) break;
         if (l[0] > l[1]) hD = hC;
         else hA = hB;
         width = hD - hA;
         it++;
     }
+    mgk_loo_batch_destroy(B);
+    if (st) return st;
     *h_opt = (hA + hD) / 2;
     if (iterations) *iterations = it;
     return MGK_OK;

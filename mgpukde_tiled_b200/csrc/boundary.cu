@@ -326,7 +326,99 @@ __global__ void k_dist2_cands(int64_t n, const float* __restrict__ x, const floa
     out[i] = best;
 }
 
+// ---- valid-cell runs per row (used by the edge-correction integral) -------
+// One warp per row: a run starts at a valid cell whose left neighbour is
+// NoData (or the row's first cell) and ends after a valid cell whose right
+// neighbour is NoData (or the row's last cell).  MODE 0 counts runs per row,
+// MODE 1 writes them at the row's offset as half-open [a, b).
+template <int MODE>
+__global__ void k_row_runs(mgk_grid g, const float* __restrict__ mask, int64_t* __restrict__ start,
+                           int2* __restrict__ runs) {
+    const int lane = threadIdx.x & 31;
+    const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+    if (r >= g.nrows) return;  // warp-uniform
+    const float* row = mask + r * g.ncols;
+    const float nd = g.nodata;
+    int64_t ns = 0, ne = 0;
+    const int64_t base = MODE ? start[r] : 0;
+    for (int64_t c0 = 0; c0 < g.ncols; c0 += 32) {
+        const int64_t c = c0 + lane;
+        bool v = false, vl = false, vr = false;
+        if (c < g.ncols) {
+            v = row[c] != nd;
+            vl = c > 0 && row[c - 1] != nd;
+            vr = c + 1 < g.ncols && row[c + 1] != nd;
+        }
+        const unsigned sm = __ballot_sync(0xffffffffu, v && !vl);
+        const unsigned em = __ballot_sync(0xffffffffu, v && !vr);
+        if (MODE) {
+            const unsigned lt = (1u << lane) - 1u;
+            if (v && !vl) runs[base + ns + __popc(sm & lt)].x = (int)c;
+            if (v && !vr) runs[base + ne + __popc(em & lt)].y = (int)(c + 1);
+        }
+        ns += __popc(sm);
+        ne += __popc(em);
+    }
+    if (!MODE && lane == 0) start[r] = ns;
+}
+
+// Exclusive scan of n int64 values in one CTA; the total goes to a[n].
+__global__ void __launch_bounds__(1024) k_scan_i64(int64_t* __restrict__ a, int64_t n) {
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t chunk = (n + 1023) / 1024;
+    const int64_t b = t * chunk, e = mgk_min64(n, b + chunk);
+    int64_t s = 0;
+    for (int64_t i = b; i < e; i++) s += a[i];
+    part[t] = s;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+        const int64_t v = t >= off ? part[t - off] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    int64_t run = t ? part[t - 1] : 0;
+    for (int64_t i = b; i < e; i++) {
+        const int64_t v = a[i];
+        a[i] = run;
+        run += v;
+    }
+    if (t == 1023) a[n] = part[1023];
+}
+
 }  // namespace
+
+int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r) {
+    if (r->has_runs) return MGK_OK;
+    const mgk_grid g = r->g;
+    mgk_free(ctx, r->run_start, sizeof(int64_t) * (size_t)(g.nrows + 1));
+    mgk_free(ctx, r->runs, sizeof(int2) * (size_t)std::max<int64_t>(r->nruns, 1));
+    r->run_start = nullptr;
+    r->runs = nullptr;
+    r->nruns = 0;
+    if (g.ncols > (int64_t)INT32_MAX - 1) return mgk_fail(ctx, MGK_ERR_INVALID, "raster wider than 2^31 - 2 columns");
+    cudaStream_t s = ctx->stream;
+    const size_t sb = sizeof(int64_t) * (size_t)(g.nrows + 1);
+    int st;
+    if ((st = mgk_alloc(ctx, (void**)&r->run_start, sb))) return st;
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->run_start, 0, sb, s));
+    const unsigned grid = (unsigned)((g.nrows * 32 + 255) / 256);
+    k_row_runs<0><<<grid, 256, 0, s>>>(g, r->mask, r->run_start, nullptr);
+    k_scan_i64<<<1, 1024, 0, s>>>(r->run_start, g.nrows);
+    MGK_CHECK_LAUNCH(ctx, "k_row_runs count");
+    MGK_COUNT_LAUNCH(ctx, 2);
+    int64_t total = 0;
+    MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&total, r->run_start + g.nrows, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+    MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+    if ((st = mgk_alloc(ctx, (void**)&r->runs, sizeof(int2) * (size_t)std::max<int64_t>(total, 1)))) return st;
+    r->nruns = total;
+    k_row_runs<1><<<grid, 256, 0, s>>>(g, r->mask, r->run_start, r->runs);
+    MGK_CHECK_LAUNCH(ctx, "k_row_runs fill");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    r->has_runs = true;
+    return MGK_OK;
+}
 
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     cudaStream_t s = ctx->stream;
@@ -415,7 +507,9 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
     mgk_free(ctx, cells, sizeof(float2) * ncell);
     r->marked = true;
-    return MGK_OK;
+    // the mask may have changed since the runs were built
+    r->has_runs = false;
+    return mgk_raster_runs(ctx, r);
 }
 
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {

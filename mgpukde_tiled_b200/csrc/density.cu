@@ -253,8 +253,10 @@ constexpr size_t kDensitySmem = kSmemStage + 3 * kSmemTab;
 #define MGK_DENSITY_MIN_CTAS 3  // resident CTAs per SM the register budget is sized for
 #endif
 
+// One work item: the gather of the candidate range [it.k0, it.k1) of one
+// 64 x 64 block (the body of k_density and of the multi-job k_density_jobs).
 template <bool VARH, bool COUNT>
-__global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DParams P) {
+__device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     extern __shared__ __align__(128) unsigned char dsm[];
     MgkPt* stage = reinterpret_cast<MgkPt*>(dsm);                                  // [2][kMB]
     float* colE = reinterpret_cast<float*>(dsm + kSmemStage);                 // [kMB][kFStride] E_j = 2^-a_j
@@ -267,7 +269,6 @@ __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DPar
     __shared__ float s_cxh[kBlk], s_cxl[kBlk], s_cyh[kBlk], s_cyl[kBlk], s_cxg[kBlk], s_cyg[kBlk];
     __shared__ int s_abort;
 
-    const Item it = P.items[blockIdx.x];
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*32..
@@ -559,6 +560,20 @@ __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DPar
     }
 }
 
+template <bool VARH, bool COUNT>
+__global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DParams P) {
+    density_item<VARH, COUNT>(P, P.items[blockIdx.x]);
+}
+
+// Several tiles (of one or several indexes and rasters) in one launch: item
+// it belongs to job it.pad, whose parameters are jobs[it.pad].
+template <bool VARH, bool COUNT>
+__global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density_jobs(const DParams* __restrict__ jobs,
+                                                                                 const Item* __restrict__ items) {
+    const Item it = items[blockIdx.x];
+    density_item<VARH, COUNT>(jobs[it.pad], it);
+}
+
 
 // Plain FP64 form: same blocks, work items and candidate lists; per pair an
 // exact FP64 distance, the cutoff, a double exp and a double accumulate.
@@ -627,11 +642,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
 }
 
 // Merge of split blocks: cell value = sum over the block's slots in order.
-__global__ void k_merge(DParams P, const int32_t* __restrict__ blocks, const int32_t* __restrict__ slot_begin,
-                        int nbx_t) {
-    const int b = blockIdx.x;
-    const int32_t blk = blocks[b];
-    const int s0 = slot_begin[b], s1 = slot_begin[b + 1];
+__device__ __forceinline__ void merge_block(const DParams& P, int32_t blk, int s0, int s1) {
+    const int nbx_t = (int)((P.nc + kBlk - 1) / kBlk);
     const int bxi = blk % nbx_t, byi = blk / nbx_t;
     const int64_t r0 = P.row0 + (int64_t)byi * kBlk, c0 = P.col0 + (int64_t)bxi * kBlk;
     const int nrow = (int)mgk_min64(kBlk, P.row0 + P.nr - r0);
@@ -647,20 +659,33 @@ __global__ void k_merge(DParams P, const int32_t* __restrict__ blocks, const int
     }
 }
 
+__global__ void k_merge(DParams P, const int32_t* __restrict__ blocks, const int32_t* __restrict__ slot_begin) {
+    merge_block(P, blocks[blockIdx.x], slot_begin[blockIdx.x], slot_begin[blockIdx.x + 1]);
+}
+
+// Merges of several jobs: entry b = {job, block, first slot, end slot}.
+__global__ void k_merge_jobs(const DParams* __restrict__ jobs, const int4* __restrict__ list) {
+    const int4 m = list[blockIdx.x];
+    merge_block(jobs[m.x], m.y, m.z, m.w);
+}
+
 template <bool VARH, bool COUNT>
 void launch_density(unsigned grid, cudaStream_t s, const DParams& P) {
     cudaFuncSetAttribute(k_density<VARH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
     k_density<VARH, COUNT><<<grid, kThreads, kDensitySmem, s>>>(P);
 }
 
-}  // namespace
+template <bool VARH, bool COUNT>
+void launch_density_jobs(unsigned grid, cudaStream_t s, const DParams* jobs, const Item* items) {
+    cudaFuncSetAttribute(k_density_jobs<VARH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)kDensitySmem);
+    k_density_jobs<VARH, COUNT><<<grid, kThreads, kDensitySmem, s>>>(jobs, items);
+}
 
-int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
-                       int64_t nr, int64_t nc, const float* d_mask, float* d_out,
-                       unsigned long long* d_evals, bool fp64) {
-    if (nr <= 0 || nc <= 0) return MGK_OK;
-    cudaStream_t s = ctx->stream;
-    DParams P{};
+// Kernel parameters of one tile over one index.
+void fill_params(DParams& P, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0, int64_t nr,
+                 int64_t nc, const float* d_mask, float* d_out) {
+    P = DParams{};
     P.xll = g->xll;
     P.yll = g->yll;
     P.cs = g->cs;
@@ -684,18 +709,72 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     P.k0 = idx->k0;
     P.cut_d2 = idx->cut_d2;
     P.reach = idx->reach;
-    {
-        const double k2 = idx->k2;
-        P.k2h = (float)k2;
-        P.k2l = (float)(k2 - (double)P.k2h);
-        // log2-unit cutoff: 9 h^2 k2 for fixed h; 4.5 log2(e) for per-point h
-        const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
-        P.cutlh = (float)cutl;
-        P.cutll = (float)(cutl - (double)P.cutlh);
-        P.cutf = (float)idx->cut_d2;
-        // ambiguity band in d^2 units: |a - T| < kAmbEps  <=>  |dx^2 - s^2| < kAmbEps / k2 (x2 margin)
-        P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
+    const double k2 = idx->k2;
+    P.k2h = (float)k2;
+    P.k2l = (float)(k2 - (double)P.k2h);
+    // log2-unit cutoff: 9 h^2 k2 for fixed h; 4.5 log2(e) for per-point h
+    const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
+    P.cutlh = (float)cutl;
+    P.cutll = (float)(cutl - (double)P.cutlh);
+    P.cutf = (float)idx->cut_d2;
+    // ambiguity band in d^2 units: |a - T| < kAmbEps  <=>  |dx^2 - s^2| < kAmbEps / k2 (x2 margin)
+    P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
+}
+
+// Work items of one tile from its per-block candidate counts: blocks above K
+// candidates are split into items of at most K (about 8 waves of the
+// resident CTAs), each split item writing an FP64 partial into its own
+// scratch slot.  K depends on this tile alone, so a tile gets the same items
+// (and bitwise the same result) alone or batched with others.
+struct TilePlan {
+    int nbx_t = 0, nby_t = 0;
+    std::vector<Item> items;
+    std::vector<int32_t> split_blocks, split_begin;
+    int32_t nslots = 0;
+};
+
+void plan_tile(const int64_t* counts, int nbx_t, int nby_t, int sm_count, int job, TilePlan& T) {
+    const int nblk = nbx_t * nby_t;
+    T.nbx_t = nbx_t;
+    T.nby_t = nby_t;
+    int64_t total = 0;
+    for (int b = 0; b < nblk; b++) total += counts[b];
+    const int64_t slots_resident = (int64_t)sm_count * 2;
+    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
+    K = (K + kMB - 1) / kMB * kMB;
+    T.items.reserve(nblk + 16);
+    for (int b = 0; b < nblk; b++) {
+        const int64_t c = counts[b];
+        const int bxi = b % nbx_t, byi = b / nbx_t;
+        if (c <= K) {
+            T.items.push_back({bxi, byi, 0, (int32_t)c, -1, job});
+        } else {
+            T.split_blocks.push_back(b);
+            T.split_begin.push_back(T.nslots);
+            for (int64_t k = 0; k < c; k += K) {
+                T.items.push_back({bxi, byi, (int32_t)k, (int32_t)std::min<int64_t>(c, k + K), T.nslots, job});
+                T.nslots++;
+            }
+        }
     }
+    T.split_begin.push_back(T.nslots);
+}
+
+// heaviest items first (they are the tail otherwise)
+void sort_items(std::vector<Item>& items) {
+    std::stable_sort(items.begin(), items.end(),
+                     [](const Item& a, const Item& b) { return (a.k1 - a.k0) > (b.k1 - b.k0); });
+}
+
+}  // namespace
+
+int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                       int64_t nr, int64_t nc, const float* d_mask, float* d_out,
+                       unsigned long long* d_evals, bool fp64) {
+    if (nr <= 0 || nc <= 0) return MGK_OK;
+    cudaStream_t s = ctx->stream;
+    DParams P;
+    fill_params(P, idx, g, row0, col0, nr, nc, d_mask, d_out);
     P.evals = d_evals;
     P.err = ctx->d_counter + 7;
 
@@ -713,40 +792,16 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
     mgk_free(ctx, d_counts, sizeof(int64_t) * nblk);
     if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
-
-    int64_t total = 0;
-    for (int64_t c : counts) total += c;
-    // Items of at most K candidates: about 8 waves of the resident CTAs.
-    const int64_t slots_resident = (int64_t)ctx->sm_count * 2;
-    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
-    K = (K + kMB - 1) / kMB * kMB;
-    std::vector<Item> items;
-    std::vector<int32_t> split_blocks, split_begin;
-    int32_t nslots = 0;
-    items.reserve(nblk + 16);
-    for (int b = 0; b < nblk; b++) {
-        const int64_t c = counts[b];
-        const int bxi = b % nbx_t, byi = b / nbx_t;
-        if (c <= K) {
-            items.push_back({bxi, byi, 0, (int32_t)c, -1, 0});
-        } else {
-            split_blocks.push_back(b);
-            split_begin.push_back(nslots);
-            for (int64_t k = 0; k < c; k += K) {
-                items.push_back({bxi, byi, (int32_t)k, (int32_t)std::min<int64_t>(c, k + K), nslots, 0});
-                nslots++;
-            }
-        }
-    }
-    split_begin.push_back(nslots);
-    // heaviest items first (they are the tail otherwise)
-    std::stable_sort(items.begin(), items.end(),
-                     [](const Item& a, const Item& b) { return (a.k1 - a.k0) > (b.k1 - b.k0); });
+    TilePlan T;
+    plan_tile(counts.data(), nbx_t, nby_t, ctx->sm_count, 0, T);
+    sort_items(T.items);
+    std::vector<Item>& items = T.items;
+    const int32_t nslots = T.nslots;
 
     const size_t b_items = sizeof(Item) * items.size();
     const size_t b_scr = sizeof(double) * (size_t)kBlk * kBlk * (size_t)std::max(nslots, 1);
-    const size_t b_sb = sizeof(int32_t) * (split_blocks.size() + 1);
-    const size_t b_sbeg = sizeof(int32_t) * split_begin.size();
+    const size_t b_sb = sizeof(int32_t) * (T.split_blocks.size() + 1);
+    const size_t b_sbeg = sizeof(int32_t) * T.split_begin.size();
     Item* d_items = nullptr;
     int32_t *d_sb = nullptr, *d_sbeg = nullptr;
     if ((st = mgk_alloc(ctx, (void**)&d_items, b_items))) return st;
@@ -762,9 +817,10 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     do {
         if ((ce = cudaMemcpyAsync(d_items, items.data(), b_items, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
         if (nslots) {
-            if ((ce = cudaMemcpyAsync(d_sb, split_blocks.data(), sizeof(int32_t) * split_blocks.size(),
+            if ((ce = cudaMemcpyAsync(d_sb, T.split_blocks.data(), sizeof(int32_t) * T.split_blocks.size(),
                                       cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
-            if ((ce = cudaMemcpyAsync(d_sbeg, split_begin.data(), b_sbeg, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
+            if ((ce = cudaMemcpyAsync(d_sbeg, T.split_begin.data(), b_sbeg, cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                break;
         }
         P.items = d_items;
         const unsigned grid = (unsigned)items.size();
@@ -783,7 +839,7 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
         MGK_COUNT_LAUNCH(ctx, 2);  // plan + density
         if (nslots) {
-            k_merge<<<(unsigned)split_blocks.size(), 256, 0, s>>>(P, d_sb, d_sbeg, nbx_t);
+            k_merge<<<(unsigned)T.split_blocks.size(), 256, 0, s>>>(P, d_sb, d_sbeg);
             if ((ce = cudaGetLastError()) != cudaSuccess) break;
             MGK_COUNT_LAUNCH(ctx, 1);
         }
@@ -801,6 +857,123 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         mgk_free(ctx, d_sbeg, b_sbeg);
     }
     return rc;
+}
+
+// Several tiles in one density launch (plus one merge launch): the tiles
+// are planned independently (their items and split slots are exactly those
+// of mgk_launch_density), their items concatenated and ordered heaviest
+// first, and each item finds its tile's parameters through its job index.
+// Jobs with per-point bandwidths and jobs with a fixed one go to two
+// launches.  evals (optional, device) receives per-job counters.
+int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, unsigned long long* d_evals) {
+    if (njobs <= 0) return MGK_OK;
+    cudaStream_t s = ctx->stream;
+    std::vector<DParams> P(njobs);
+    std::vector<int> nbx(njobs), nby(njobs), off(njobs + 1, 0);
+    for (int j = 0; j < njobs; j++) {
+        const mgk_tile_job& J = jobs[j];
+        fill_params(P[j], J.index, &J.grid, J.row0, J.col0, J.nrows, J.ncols, J.d_mask, J.d_out);
+        P[j].evals = d_evals ? d_evals + j : nullptr;
+        P[j].err = ctx->d_counter + 7;
+        nbx[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.ncols + kBlk - 1) / kBlk) : 0;
+        nby[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.nrows + kBlk - 1) / kBlk) : 0;
+        off[j + 1] = off[j] + nbx[j] * nby[j];
+    }
+    const int nblk_all = off[njobs];
+    if (nblk_all == 0) return MGK_OK;
+    int st;
+    int64_t* d_counts = nullptr;
+    if ((st = mgk_alloc(ctx, (void**)&d_counts, sizeof(int64_t) * nblk_all))) return st;
+    cudaError_t ce = cudaMemsetAsync(ctx->d_counter + 7, 0, sizeof(unsigned long long), s);
+    for (int j = 0; j < njobs && ce == cudaSuccess; j++) {
+        const int nb = nbx[j] * nby[j];
+        if (nb) k_block_counts<<<(nb + 255) / 256, 256, 0, s>>>(P[j], nbx[j], nby[j], d_counts + off[j]);
+        ce = cudaGetLastError();
+    }
+    std::vector<int64_t> counts(nblk_all);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpyAsync(counts.data(), d_counts, sizeof(int64_t) * nblk_all, cudaMemcpyDeviceToHost, s);
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    mgk_free(ctx, d_counts, sizeof(int64_t) * nblk_all);
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density jobs plan");
+    MGK_COUNT_LAUNCH(ctx, njobs);
+    // plan each job; items of both bandwidth kinds, merges, slot offsets
+    std::vector<Item> items_fix, items_var;
+    std::vector<int4> merges;
+    int32_t nslots = 0;
+    std::vector<int32_t> slot0(njobs, 0);
+    for (int j = 0; j < njobs; j++) {
+        if (!nbx[j]) continue;
+        TilePlan T;
+        plan_tile(counts.data() + off[j], nbx[j], nby[j], ctx->sm_count, j, T);
+        slot0[j] = nslots;
+        for (size_t b = 0; b < T.split_blocks.size(); b++)
+            merges.push_back(make_int4(j, T.split_blocks[b], T.split_begin[b], T.split_begin[b + 1]));
+        nslots += T.nslots;
+        std::vector<Item>& dst = jobs[j].index->varh ? items_var : items_fix;
+        dst.insert(dst.end(), T.items.begin(), T.items.end());
+    }
+    sort_items(items_fix);
+    sort_items(items_var);
+    const size_t b_jobs = sizeof(DParams) * njobs;
+    const size_t b_items = sizeof(Item) * std::max<size_t>(items_fix.size() + items_var.size(), 1);
+    const size_t b_scr = sizeof(double) * (size_t)kBlk * kBlk * (size_t)std::max(nslots, 1);
+    const size_t b_mg = sizeof(int4) * std::max<size_t>(merges.size(), 1);
+    DParams* d_jobs = nullptr;
+    Item* d_items = nullptr;
+    double* d_scr = nullptr;
+    int4* d_mg = nullptr;
+    st = mgk_alloc(ctx, (void**)&d_jobs, b_jobs);
+    if (st == MGK_OK) st = mgk_alloc(ctx, (void**)&d_items, b_items);
+    if (st == MGK_OK && nslots) st = mgk_alloc(ctx, (void**)&d_scr, b_scr);
+    if (st == MGK_OK && !merges.empty()) st = mgk_alloc(ctx, (void**)&d_mg, b_mg);
+    unsigned long long err = 0;
+    if (st == MGK_OK) {
+        for (int j = 0; j < njobs; j++)
+            P[j].scratch = d_scr ? d_scr + (size_t)slot0[j] * kBlk * kBlk : nullptr;  // slots are job-local
+        std::vector<Item> all(items_fix);
+        all.insert(all.end(), items_var.begin(), items_var.end());
+        do {
+            if ((ce = cudaMemcpyAsync(d_jobs, P.data(), b_jobs, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
+            if ((ce = cudaMemcpyAsync(d_items, all.data(), sizeof(Item) * all.size(), cudaMemcpyHostToDevice, s)) !=
+                cudaSuccess)
+                break;
+            if (!merges.empty() && (ce = cudaMemcpyAsync(d_mg, merges.data(), sizeof(int4) * merges.size(),
+                                                         cudaMemcpyHostToDevice, s)) != cudaSuccess)
+                break;
+            cudaEventRecord(ctx->ev_a, s);
+            if (!items_fix.empty()) {
+                if (d_evals) launch_density_jobs<false, true>((unsigned)items_fix.size(), s, d_jobs, d_items);
+                else launch_density_jobs<false, false>((unsigned)items_fix.size(), s, d_jobs, d_items);
+                MGK_COUNT_LAUNCH(ctx, 1);
+            }
+            if (!items_var.empty()) {
+                const Item* iv = d_items + items_fix.size();
+                if (d_evals) launch_density_jobs<true, true>((unsigned)items_var.size(), s, d_jobs, iv);
+                else launch_density_jobs<true, false>((unsigned)items_var.size(), s, d_jobs, iv);
+                MGK_COUNT_LAUNCH(ctx, 1);
+            }
+            cudaEventRecord(ctx->ev_b, s);
+            if ((ce = cudaGetLastError()) != cudaSuccess) break;
+            if (!merges.empty()) {
+                k_merge_jobs<<<(unsigned)merges.size(), 256, 0, s>>>(d_jobs, d_mg);
+                if ((ce = cudaGetLastError()) != cudaSuccess) break;
+                MGK_COUNT_LAUNCH(ctx, 1);
+            }
+            if ((ce = cudaMemcpyAsync(&err, ctx->d_counter + 7, sizeof(err), cudaMemcpyDeviceToHost, s)) !=
+                cudaSuccess)
+                break;
+            ce = cudaStreamSynchronize(s);
+            if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
+        } while (0);
+        if (ce != cudaSuccess) st = mgk_cuda_fail(ctx, ce, "density jobs");
+        else if (err) st = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    }
+    mgk_free(ctx, d_jobs, b_jobs);
+    mgk_free(ctx, d_items, b_items);
+    mgk_free(ctx, d_scr, b_scr);
+    mgk_free(ctx, d_mg, b_mg);
+    return st;
 }
 
 // ---------------------------------------------------------------------------
@@ -971,7 +1144,7 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc");
     MGK_COUNT_LAUNCH(ctx, 2);
     if (nsplit) {
-        k_merge<<<(unsigned)nsplit, 256, 0, s>>>(P, d_sb, d_sbeg, nbx_t);
+        k_merge<<<(unsigned)nsplit, 256, 0, s>>>(P, d_sb, d_sbeg);
         if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc merge");
         MGK_COUNT_LAUNCH(ctx, 1);
     }

@@ -6,108 +6,252 @@
 //   e_p = 1 / sum_{valid c, d^2 < 9h^2} K_h(d) cellArea   otherwise
 // over the reference's NARROW row/column window (a superset of the 3h disc).
 //
-// One warp per point: rows of the window in turn, the 32 lanes across the
-// row's columns, so each mask row segment is one coalesced read.  The cutoff
-// is decided in FP64 exactly as the FP64 CPU path decides it; each in-cutoff
-// term exp2(-dx^2 k2) * exp2(-dy^2 k2) is formed in FP32 from FP64 exponents
-// (hi + lo split) and summed per lane with Kahan compensation; the lanes are
-// merged in FP64 and the normalisation 1 / (sum * cellArea / (h^2 TWO_PI)) is
-// taken in FP64.
+// The Gaussian factorises over the raster, K ~ exp(-dx^2/2h^2) exp(-dy^2/2h^2),
+// and for one row the in-cutoff cells are one contiguous column interval:
+// the FP64 test fl(fl(dx^2) + dy^2) < 9h^2 is monotone in |dx| and the cell
+// centres are monotone in the column.  So per (point, h), with the column
+// factors' prefix sums Q over the window,
+//   sum = sum_rows exp(-dy^2/2h^2) * sum_{valid runs of the row} (Q[b] - Q[a])
+// where [a, b) is a run of valid cells clipped to the row's in-cutoff
+// interval.  The interval ends are found with the oracle's exact FP64 test
+// (an estimate from sqrt(9h^2 - dy^2), verified, with a binary search when the
+// estimate misses), so the summed cell set and the eval count are exactly the
+// reference's.  Work per (point, h) is O(window width + window height) rather
+// than O(width x height); factors and sums are FP64, so the weight is the
+// FP64 value to a few ulps before its rounding to float.
+//
+// One warp per point: the lanes build the prefix table of a chunk of up to
+// 1024 window columns in shared memory (a contiguous segment per lane and a
+// warp scan of the segment totals), then take the window rows in turn.  A
+// list of bandwidths is handled in one launch (the LOO bandwidth search needs
+// e_p(h) for every candidate h); the weights for h_k go to row k of the
+// output.
 #include <algorithm>
 
 #include "mgk_internal.cuh"
 
 namespace {
 
+constexpr int kEdgeWarps = 4;     // warps per CTA
+constexpr int kEdgeChunk = 1024;  // window columns per prefix table
+
+struct EdgeParams {
+    int64_t n;
+    const float* x;
+    const float* y;
+    const float* hpp;    // per-point bandwidths (nh = 1) or null
+    const float* hgrid;  // device bandwidth list (nh entries) or null: use hfix
+    float hfix;
+    int nh;
+    const double* dist2;  // may be null: no short-circuit
+    mgk_grid g;
+    const int64_t* run_start;
+    const int2* runs;
+    float* ew;  // [nh][ew_stride]
+    int64_t ew_stride;
+    unsigned long long* evals;
+};
+
 __device__ __forceinline__ int64_t trunc_index(double v) {
     v = fmin(fmax(v, -1.0e15), 1.0e15);
     return (int64_t)trunc(v);
 }
 
-constexpr int kEdgeThreads = 256;
+__device__ __forceinline__ int64_t clamp_index(double v, int64_t lo, int64_t hi) {
+    v = fmin(fmax(v, (double)lo), (double)hi);
+    return (int64_t)v;
+}
 
-__global__ void __launch_bounds__(kEdgeThreads) k_edge(int64_t n, const float* __restrict__ x,
-                                                       const float* __restrict__ y,
-                                                       const float* __restrict__ hpp, float hfix,
-                                                       const double* __restrict__ dist2, mgk_grid g,
-                                                       const float* __restrict__ mask, float* __restrict__ ew,
-                                                       unsigned long long* __restrict__ evals) {
+__device__ __forceinline__ double cell_xd(const mgk_grid& g, int64_t c) { return (double)mgk_cell_x(g.xll, g.cs, c); }
+
+// The oracle's FP64 cutoff decision for column c of a row at dy^2.
+__device__ __forceinline__ bool in_cut(const mgk_grid& g, int64_t c, double px, double dy2, double cut) {
+    const double dx = __dsub_rn(cell_xd(g, c), px);
+    return __dadd_rn(__dmul_rn(dx, dx), dy2) < cut;
+}
+
+// Smallest c in [a, b] with in_cut true; in_cut is false..true over [a, b]
+// and true at b.
+__device__ __forceinline__ int64_t first_in(const mgk_grid& g, int64_t a, int64_t b, double px, double dy2,
+                                            double cut) {
+    while (a < b) {
+        const int64_t m = a + ((b - a) >> 1);
+        if (in_cut(g, m, px, dy2, cut)) b = m;
+        else a = m + 1;
+    }
+    return a;
+}
+
+// Largest c in [a, b] with in_cut true; true..false over [a, b], true at a.
+__device__ __forceinline__ int64_t last_in(const mgk_grid& g, int64_t a, int64_t b, double px, double dy2,
+                                           double cut) {
+    while (a < b) {
+        const int64_t m = a + ((b - a + 1) >> 1);
+        if (in_cut(g, m, px, dy2, cut)) a = m;
+        else b = m - 1;
+    }
+    return a;
+}
+
+template <bool VARH>
+__global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
+    __shared__ double qsum[kEdgeWarps][kEdgeChunk + 1];
     const int lane = threadIdx.x & 31;
+    double* Q = qsum[threadIdx.x >> 5];
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    const mgk_grid g = E.g;
     const double xll = g.xll, yll = g.yll, cs = g.cs;
     const double cell_area = (double)(g.cs * g.cs);  // float product, kde_cuda_kdtr_tiled.cu:2698
+    const int nh = VARH ? 1 : E.nh;
     unsigned long long cnt_total = 0;
-    for (int64_t p = warp0; p < n; p += nwarps) {
-        const float hp = hpp ? hpp[p] : hfix;
-        const double h2 = mgk_h2(hp);
-        const double cut = MGK_CUT * h2;
-        if (dist2 && dist2[p] >= cut) {
-            if (lane == 0) ew[p] = 1.0f;
-            continue;
-        }
-        const float px = x[p], py = y[p];
-        const double reach = 3.0 * (double)hp;
-        // NARROW window (kde_cuda_kdtr_tiled.cu:2719-2727), truncating casts as in Utilities.h:16-17
-        int64_t rl = g.nrows - 1 - trunc_index(((double)py + reach - yll) / cs);
-        int64_t ru = g.nrows - 1 - trunc_index(((double)py - reach - yll) / cs);
-        int64_t cl = trunc_index(((double)px - reach - xll) / cs);
-        int64_t cu = trunc_index(((double)px + reach - xll) / cs);
-        rl = rl < 0 ? 0 : rl;
-        ru = ru > g.nrows - 1 ? g.nrows - 1 : ru;
-        cl = cl < 0 ? 0 : cl;
-        cu = cu > g.ncols - 1 ? g.ncols - 1 : cu;
-        const double k2 = MGK_LOG2E / (2.0 * h2);
-        float s = 0.0f, c = 0.0f;
-        unsigned cnt = 0;
-        for (int64_t r = rl; r <= ru; r++) {
-            const float cy = mgk_cell_y(yll, cs, g.nrows, r);
-            const double dy = __dsub_rn((double)cy, (double)py);
-            const double dy2 = __dmul_rn(dy, dy);
-            if (dy2 >= cut) continue;
-            const float fy = mgk_exp2_neg(dy2 * k2);
-            const float* mrow = mask + r * g.ncols;
-            for (int64_t col = cl + lane; col <= cu; col += 32) {
-                if (mrow[col] == g.nodata) continue;
-                const float cx = mgk_cell_x(xll, cs, col);
-                const double dx = __dsub_rn((double)cx, (double)px);
-                const double dx2 = __dmul_rn(dx, dx);
-                if (__dadd_rn(dx2, dy2) < cut) {
-                    const float t = mgk_exp2_neg(dx2 * k2) * fy;
-                    const float yk = t - c;
-                    const float tk = s + yk;
-                    c = (tk - s) - yk;
-                    s = tk;
-                    cnt++;
+    for (int64_t p = warp0; p < E.n; p += nwarps) {
+        const double px = E.x[p], py = E.y[p];
+        const double d2b = E.dist2 ? E.dist2[p] : 0.0;
+        for (int k = 0; k < nh; k++) {
+            const float hp = VARH ? E.hpp[p] : (E.hgrid ? E.hgrid[k] : E.hfix);
+            const double h2 = mgk_h2(hp);
+            const double cut = MGK_CUT * h2;
+            float* out = E.ew + (int64_t)k * E.ew_stride + p;
+            if (E.dist2 && d2b >= cut) {
+                if (lane == 0) *out = 1.0f;
+                continue;
+            }
+            const double reach = 3.0 * (double)hp;
+            // NARROW window (kde_cuda_kdtr_tiled.cu:2719-2727), truncating casts as in Utilities.h:16-17
+            int64_t rl = g.nrows - 1 - trunc_index((py + reach - yll) / cs);
+            int64_t ru = g.nrows - 1 - trunc_index((py - reach - yll) / cs);
+            int64_t cl = trunc_index((px - reach - xll) / cs);
+            int64_t cu = trunc_index((px + reach - xll) / cs);
+            rl = rl < 0 ? 0 : rl;
+            ru = ru > g.nrows - 1 ? g.nrows - 1 : ru;
+            cl = cl < 0 ? 0 : cl;
+            cu = cu > g.ncols - 1 ? g.ncols - 1 : cu;
+            const double m2h2 = -2.0 * h2;
+            double acc = 0.0;
+            unsigned long long cnt = 0;
+            for (int64_t c0 = cl; c0 <= cu && rl <= ru; c0 += kEdgeChunk) {
+                const int64_t c1 = mgk_min64(cu, c0 + kEdgeChunk - 1);
+                const int len = (int)(c1 - c0 + 1);
+                // prefix sums of the column factors: Q[j] = sum of the first j
+                const int per = (len + 31) >> 5;
+                const int j0 = min(len, lane * per), j1 = min(len, j0 + per);
+                double run = 0.0;
+                for (int j = j0; j < j1; j++) {
+                    const double dx = __dsub_rn(cell_xd(g, c0 + j), px);
+                    run += exp(__dmul_rn(dx, dx) / m2h2);
+                    Q[j + 1] = run;
                 }
+                double off = run;
+                for (int o = 1; o < 32; o <<= 1) {
+                    const double v = __shfl_up_sync(0xffffffffu, off, o);
+                    if (lane >= o) off += v;
+                }
+                off -= run;  // exclusive prefix of the segment totals
+                for (int j = j0; j < j1; j++) Q[j + 1] += off;
+                if (lane == 0) Q[0] = 0.0;
+                __syncwarp();
+                // the chunk column nearest the point: every non-empty row interval holds it
+                int64_t a = c0, b = c1 + 1;
+                while (a < b) {
+                    const int64_t m = a + ((b - a) >> 1);
+                    if (cell_xd(g, m) >= px) b = m;
+                    else a = m + 1;
+                }
+                int64_t cm = a > c1 ? c1 : a;
+                if (a > c0 && a <= c1 && __dsub_rn(px, cell_xd(g, a - 1)) < __dsub_rn(cell_xd(g, a), px)) cm = a - 1;
+                for (int64_t r = rl + lane; r <= ru; r += 32) {
+                    const double dy = __dsub_rn((double)mgk_cell_y(yll, cs, g.nrows, r), py);
+                    const double dy2 = __dmul_rn(dy, dy);
+                    if (dy2 >= cut || !in_cut(g, cm, px, dy2, cut)) continue;
+                    const double t = sqrt(cut - dy2);
+                    int64_t lo = clamp_index(ceil((px - t - xll) / cs - 0.5), c0, cm);
+                    if (in_cut(g, lo, px, dy2, cut)) {
+                        if (lo > c0 && in_cut(g, lo - 1, px, dy2, cut)) lo = first_in(g, c0, lo - 1, px, dy2, cut);
+                    } else {
+                        lo = first_in(g, lo + 1, cm, px, dy2, cut);
+                    }
+                    int64_t hi = clamp_index(floor((px + t - xll) / cs - 0.5), cm, c1);
+                    if (in_cut(g, hi, px, dy2, cut)) {
+                        if (hi < c1 && in_cut(g, hi + 1, px, dy2, cut)) hi = last_in(g, hi + 1, c1, px, dy2, cut);
+                    } else {
+                        hi = last_in(g, cm, hi - 1, px, dy2, cut);
+                    }
+                    // valid runs of the row clipped to [lo, hi]
+                    int64_t q = E.run_start[r];
+                    const int64_t qe = E.run_start[r + 1];
+                    if (qe - q > 8) {  // first run ending after lo
+                        int64_t x0 = q, x1 = qe;
+                        while (x0 < x1) {
+                            const int64_t m = x0 + ((x1 - x0) >> 1);
+                            if (E.runs[m].y <= lo) x0 = m + 1;
+                            else x1 = m;
+                        }
+                        q = x0;
+                    }
+                    double S = 0.0;
+                    for (; q < qe; q++) {
+                        const int2 rr = E.runs[q];
+                        if (rr.y <= lo) continue;
+                        if (rr.x > hi) break;
+                        const int64_t ra = mgk_max64(rr.x, lo), rb = mgk_min64((int64_t)rr.y - 1, hi);
+                        S += Q[rb - c0 + 1] - Q[ra - c0];
+                        cnt += (unsigned long long)(rb - ra + 1);
+                    }
+                    if (S != 0.0) acc += exp(dy2 / m2h2) * S;
+                }
+                __syncwarp();
+            }
+            for (int o = 16; o; o >>= 1) {
+                acc += __shfl_xor_sync(0xffffffffu, acc, o);
+                cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+            }
+            if (lane == 0) {
+                const double k0 = 1.0 / (h2 * (double)MGK_TWO_PI_F);
+                *out = (float)(1.0 / (acc * k0 * cell_area));
+                cnt_total += cnt;
             }
         }
-        double v = (double)s - (double)c;
-        for (int o = 16; o; o >>= 1) {
-            v += __shfl_xor_sync(0xffffffffu, v, o);
-            cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-        }
-        if (lane == 0) {
-            const double k0 = 1.0 / (h2 * (double)MGK_TWO_PI_F);
-            ew[p] = (float)(1.0 / (v * k0 * cell_area));
-            cnt_total += cnt;
-        }
     }
-    if (evals && lane == 0 && cnt_total) atomicAdd(evals, cnt_total);
+    if (E.evals && lane == 0 && cnt_total) atomicAdd(E.evals, cnt_total);
 }
 
 }  // namespace
 
+int mgk_launch_edge_weights_multi(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp,
+                                  float hfix, const float* d_hgrid, int nh, const double* dist2,
+                                  const mgk_raster* rc, float* ew_out, int64_t ew_stride,
+                                  unsigned long long* d_evals) {
+    if (n == 0 || nh <= 0) return MGK_OK;
+    mgk_raster* r = const_cast<mgk_raster*>(rc);  // the run table is a cache of the mask
+    int st;
+    if ((st = mgk_raster_runs(ctx, r))) return st;
+    EdgeParams E{};
+    E.n = n;
+    E.x = x;
+    E.y = y;
+    E.hpp = hpp;
+    E.hgrid = d_hgrid;
+    E.hfix = hfix;
+    E.nh = hpp ? 1 : nh;
+    E.dist2 = dist2;
+    E.g = r->g;
+    E.run_start = r->run_start;
+    E.runs = r->runs;
+    E.ew = ew_out;
+    E.ew_stride = ew_stride;
+    E.evals = d_evals;
+    const int threads = kEdgeWarps * 32;
+    const int64_t blocks = std::min<int64_t>((int64_t)ctx->sm_count * 8, (n + kEdgeWarps - 1) / kEdgeWarps);
+    if (hpp) k_edge_rows<true><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
+    else k_edge_rows<false><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
+    MGK_CHECK_LAUNCH(ctx, "k_edge_rows");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    return MGK_OK;
+}
+
 int mgk_launch_edge_weights(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp, float h,
                             const double* dist2, const mgk_raster* r, float* ew_out,
                             unsigned long long* d_evals) {
-    if (n == 0) return MGK_OK;
-    const int64_t warps_needed = n;
-    const int64_t max_blocks = (int64_t)ctx->sm_count * 16;
-    const int64_t blocks = std::min<int64_t>(max_blocks, (warps_needed * 32 + kEdgeThreads - 1) / kEdgeThreads);
-    k_edge<<<(unsigned)blocks, kEdgeThreads, 0, ctx->stream>>>(n, x, y, hpp, h, dist2, r->g, r->mask, ew_out,
-                                                               d_evals);
-    MGK_CHECK_LAUNCH(ctx, "k_edge");
-    MGK_COUNT_LAUNCH(ctx, 1);
-    return MGK_OK;
+    return mgk_launch_edge_weights_multi(ctx, n, x, y, hpp, h, nullptr, 1, dist2, r, ew_out, n, d_evals);
 }

@@ -256,7 +256,9 @@ int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float b
     idx->cut_d2 = MGK_CUT * idx->h2;
     idx->k2 = MGK_LOG2E / (2.0 * idx->h2);
     idx->k0 = 1.0 / (idx->h2 * (double)MGK_TWO_PI_F);
-    idx->reach = 3.0 * (double)hmax;
+    // 3h plus a margin: 9 h^2 is formed from the float square, which may
+    // exceed h^2 by a relative 2^-24
+    idx->reach = 3.0 * (double)hmax * (1.0 + 1e-6);
     double side = bin_size > 0.0f ? (double)bin_size : 0.75 * (double)hmax;
     const double ext = std::max(xmax - xmin, ymax - ymin);
     side = std::max(side, ext / 4096.0);

@@ -1,138 +1,525 @@
-// Leave-one-out log likelihood of a fixed bandwidth.
+// Leave-one-out log likelihood for a list of bandwidths in one launch.
 //
 // LogLikelihood (kde_cuda_kdtr_tiled.cu:3214-3299) recomputes the edge
 // weights at h, scatters K_h(d) w_i e_i into every neighbour of i found by a
 // k-d tree range search (DensityAtPointsKdtr, kde_kernel_kdtr.cu:681-804),
 // subtracts the self term and takes logf(max(den, EPSILONDENSITY))
 // (dCopyDensityValues, :806-830), then sums in float (ReductionSum,
-// :1045-1111).  Here the density at query point j is gathered directly over
-// its neighbours i != j in the cell-binned index:
-//   loo_j = sum_{i != j, d^2 < 9h^2} K_h(d) w_i e_i(h)
-// one warp per query, the cutoff decided in FP64 exactly as the oracle does,
-// terms in FP32 from FP64 exponents with Kahan compensation per lane, an FP64
-// lane merge, log in FP64, and a fixed-order FP64 tree reduction over the
-// queries (bitwise reproducible).
+// :1045-1111); MLE_FixedBandWidth (:3044-3093) calls it twice per
+// golden-section step.  Here the density at query point j is gathered over
+// its neighbours i != j:
+//   loo_j(h) = sum_{i != j, d^2 < 9h^2} exp(-d^2 / 2h^2) / (h^2 TWO_PI) w_i e_i(h)
+//   logL(h)  = sum_j log(max(loo_j(h), EPSILONDENSITY))
+// for every h of a list, as one persistent launch over work items
+// (h, group of 128 queries), heaviest h first, fed from a global item
+// counter.  The points are indexed once per bandwidth octave (row-major bins
+// of side in (0.375 h, 0.75 h] for the h that use the level), so the
+// candidates of a group are one contiguous range per bin row; they arrive in
+// batches of 32 through a double-buffered TMA bulk copy into shared memory
+// and every thread (one query) scans them.  The cutoff is decided in FP32
+// with a band around 9h^2 re-decided by the oracle's exact FP64 test, so the
+// summed pair set is exactly the oracle's; terms are FP32 (an exp2 by range
+// reduction and a polynomial, free of the systematic bias an approximate
+// special-function exp2 would add to every one of the sum's terms), summed
+// per batch and added into a Kahan-compensated FP32 accumulator; the per-query log is FP64, and the per-group and per-h sums
+// are fixed-order FP64 trees (bitwise reproducible).  The argmax is taken on
+// the device.  The whole sequence (edge weights for every h, the gather, the
+// sums, the argmax) is captured once into a CUDA graph and replayed, with the
+// bandwidths read from device memory, so a golden-section step is one graph
+// launch.
 #include <algorithm>
+#include <cfloat>
+#include <cmath>
+#include <vector>
 
 #include "mgk_internal.cuh"
 
 namespace {
 
-constexpr int kLooThreads = 256;
+constexpr int kLooQ = 128;    // queries (threads) per work item
+constexpr int kLooB = 32;     // candidates per staged batch
+constexpr int kMaxLev = 16;   // bandwidth octaves
+constexpr long long kLooSpin = 1ll << 24;
 
-__global__ void k_gather_ew(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ ew,
-                            float* __restrict__ sew) {
-    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    if (i < n) sew[i] = ew ? ew[perm[i]] : 1.0f;
+struct LevelDesc {
+    const MgkPt* pts;
+    const int32_t* bin_start;
+    const int32_t* perm;
+    double ox, oy, side, inv_side;
+    int64_t nbx, nby;
+};
+
+struct LooParams {
+    const LevelDesc* lev;  // [nlev], device
+    double side[kMaxLev];  // bin side of each level
+    int nlev;
+    int64_t n;
+    int ngroups;
+    int nh;
+    const float* hgrid;   // [nh]
+    int* korder;          // [nh] processing order (largest h first)
+    int* klevel;          // [nh] level of each h
+    const float* ew;      // [nh][n] input order, or null (no edge correction)
+    double* part;         // [nh][ngroups]
+    unsigned* counter;    // work-item queue head
+    unsigned long long* evals;
+    unsigned long long* err;
+};
+
+// ---- TMA bulk copy + mbarrier (sm_90+ PTX) ---------------------------------
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t* b, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void fence_mbar_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_arrive_tx(uint64_t* b, unsigned bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, uint64_t* b) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(b))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* b, unsigned parity) {
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(b)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
+    for (long long i = 0; i < kLooSpin; i++)
+        if (mbar_try_wait(b, parity)) return true;
+    return false;
 }
 
-__global__ void __launch_bounds__(kLooThreads) k_loo(int64_t n, const MgkPt* __restrict__ pts,
-                                                     const float* __restrict__ sew,
-                                                     const int32_t* __restrict__ bin_start, double ox, double oy,
-                                                     double inv_side, int64_t nbx, int64_t nby, float h,
-                                                     double* __restrict__ logs,
-                                                     unsigned long long* __restrict__ evals) {
-    const int lane = threadIdx.x & 31;
-    const int64_t j = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    if (j >= n) return;
-    const double h2 = mgk_h2(h);
-    const double cut = MGK_CUT * h2;
-    const double k2 = MGK_LOG2E / (2.0 * h2);
-    const double reach = 3.0 * (double)h;
-    const MgkPt qr = pts[j];
-    const float2 q = make_float2(qr.xh + qr.xl, qr.yh + qr.yl);
-    int64_t bx0 = (int64_t)floor(((double)q.x - reach - ox) * inv_side);
-    int64_t bx1 = (int64_t)floor(((double)q.x + reach - ox) * inv_side);
-    int64_t by0 = (int64_t)floor(((double)q.y - reach - oy) * inv_side);
-    int64_t by1 = (int64_t)floor(((double)q.y + reach - oy) * inv_side);
-    bx0 = mgk_max64(bx0, 0);
-    by0 = mgk_max64(by0, 0);
-    bx1 = mgk_min64(bx1, nbx - 1);
-    by1 = mgk_min64(by1, nby - 1);
-    float s = 0.0f, c = 0.0f;
-    unsigned cnt = 0;
-    for (int64_t by = by0; by <= by1; by++) {
-        const int64_t sb = bin_start[by * nbx + bx0], se = bin_start[by * nbx + bx1 + 1];
-        for (int64_t i = sb + lane; i < se; i += 32) {
-            if (i == j) continue;
-            const MgkPt p = pts[i];
-            const double dx = __dsub_rn((double)(p.xh + p.xl), (double)q.x);
-            const double dy = __dsub_rn((double)(p.yh + p.yl), (double)q.y);
-            const double d2 = __dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy));
-            if (d2 < cut) {
-                const float t = mgk_exp2_neg(d2 * k2) * (p.wk * sew[i]);
-                const float yk = t - c;
-                const float tk = s + yk;
-                c = (tk - s) - yk;
-                s = tk;
-                cnt++;
-            }
+__device__ __forceinline__ double block_sum_fixed(double v, double* sh) {
+    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += sh[i];
+    return t;
+}
+
+// Level and processing order of every h (one CTA; nh is small).
+__global__ void k_loo_prep(LooParams P) {
+    for (int k = threadIdx.x; k < P.nh; k += blockDim.x) {
+        const float h = P.hgrid[k];
+        int L = 0;
+        for (int l = 1; l < P.nlev; l++)
+            if (P.side[l] <= 0.75 * (double)h) L = l;
+        int rank = 0;
+        for (int j = 0; j < P.nh; j++) {
+            const float hj = P.hgrid[j];
+            rank += (hj > h) || (hj == h && j < k);
         }
-    }
-    double v = (double)s - (double)c;
-    for (int o = 16; o; o >>= 1) {
-        v += __shfl_xor_sync(0xffffffffu, v, o);
-        cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
-    }
-    if (lane == 0) {
-        const double loo = v / (h2 * (double)MGK_TWO_PI_F);
-        const double floor_v = (double)MGK_EPS_DENSITY_F;
-        logs[j] = log(loo > floor_v ? loo : floor_v);
-        if (evals && cnt) atomicAdd(evals, (unsigned long long)cnt);
+        P.klevel[k] = L;
+        P.korder[rank] = k;
     }
 }
 
-// Fixed-order FP64 sum: each block sums a contiguous range with a tree, one
-// partial per block; a second single-block pass sums the partials.
-__global__ void k_sum_fixed(int64_t n, const double* __restrict__ in, double* __restrict__ out) {
+__global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
+    __shared__ __align__(128) MgkPt stage[2][kLooB];
+    __shared__ float sw[2][kLooB];
+    __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ double red[kLooQ / 32];
+    __shared__ float bb[4][kLooQ / 32];
+    __shared__ int s_item;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (tid == 0) {
+        mbar_init(&mbar[0], 1);
+        mbar_init(&mbar[1], 1);
+        fence_mbar_init();
+    }
+    __syncthreads();
+    unsigned ph0 = 0u, ph1 = 0u;  // mbarrier phase parities of the two buffers
+    const unsigned total = (unsigned)P.nh * (unsigned)P.ngroups;
+    unsigned long long cnt_all = 0;
+    for (;;) {
+        if (tid == 0) s_item = (int)atomicAdd(P.counter, 1u);
+        __syncthreads();
+        const unsigned item = (unsigned)s_item;
+        if (item >= total) break;
+        const int k = P.korder[item / (unsigned)P.ngroups];
+        const int grp = (int)(item % (unsigned)P.ngroups);
+        const LevelDesc L = P.lev[P.klevel[k]];
+        const float h = P.hgrid[k];
+        const double h2 = mgk_h2(h);
+        const double cut = MGK_CUT * h2;
+        const float cutf = (float)cut;
+        const float epsd2 = cutf * 4e-6f;
+        // log2(e) / (2 h^2) as a float pair: a one-float scale would bias every
+        // exponent of the batch the same way
+        const double k2 = MGK_LOG2E / (2.0 * h2);
+        const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
+        const double reach = sqrt(cut) * (1.0 + 1e-9);
+        const float* ewk = P.ew ? P.ew + (int64_t)k * P.n : nullptr;
+
+        // this item's query
+        const int64_t qpos = (int64_t)grp * kLooQ + tid;
+        const bool qv = qpos < P.n;
+        MgkPt q{};
+        if (qv) q = L.pts[qpos];
+        const float qx = q.xh + q.xl, qy = q.yh + q.yl;
+        // bounding box of the group's queries
+        float mnx = qv ? qx : FLT_MAX, mxx = qv ? qx : -FLT_MAX, mny = qv ? qy : FLT_MAX, mxy = qv ? qy : -FLT_MAX;
+        for (int o = 16; o; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+            mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+        }
+        if (lane == 0) {
+            bb[0][warp] = mnx;
+            bb[1][warp] = mxx;
+            bb[2][warp] = mny;
+            bb[3][warp] = mxy;
+        }
+        __syncthreads();
+        for (int i = 0; i < kLooQ / 32; i++) {
+            mnx = fminf(mnx, bb[0][i]);
+            mxx = fmaxf(mxx, bb[1][i]);
+            mny = fminf(mny, bb[2][i]);
+            mxy = fmaxf(mxy, bb[3][i]);
+        }
+        const int64_t bx0 = mgk_max64(0, (int64_t)floor(((double)mnx - reach - L.ox) * L.inv_side));
+        const int64_t bx1 = mgk_min64(L.nbx - 1, (int64_t)floor(((double)mxx + reach - L.ox) * L.inv_side));
+        const int64_t by0 = mgk_max64(0, (int64_t)floor(((double)mny - reach - L.oy) * L.inv_side));
+        const int64_t by1 = mgk_min64(L.nby - 1, (int64_t)floor(((double)mxy + reach - L.oy) * L.inv_side));
+
+        float s = 0.0f, c = 0.0f;
+        unsigned cnt = 0;
+        // candidate stream: batches of <= kLooB within one bin row
+        int64_t by = by0, pos = 0, end = 0;
+        auto next = [&](int64_t& src) -> int {
+            while (pos >= end) {
+                if (by > by1 || bx0 > bx1) return 0;
+                pos = L.bin_start[by * L.nbx + bx0];
+                end = L.bin_start[by * L.nbx + bx1 + 1];
+                by++;
+            }
+            const int m = (int)mgk_min64(kLooB, end - pos);
+            src = pos;
+            pos += m;
+            return m;
+        };
+        int64_t src = 0, nsrc = 0;
+        int m = next(src);
+        int buf = 0;
+        if (m > 0 && tid == 0) {
+            mbar_arrive_tx(&mbar[0], (unsigned)(m * sizeof(MgkPt)));
+            bulk_g2s(&stage[0][0], L.pts + src, (unsigned)(m * sizeof(MgkPt)), &mbar[0]);
+        }
+        while (m > 0) {
+            const int nm = next(nsrc);
+            if (nm > 0 && tid == 0) {
+                mbar_arrive_tx(&mbar[buf ^ 1], (unsigned)(nm * sizeof(MgkPt)));
+                bulk_g2s(&stage[buf ^ 1][0], L.pts + nsrc, (unsigned)(nm * sizeof(MgkPt)), &mbar[buf ^ 1]);
+            }
+            if (tid < m) {
+                const int64_t i = src + tid;
+                sw[buf][tid] = L.pts[i].wk * (ewk ? ewk[L.perm[i]] : 1.0f);
+            }
+            const unsigned par = buf ? ph1 : ph0;
+            const bool ok = mbar_wait(&mbar[buf], par);
+            if (__syncthreads_or(!ok)) {
+                // a staging wait ran out: flag it and give the copies in
+                // flight a second bounded wait before the CTA goes away
+                if (tid == 0) {
+                    atomicExch(P.err, 1ull);
+                    mbar_wait(&mbar[buf], par);
+                    if (nm > 0) mbar_wait(&mbar[buf ^ 1], buf ? ph0 : ph1);
+                }
+                __syncthreads();
+                return;
+            }
+            if (buf) ph1 ^= 1u;
+            else ph0 ^= 1u;
+            if (qv) {
+                float part = 0.0f;
+                const MgkPt* st = stage[buf];
+                for (int t = 0; t < m; t++) {
+                    const float4 cp = *reinterpret_cast<const float4*>(&st[t]);
+                    const float dx = __fadd_rn(__fsub_rn(cp.x, q.xh), __fsub_rn(cp.z, q.xl));
+                    const float dy = __fadd_rn(__fsub_rn(cp.y, q.yh), __fsub_rn(cp.w, q.yl));
+                    const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                    bool in = d2 < cutf;
+                    if (fabsf(d2 - cutf) <= epsd2)  // near the cutoff: the oracle's FP64 decision
+                        in = mgk_d2_exact(qx, qy, cp.x + cp.z, cp.y + cp.w) < cut;
+                    if (in && src + t != qpos) {
+                        const float a = __fmaf_rn(d2, k2h, __fmul_rn(d2, k2l));
+                        part = __fmaf_rn(mgk_exp2_neg_poly(a), sw[buf][t], part);
+                        cnt++;
+                    }
+                }
+                const float y = part - c;
+                const float tt = s + y;
+                c = (tt - s) - y;
+                s = tt;
+            }
+            __syncthreads();  // stage[buf] and sw[buf] are reused two batches on
+            m = nm;
+            src = nsrc;
+            buf ^= 1;
+        }
+        double lg = 0.0;
+        if (qv) {
+            const double loo = ((double)s - (double)c) / (h2 * (double)MGK_TWO_PI_F);
+            const double fl = (double)MGK_EPS_DENSITY_F;
+            lg = log(loo > fl ? loo : fl);
+        }
+        const double sum = block_sum_fixed(lg, red);
+        if (tid == 0) P.part[(int64_t)k * P.ngroups + grp] = sum;
+        cnt_all += cnt;
+        __syncthreads();  // s_item is rewritten next
+    }
+    if (P.evals) {
+        for (int o = 16; o; o >>= 1) cnt_all += __shfl_xor_sync(0xffffffffu, cnt_all, o);
+        if (lane == 0 && cnt_all) atomicAdd(P.evals, cnt_all);
+    }
+}
+
+// logL[k] = fixed-order sum of the group partials of h_k (one CTA per h).
+__global__ void k_loo_finish(const double* __restrict__ part, int ngroups, double* __restrict__ logl) {
     __shared__ double sh[256];
-    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
-    const int64_t b = blockIdx.x * per, e = mgk_min64(n, b + per);
+    const int k = blockIdx.x;
     double v = 0.0;
-    for (int64_t i = b + threadIdx.x; i < e; i += blockDim.x) v += in[i];
+    for (int i = threadIdx.x; i < ngroups; i += blockDim.x) v += part[(int64_t)k * ngroups + i];
     sh[threadIdx.x] = v;
     __syncthreads();
     for (int o = 128; o; o >>= 1) {
         if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
         __syncthreads();
     }
-    if (threadIdx.x == 0) out[blockIdx.x] = sh[0];
+    if (threadIdx.x == 0) logl[k] = sh[0];
+}
+
+// First index of the largest logL (ties resolve to the lower index).
+__global__ void k_argmax(const double* __restrict__ logl, int nh, int* __restrict__ best) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        int b = 0;
+        for (int k = 1; k < nh; k++)
+            if (logl[k] > logl[b]) b = k;
+        *best = b;
+    }
 }
 
 }  // namespace
 
-int mgk_launch_loo(mgk_ctx* ctx, const mgk_index* idx, const float* ew_input_order, float h, double* d_logl,
-                   unsigned long long* d_evals) {
-    const int64_t n = idx->n;
+// ---- the batch object ------------------------------------------------------
+struct mgk_loo_batch {
+    mgk_ctx* ctx = nullptr;
+    const mgk_points* pts = nullptr;
+    const mgk_raster* mask = nullptr;
+    int64_t n = 0;
+    int nh = 0;
+    int ngroups = 0;
+    std::vector<mgk_index*> lev;
+    float* d_h = nullptr;
+    float* d_ew = nullptr;
+    LevelDesc* d_lev = nullptr;
+    cudaStream_t cap = nullptr;  // capture stream
+    int* d_korder = nullptr;
+    int* d_klevel = nullptr;
+    double* d_part = nullptr;
+    double* d_logl = nullptr;
+    int* d_best = nullptr;
+    unsigned* d_counter = nullptr;
+    unsigned long long* d_evals = nullptr;  // [0] edge, [1] loo
+    unsigned long long* d_err = nullptr;
+    float* h_h = nullptr;       // pinned
+    double* h_logl = nullptr;   // pinned: nh logL, then the argmax and the eval counts
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    LooParams P{};
+    size_t bytes_ew = 0, bytes_part = 0;
+};
+
+static int loo_enqueue(mgk_loo_batch* B) {
+    mgk_ctx* ctx = B->ctx;
     cudaStream_t s = ctx->stream;
-    if (n == 0) {
-        MGK_CHECK_CUDA(ctx, cudaMemsetAsync(d_logl, 0, sizeof(double), s));
-        return MGK_OK;
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(B->d_counter, 0, sizeof(unsigned), s));
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(B->d_evals, 0, 2 * sizeof(unsigned long long), s));
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(B->d_err, 0, sizeof(unsigned long long), s));
+    if (B->mask) {
+        int st = mgk_launch_edge_weights_multi(ctx, B->n, B->pts->x, B->pts->y, nullptr, 0.0f, B->d_h, B->nh,
+                                               B->pts->dist2, B->mask, B->d_ew, B->n, B->d_evals);
+        if (st) return st;
     }
-    float* sew = nullptr;
-    double* logs = nullptr;
-    double* part = nullptr;
-    const int nblk = 256;
-    int st;
-    if ((st = mgk_alloc(ctx, (void**)&sew, sizeof(float) * n))) return st;
-    if ((st = mgk_alloc(ctx, (void**)&logs, sizeof(double) * n))) { mgk_free(ctx, sew, sizeof(float) * n); return st; }
-    if ((st = mgk_alloc(ctx, (void**)&part, sizeof(double) * nblk))) {
-        mgk_free(ctx, sew, sizeof(float) * n);
-        mgk_free(ctx, logs, sizeof(double) * n);
+    k_loo_prep<<<1, 256, 0, s>>>(B->P);
+    const int occ = 8;  // resident CTAs of 128 threads per SM targeted by the persistent grid
+    const unsigned items = (unsigned)B->nh * (unsigned)B->ngroups;
+    const unsigned grid = std::max(1u, std::min(items, (unsigned)(ctx->sm_count * occ)));
+    k_loo_multi<<<grid, kLooQ, 0, s>>>(B->P);
+    k_loo_finish<<<B->nh, 256, 0, s>>>(B->d_part, B->ngroups, B->d_logl);
+    k_argmax<<<1, 32, 0, s>>>(B->d_logl, B->nh, B->d_best);
+    MGK_CHECK_LAUNCH(ctx, "loo batch");
+    MGK_COUNT_LAUNCH(ctx, 4);
+    return MGK_OK;
+}
+
+void mgk_loo_batch_destroy(mgk_loo_batch* B) {
+    if (!B) return;
+    mgk_ctx* c = B->ctx;
+    if (B->exec) cudaGraphExecDestroy(B->exec);
+    if (B->graph) cudaGraphDestroy(B->graph);
+    if (B->cap) cudaStreamDestroy(B->cap);
+    mgk_free(c, B->d_lev, sizeof(LevelDesc) * kMaxLev);
+    for (mgk_index* i : B->lev) mgk_index_destroy(i);
+    const size_t nh = (size_t)B->nh;
+    mgk_free(c, B->d_h, sizeof(float) * nh);
+    mgk_free(c, B->d_ew, B->bytes_ew);
+    mgk_free(c, B->d_korder, sizeof(int) * nh);
+    mgk_free(c, B->d_klevel, sizeof(int) * nh);
+    mgk_free(c, B->d_part, B->bytes_part);
+    mgk_free(c, B->d_logl, sizeof(double) * nh);
+    mgk_free(c, B->d_best, sizeof(int));
+    mgk_free(c, B->d_counter, sizeof(unsigned));
+    mgk_free(c, B->d_evals, 2 * sizeof(unsigned long long));
+    mgk_free(c, B->d_err, sizeof(unsigned long long));
+    if (B->h_h) cudaFreeHost(B->h_h);
+    if (B->h_logl) cudaFreeHost(B->h_logl);
+    delete B;
+}
+
+// Plans a batch of nh bandwidths within [h_lo, h_hi]: one point index per
+// bandwidth octave, buffers, and the captured graph.
+int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi, int nh,
+                         mgk_loo_batch** out) {
+    mgk_loo_batch* B = new (std::nothrow) mgk_loo_batch();
+    if (!B) return mgk_fail(c, MGK_ERR_INVALID, "loo batch: out of host memory");
+    B->ctx = c;
+    B->pts = p;
+    B->mask = r;
+    B->n = p->n;
+    B->nh = nh;
+    B->ngroups = (int)((p->n + kLooQ - 1) / kLooQ);
+    int st = MGK_OK;
+    // levels: bin sides 0.75 h_lo * 2^l up to the side for h_hi
+    mgk_points view = *p;  // index over w only; e(h) is applied per h
+    view.has_ew = false;
+    view.h = nullptr;
+    const int nlev = std::min(kMaxLev, 1 + std::max(0, (int)std::ceil(std::log2((double)h_hi / (double)h_lo))));
+    for (int l = 0; l < nlev && st == MGK_OK; l++) {
+        const float side = (float)(0.75 * (double)h_lo * std::ldexp(1.0, l));
+        mgk_index* idx = nullptr;
+        st = mgk_index_build(c, &view, h_lo, side, &idx);
+        if (st == MGK_OK) {
+            B->lev.push_back(idx);
+            // levels whose side was raised to the bin-count limit repeat the previous one
+            if (l > 0 && idx->side <= B->lev[l - 1]->side) break;
+        }
+    }
+    const size_t n1 = (size_t)std::max<int64_t>(p->n, 1);
+    B->bytes_ew = r ? sizeof(float) * n1 * (size_t)nh : 16;
+    B->bytes_part = sizeof(double) * (size_t)nh * (size_t)std::max(B->ngroups, 1);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_h, sizeof(float) * nh);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_ew, B->bytes_ew);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_korder, sizeof(int) * nh);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_klevel, sizeof(int) * nh);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_part, B->bytes_part);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_logl, sizeof(double) * nh);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_best, sizeof(int));
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_counter, sizeof(unsigned));
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_evals, 2 * sizeof(unsigned long long));
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_err, sizeof(unsigned long long));
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_lev, sizeof(LevelDesc) * kMaxLev);
+    if (st == MGK_OK && r) st = mgk_raster_runs(c, const_cast<mgk_raster*>(r));
+    if (st == MGK_OK && cudaMallocHost((void**)&B->h_h, sizeof(float) * nh) != cudaSuccess)
+        st = mgk_fail(c, MGK_ERR_CUDA, "loo batch: pinned allocation");
+    if (st == MGK_OK && cudaMallocHost((void**)&B->h_logl, sizeof(double) * (nh + 3)) != cudaSuccess)
+        st = mgk_fail(c, MGK_ERR_CUDA, "loo batch: pinned allocation");
+    if (st) {
+        mgk_loo_batch_destroy(B);
         return st;
     }
-    k_gather_ew<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, idx->perm, ew_input_order, sew);
-    const int64_t blocks = (n * 32 + kLooThreads - 1) / kLooThreads;
-    k_loo<<<(unsigned)blocks, kLooThreads, 0, s>>>(n, idx->pts, sew, idx->bin_start, idx->ox, idx->oy,
-                                                   1.0 / idx->side, idx->nbx, idx->nby, h, logs, d_evals);
-    k_sum_fixed<<<nblk, 256, 0, s>>>(n, logs, part);
-    k_sum_fixed<<<1, 256, 0, s>>>(nblk, part, d_logl);
-    cudaError_t ce = cudaGetLastError();
-    MGK_COUNT_LAUNCH(ctx, 4);
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    mgk_free(ctx, sew, sizeof(float) * n);
-    mgk_free(ctx, logs, sizeof(double) * n);
-    mgk_free(ctx, part, sizeof(double) * nblk);
-    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "loo");
+    LooParams& P = B->P;
+    P.nlev = (int)B->lev.size();
+    LevelDesc hl[kMaxLev];
+    for (int l = 0; l < P.nlev; l++) {
+        const mgk_index* I = B->lev[l];
+        hl[l] = LevelDesc{I->pts, I->bin_start, I->perm, I->ox, I->oy, I->side, 1.0 / I->side, I->nbx, I->nby};
+        P.side[l] = I->side;
+    }
+    if (cudaMemcpy(B->d_lev, hl, sizeof(LevelDesc) * P.nlev, cudaMemcpyHostToDevice) != cudaSuccess) {
+        mgk_loo_batch_destroy(B);
+        return mgk_fail(c, MGK_ERR_CUDA, "loo batch: level table");
+    }
+    P.lev = B->d_lev;
+    P.n = p->n;
+    P.ngroups = B->ngroups;
+    P.nh = nh;
+    P.hgrid = B->d_h;
+    P.korder = B->d_korder;
+    P.klevel = B->d_klevel;
+    P.ew = r ? B->d_ew : nullptr;
+    P.part = B->d_part;
+    P.counter = B->d_counter;
+    P.evals = B->d_evals + 1;
+    P.err = B->d_err;
+    // capture the sequence into a graph on a private stream (the graph is
+    // then launched into the context's stream); if capture fails the batch
+    // launches its kernels directly
+    if (cudaStreamSynchronize(c->stream) == cudaSuccess &&
+        cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking) == cudaSuccess &&
+        cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        cudaStream_t keep = c->stream;
+        const uint64_t l0 = c->launches;
+        c->stream = B->cap;
+        const int est = loo_enqueue(B);
+        c->stream = keep;
+        c->launches = l0;  // counted at each replay
+        cudaGraph_t g = nullptr;
+        const cudaError_t ce = cudaStreamEndCapture(B->cap, &g);
+        if (est == MGK_OK && ce == cudaSuccess && g) {
+            B->graph = g;
+            if (cudaGraphInstantiate(&B->exec, g, 0) != cudaSuccess) B->exec = nullptr;
+        } else if (g) {
+            cudaGraphDestroy(g);
+        }
+        cudaGetLastError();
+    }
+    *out = B;
+    return MGK_OK;
+}
+
+// Scores the nh bandwidths hs (host) of a planned batch: logL, argmax and the
+// edge and LOO eval counts.
+int mgk_loo_batch_run(mgk_loo_batch* B, const float* hs, double* logl, int* best, int64_t* edge_evals,
+                      int64_t* loo_evals) {
+    mgk_ctx* c = B->ctx;
+    cudaStream_t s = c->stream;
+    for (int k = 0; k < B->nh; k++) B->h_h[k] = hs[k];
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(B->d_h, B->h_h, sizeof(float) * B->nh, cudaMemcpyHostToDevice, s));
+    MGK_CHECK_CUDA(c, cudaEventRecord(c->ev_a, s));
+    if (B->exec) {
+        MGK_CHECK_CUDA(c, cudaGraphLaunch(B->exec, s));
+        MGK_COUNT_LAUNCH(c, 4 + (B->mask ? 1 : 0));
+    } else {
+        int st = loo_enqueue(B);
+        if (st) return st;
+    }
+    MGK_CHECK_CUDA(c, cudaEventRecord(c->ev_b, s));
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(B->h_logl, B->d_logl, sizeof(double) * B->nh, cudaMemcpyDeviceToHost, s));
+    unsigned long long* tail = reinterpret_cast<unsigned long long*>(B->h_logl + B->nh);
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(tail, B->d_evals, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(tail + 2, B->d_err, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+    int* hb = reinterpret_cast<int*>(c->h_counter);
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(hb, B->d_best, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(s));
+    if (tail[2]) return mgk_fail(c, MGK_ERR_TIMEOUT, "loo batch: a staging wait timed out");
+    for (int k = 0; k < B->nh; k++) logl[k] = B->h_logl[k];
+    if (best) *best = *hb;
+    if (edge_evals) *edge_evals = (int64_t)tail[0];
+    if (loo_evals) *loo_evals = (int64_t)tail[1];
+    c->last_loo_evals[0] = (int64_t)tail[0];
+    c->last_loo_evals[1] = (int64_t)tail[1];
+    cudaEventElapsedTime(&c->last_loo_ms, c->ev_a, c->ev_b);
     return MGK_OK;
 }

@@ -38,6 +38,8 @@ struct mgk_ctx {
     uint64_t launches = 0;                    // kernels launched by this context
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
     float last_density_ms = 0.0f;
+    int64_t last_loo_evals[2] = {0, 0};  // edge and LOO evals of the last LOO batch run
+    float last_loo_ms = 0.0f;
 };
 
 #define MGK_COUNT_LAUNCH(ctx, k) ((ctx)->launches += (k))
@@ -70,6 +72,11 @@ struct mgk_raster {
     int64_t nbins = 0;
     int64_t nb = 0;
     bool marked = false;
+    // valid-cell runs per row: runs[run_start[r] .. run_start[r+1]) = [a, b)
+    int64_t* run_start = nullptr;  // nrows + 1
+    int2* runs = nullptr;
+    int64_t nruns = 0;
+    bool has_runs = false;
 };
 
 // One point of the bin-major index (32 B, one bulk copy moves whole records).
@@ -141,6 +148,28 @@ __device__ __forceinline__ float mgk_exp2_neg(double a) {
     return fmaf(-al * MGK_LN2F, e, e);
 }
 
+// 2^-a for 0 <= a < 120, without the special-function unit: a = n + f with
+// n = rint(a), |f| <= 1/2 (Cody-Waite reduction), e^t for t = -f ln 2 from its
+// Taylor series to degree 8 (truncation below 2.1e-10 relative for
+// |t| <= ln2/2), Horner in FMA, then scaled by 2^-n through the exponent
+// bits.  Its rounding errors have no common sign across inputs, so sums of
+// many terms carry no systematic bias (used where millions of terms feed one
+// logarithm sum).
+__device__ __forceinline__ float mgk_exp2_neg_poly(float a) {
+    const float n = rintf(a);
+    const float t = __fmul_rn(__fsub_rn(n, a), MGK_LN2F);
+    float p = 2.4801587301587302e-05f;  // 1/8!
+    p = __fmaf_rn(p, t, 1.9841269841269841e-04f);  // 1/7!
+    p = __fmaf_rn(p, t, 1.3888888888888889e-03f);  // 1/6!
+    p = __fmaf_rn(p, t, 8.3333333333333333e-03f);  // 1/5!
+    p = __fmaf_rn(p, t, 4.1666666666666667e-02f);  // 1/4!
+    p = __fmaf_rn(p, t, 1.6666666666666667e-01f);  // 1/3!
+    p = __fmaf_rn(p, t, 0.5f);
+    p = __fmaf_rn(p, t, 1.0f);
+    p = __fmaf_rn(p, t, 1.0f);
+    return __fmul_rn(p, __int_as_float((127 - (int)n) << 23));
+}
+
 // Cell centres as the reference computes them (Utilities.h:13-14): double
 // arithmetic, stored to float.
 __device__ __host__ __forceinline__ float mgk_cell_x(double xll, double cs, int64_t col) {
@@ -177,10 +206,22 @@ int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float b
 int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
                        int64_t col0, int64_t nr, int64_t nc, const float* d_mask, float* d_out,
                        unsigned long long* d_evals, bool fp64);
+int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, unsigned long long* d_evals);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
+int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r);
 int mgk_launch_edge_weights(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp,
                             float h, const double* dist2, const mgk_raster* r, float* ew_out,
                             unsigned long long* d_evals);
-int mgk_launch_loo(mgk_ctx* ctx, const mgk_index* idx, const float* ew_sorted_or_null, float h,
-                   double* d_logl, unsigned long long* d_evals);
+int mgk_launch_edge_weights_multi(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp,
+                                  float hfix, const float* d_hgrid, int nh, const double* dist2,
+                                  const mgk_raster* r, float* ew_out, int64_t ew_stride,
+                                  unsigned long long* d_evals);
+
+// Batched leave-one-out likelihood (loo.cu).
+struct mgk_loo_batch;
+int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi, int nh,
+                         mgk_loo_batch** out);
+int mgk_loo_batch_run(mgk_loo_batch* B, const float* hs, double* logl, int* best, int64_t* edge_evals,
+                      int64_t* loo_evals);
+void mgk_loo_batch_destroy(mgk_loo_batch* B);

@@ -1,0 +1,367 @@
+// Serving loop: KDE requests of uneven size with continuous batching.
+//
+// The reference has no server: it runs one study per process invocation
+// (main, kde_cuda_kdtr_tiled.cu:290-1540).  Here a worker thread owns one
+// context (one stream, one device allocator under an HBM budget) and serves a
+// queue of requests, each a whole fixed-bandwidth KDE (points, bandwidth,
+// density raster and optional mask, optional edge correction):
+//
+//  * admission: a queued request becomes active when the number of active
+//    requests is below the slot count and its estimated device footprint fits
+//    beside the active ones inside the budget;
+//  * preparation: its points, index (and edge-correction weights) are built
+//    and stay resident on the device while it is active;
+//  * ticks: each tick takes the next tile of every active request (row-major
+//    tiles of tile_side x tile_side cells) and runs all of them in one density
+//    launch (mgk_launch_density_jobs), then copies each tile to its request's
+//    host output.  Requests admitted between ticks join the next tick, so a
+//    short request that arrives while a large one is running finishes after a
+//    few ticks instead of waiting for the large one.
+//
+// Each tile is planned on its own, so a request's raster is bitwise the same
+// whether it ran alone or in a mix.  Callers submit from any thread and wait
+// or poll on a ticket; the host buffers of a request must stay valid until it
+// completes.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "mgk_internal.cuh"
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct Job {
+    uint64_t id = 0;
+    mgk_request req{};
+    int state = 0;  // 0 queued, 1 active, 2 done
+    int status = MGK_OK;
+    uint64_t est = 0;
+    Clock::time_point t_submit, t_start, t_done;
+    mgk_points* p = nullptr;
+    mgk_raster* em = nullptr;
+    mgk_index* idx = nullptr;
+    float* d_mask = nullptr;
+    float* d_out = nullptr;
+    size_t tile_bytes = 0;
+    int64_t tiles_x = 0, tiles_y = 0, next_tile = 0;
+    int64_t evals = 0;
+};
+
+}  // namespace
+
+struct mgk_server {
+    mgk_ctx* ctx = nullptr;
+    int64_t tile = 2048;
+    int max_active = 8;
+    uint64_t budget = 0;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Job*> queue;
+    std::map<uint64_t, Job*> jobs;  // every job until its result is collected
+    std::vector<Job*> active;
+    uint64_t reserved = 0;
+    uint64_t next_id = 1;
+    bool stop = false;
+    std::thread worker;
+    // statistics
+    uint64_t ticks = 0, tiles = 0, max_batch = 0, completed = 0;
+};
+
+namespace {
+
+// Device bytes a request holds while active (an upper estimate).
+uint64_t estimate_bytes(const mgk_request& r, int64_t tile) {
+    const uint64_t n = (uint64_t)std::max<int64_t>(r.n, 1);
+    uint64_t b = n * 24;         // x, y, w, dist2, ew
+    b += n * 64;                 // index records, permutation and sort scratch
+    const double ext = std::max(r.grid.ncols, r.grid.nrows) * (double)r.grid.cs + 6.0 * r.h;
+    const double side = std::max(0.75 * (double)r.h, ext / 4096.0);
+    const double bins = std::min(4096.0 * 4096.0, std::pow(ext / side + 2.0, 2.0));
+    b += (uint64_t)(bins * 4.0);
+    if (r.edge) b += (uint64_t)r.edge_grid.ncols * (uint64_t)r.edge_grid.nrows * 24;
+    const uint64_t tr = (uint64_t)std::min<int64_t>(tile, r.grid.nrows), tc = (uint64_t)std::min<int64_t>(tile, r.grid.ncols);
+    b += 2 * tr * tc * 4;                                 // mask and output tile
+    b += ((tr + 63) / 64) * ((tc + 63) / 64) * 64 * 1024;  // split-block scratch and work list
+    return b + b / 4 + (16u << 20);
+}
+
+void release(mgk_server* S, Job* J) {
+    mgk_ctx* c = S->ctx;
+    mgk_index_destroy(J->idx);
+    mgk_raster_destroy(J->em);
+    mgk_points_destroy(J->p);
+    mgk_free(c, J->d_mask, J->tile_bytes);
+    mgk_free(c, J->d_out, J->tile_bytes);
+    J->idx = nullptr;
+    J->em = nullptr;
+    J->p = nullptr;
+    J->d_mask = J->d_out = nullptr;
+}
+
+// Uploads and indexes a newly admitted request (worker thread).
+int prepare(mgk_server* S, Job* J) {
+    mgk_ctx* c = S->ctx;
+    const mgk_request& r = J->req;
+    int st = mgk_points_upload(c, r.n, r.x, r.y, r.w, nullptr, &J->p);
+    if (st) return st;
+    if (r.edge) {
+        int64_t ev = 0;
+        if ((st = mgk_raster_upload(c, &r.edge_grid, r.edge_mask, &J->em))) return st;
+        if ((st = mgk_boundary_dist(c, J->p, J->em))) return st;
+        if ((st = mgk_edge_weights(c, J->p, J->em, r.h, &ev))) return st;
+        J->evals += ev;
+    } else if ((st = mgk_edge_weights_unit(c, J->p))) {
+        return st;
+    }
+    if ((st = mgk_index_build(c, J->p, r.h, 0.0f, &J->idx))) return st;
+    const int64_t tr = std::min<int64_t>(S->tile, r.grid.nrows), tc = std::min<int64_t>(S->tile, r.grid.ncols);
+    J->tile_bytes = sizeof(float) * (size_t)tr * (size_t)tc;
+    if ((st = mgk_alloc(c, (void**)&J->d_out, J->tile_bytes))) return st;
+    if (r.mask && (st = mgk_alloc(c, (void**)&J->d_mask, J->tile_bytes))) return st;
+    J->tiles_x = (r.grid.ncols + tc - 1) / tc;
+    J->tiles_y = (r.grid.nrows + tr - 1) / tr;
+    J->next_tile = 0;
+    return MGK_OK;
+}
+
+void finish(mgk_server* S, Job* J, int status) {
+    release(S, J);
+    std::lock_guard<std::mutex> lk(S->mu);
+    J->status = status;
+    J->state = 2;
+    J->t_done = Clock::now();
+    S->reserved -= J->est;
+    S->active.erase(std::remove(S->active.begin(), S->active.end(), J), S->active.end());
+    S->completed++;
+    S->cv_done.notify_all();
+}
+
+// One tick: the next tile of every active, prepared request in one launch.
+void tick(mgk_server* S, std::vector<Job*>& act) {
+    mgk_ctx* c = S->ctx;
+    cudaStream_t s = c->stream;
+    std::vector<mgk_tile_job> tj;
+    std::vector<Job*> owner;
+    std::vector<int64_t> r0s, c0s;
+    int st = MGK_OK;
+    for (Job* J : act) {
+        const mgk_request& r = J->req;
+        const int64_t tr = std::min<int64_t>(S->tile, r.grid.nrows), tc = std::min<int64_t>(S->tile, r.grid.ncols);
+        const int64_t ty = J->next_tile / J->tiles_x, tx = J->next_tile % J->tiles_x;
+        const int64_t r0 = ty * tr, c0 = tx * tc;
+        const int64_t nr = std::min(tr, r.grid.nrows - r0), nc = std::min(tc, r.grid.ncols - c0);
+        if (r.mask) {
+            const cudaError_t e = cudaMemcpy2DAsync(J->d_mask, sizeof(float) * nc, r.mask + r0 * r.grid.ncols + c0,
+                                                    sizeof(float) * r.grid.ncols, sizeof(float) * nc, nr,
+                                                    cudaMemcpyHostToDevice, s);
+            if (e != cudaSuccess) {
+                st = mgk_cuda_fail(c, e, "serve: tile mask");
+                break;
+            }
+        }
+        tj.push_back(mgk_tile_job{J->idx, r.grid, r0, c0, nr, nc, r.mask ? J->d_mask : nullptr, J->d_out});
+        owner.push_back(J);
+        r0s.push_back(r0);
+        c0s.push_back(c0);
+    }
+    unsigned long long* d_ev = nullptr;
+    const size_t bev = sizeof(unsigned long long) * std::max<size_t>(tj.size(), 1);
+    if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_ev, bev);
+    if (st == MGK_OK && cudaMemsetAsync(d_ev, 0, bev, s) != cudaSuccess) st = MGK_ERR_CUDA;
+    if (st == MGK_OK) st = mgk_launch_density_jobs(c, (int)tj.size(), tj.data(), d_ev);
+    std::vector<unsigned long long> ev(tj.size(), 0);
+    for (size_t k = 0; k < tj.size() && st == MGK_OK; k++) {
+        const mgk_request& r = owner[k]->req;
+        const cudaError_t e = cudaMemcpy2DAsync(r.out + r0s[k] * r.grid.ncols + c0s[k], sizeof(float) * r.grid.ncols,
+                                                tj[k].d_out, sizeof(float) * tj[k].ncols, sizeof(float) * tj[k].ncols,
+                                                tj[k].nrows, cudaMemcpyDeviceToHost, s);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "serve: tile result");
+    }
+    if (st == MGK_OK && cudaMemcpyAsync(ev.data(), d_ev, sizeof(unsigned long long) * tj.size(),
+                                        cudaMemcpyDeviceToHost, s) != cudaSuccess)
+        st = MGK_ERR_CUDA;
+    if (st == MGK_OK && cudaStreamSynchronize(s) != cudaSuccess) st = MGK_ERR_CUDA;
+    mgk_free(c, d_ev, bev);
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->ticks++;
+        S->tiles += tj.size();
+        S->max_batch = std::max<uint64_t>(S->max_batch, tj.size());
+    }
+    for (size_t k = 0; k < owner.size(); k++) {
+        Job* J = owner[k];
+        if (st) {
+            finish(S, J, st);
+            continue;
+        }
+        J->evals += (int64_t)ev[k];
+        if (++J->next_tile == J->tiles_x * J->tiles_y) finish(S, J, MGK_OK);
+    }
+}
+
+void worker_main(mgk_server* S) {
+    cudaSetDevice(S->ctx->device);
+    std::vector<Job*> fresh;
+    for (;;) {
+        fresh.clear();
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            if (S->active.empty() && S->queue.empty()) {
+                if (S->stop) return;
+                S->cv_work.wait_for(lk, std::chrono::milliseconds(50));
+                continue;
+            }
+            // admission: slots and the HBM budget; a request that fits nowhere
+            // alone is still admitted when nothing else is active
+            while (!S->queue.empty() && (int)S->active.size() < S->max_active) {
+                Job* J = S->queue.front();
+                if (!S->active.empty() && S->reserved + J->est > S->budget) break;
+                S->queue.pop_front();
+                J->state = 1;
+                J->t_start = Clock::now();
+                S->reserved += J->est;
+                S->active.push_back(J);
+                fresh.push_back(J);
+            }
+        }
+        for (Job* J : fresh) {
+            const int st = prepare(S, J);
+            if (st) finish(S, J, st);
+        }
+        std::vector<Job*> act;
+        {
+            std::lock_guard<std::mutex> lk(S->mu);
+            act = S->active;
+        }
+        if (!act.empty()) tick(S, act);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, int max_active, mgk_server** out) {
+    if (!out || max_active <= 0 || tile_side < 64) return MGK_ERR_INVALID;
+    *out = nullptr;
+    mgk_ctx* c = nullptr;
+    int st = mgk_ctx_create(device, hbm_budget_bytes, &c);
+    if (st) return st;
+    mgk_server* S = new (std::nothrow) mgk_server();
+    if (!S) {
+        mgk_ctx_destroy(c);
+        return MGK_ERR_INVALID;
+    }
+    S->ctx = c;
+    S->tile = tile_side;
+    S->max_active = max_active;
+    S->budget = c->budget;
+    S->worker = std::thread(worker_main, S);
+    *out = S;
+    return MGK_OK;
+}
+
+int mgk_serve_submit(mgk_server* S, const mgk_request* r, uint64_t* ticket) {
+    if (!S || !r || !ticket || r->n < 0 || (r->n > 0 && (!r->x || !r->y)) || !(r->h > 0.0f) || !r->out ||
+        r->grid.ncols <= 0 || r->grid.nrows <= 0 || !(r->grid.cs > 0.0f) ||
+        (r->edge && (!r->edge_mask || r->edge_grid.ncols <= 0 || r->edge_grid.nrows <= 0 || !(r->edge_grid.cs > 0.0f))))
+        return MGK_ERR_INVALID;
+    Job* J = new (std::nothrow) Job();
+    if (!J) return MGK_ERR_INVALID;
+    J->req = *r;
+    J->est = estimate_bytes(*r, S->tile);
+    J->t_submit = Clock::now();
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (S->stop) {
+        delete J;
+        return MGK_ERR_INVALID;
+    }
+    J->id = S->next_id++;
+    S->jobs[J->id] = J;
+    S->queue.push_back(J);
+    *ticket = J->id;
+    S->cv_work.notify_one();
+    return MGK_OK;
+}
+
+static void fill_result(const Job* J, mgk_result* res) {
+    if (!res) return;
+    res->status = J->status;
+    res->evals = J->evals;
+    res->queue_ms = ms_between(J->t_submit, J->t_start);
+    res->run_ms = ms_between(J->t_start, J->t_done);
+    res->total_ms = ms_between(J->t_submit, J->t_done);
+}
+
+int mgk_serve_poll(mgk_server* S, uint64_t ticket, int* done, mgk_result* res) {
+    if (!S || !done) return MGK_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    auto it = S->jobs.find(ticket);
+    if (it == S->jobs.end()) return MGK_ERR_INVALID;
+    Job* J = it->second;
+    *done = J->state == 2;
+    if (*done) {
+        fill_result(J, res);
+        S->jobs.erase(it);
+        delete J;
+    }
+    return MGK_OK;
+}
+
+int mgk_serve_wait(mgk_server* S, uint64_t ticket, double timeout_s, mgk_result* res) {
+    if (!S) return MGK_ERR_INVALID;
+    std::unique_lock<std::mutex> lk(S->mu);
+    auto it = S->jobs.find(ticket);
+    if (it == S->jobs.end()) return MGK_ERR_INVALID;
+    Job* J = it->second;
+    const auto until = Clock::now() + std::chrono::duration_cast<Clock::duration>(std::chrono::duration<double>(timeout_s));
+    while (J->state != 2)
+        if (S->cv_done.wait_until(lk, until) == std::cv_status::timeout && J->state != 2) return MGK_ERR_TIMEOUT;
+    fill_result(J, res);
+    S->jobs.erase(ticket);
+    const int st = J->status;
+    delete J;
+    return st;
+}
+
+int mgk_serve_stats(mgk_server* S, mgk_serve_info* out) {
+    if (!S || !out) return MGK_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(S->mu);
+    out->ticks = S->ticks;
+    out->tiles = S->tiles;
+    out->max_batch = S->max_batch;
+    out->completed = S->completed;
+    out->queued = S->queue.size();
+    out->active = S->active.size();
+    out->reserved_bytes = S->reserved;
+    out->device_bytes = S->ctx->in_use;
+    return MGK_OK;
+}
+
+int mgk_serve_destroy(mgk_server* S) {
+    if (!S) return MGK_OK;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->stop = true;
+        S->cv_work.notify_all();
+    }
+    if (S->worker.joinable()) S->worker.join();  // finishes queued and active requests first
+    for (auto& kv : S->jobs) delete kv.second;
+    mgk_ctx_destroy(S->ctx);
+    delete S;
+    return MGK_OK;
+}
+
+}  // extern "C"

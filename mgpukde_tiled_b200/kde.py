@@ -14,7 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import MgkError, MgkGrid, lib
+from ._native import MgkError, MgkGrid, MgkTileJob, lib
 
 
 def _ptr(a):
@@ -86,6 +86,17 @@ class Context:
     @property
     def last_density_ms(self) -> float:
         return float(lib().mgk_ctx_last_density_ms(self._h))
+
+    @property
+    def last_loo_ms(self) -> float:
+        return float(lib().mgk_ctx_last_loo_ms(self._h))
+
+    @property
+    def last_loo_evals(self):
+        """(edge-mask cells, point pairs) in the cutoff in the last LOO batch run."""
+        e, l = C.c_int64(), C.c_int64()
+        lib().mgk_ctx_last_loo_evals(self._h, C.byref(e), C.byref(l))
+        return int(e.value), int(l.value)
 
     @property
     def handle(self):
@@ -244,6 +255,18 @@ def density_tile(ctx: Context, index: Index, grid: Grid, row0, col0, nr, nc, d_m
     ctx.check(f(ctx.handle, index._h, C.byref(g), int(row0), int(col0), int(nr), int(nc), _ptr(d_mask),
                 _ptr(d_out), C.byref(ev) if count else None))
     return ev.value if count else None
+
+
+def density_tiles(ctx: Context, jobs, count=False):
+    """Several tiles in one launch.  jobs: sequence of (index, grid, row0,
+    col0, nr, nc, d_mask, d_out) tuples; returns per-job eval counts when
+    count is set."""
+    arr = (MgkTileJob * max(len(jobs), 1))()
+    for k, (index, grid, row0, col0, nr, nc, d_mask, d_out) in enumerate(jobs):
+        arr[k] = MgkTileJob(index._h, grid.c(), int(row0), int(col0), int(nr), int(nc), _ptr(d_mask), _ptr(d_out))
+    ev = (C.c_int64 * max(len(jobs), 1))()
+    ctx.check(lib().mgk_density_tiles(ctx.handle, len(jobs), arr, ev if count else None))
+    return [int(ev[k]) for k in range(len(jobs))] if count else None
 
 
 def log_likelihood_batch(ctx: Context, points: Points, raster: Raster | None, hgrid):

@@ -327,7 +327,7 @@ void orc_density(int64_t n, const float* x, const float* y, const float* w,
                     }
                 }
             } else {
-                const double reach = 3.0 * (double)hmax;
+                const double reach = 3.0 * (double)hmax * (1.0 + 1e-6); /* 9h^2 uses the float square */
                 int64_t bx0, bx1, by0, by1;
                 bin_span((double)cx - reach, (double)cx + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
                 bin_span((double)cy - reach, (double)cy + reach, b.y0, b.side, b.nby, &by0, &by1);
@@ -362,7 +362,7 @@ double orc_loo_loglik(int64_t n, const float* x, const float* y, const float* w,
     int64_t total = 0;
 #pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 64) reduction(+ : logl, total)
     for (int64_t j = 0; j < n; j++) {
-        const double reach = 3.0 * (double)h;
+        const double reach = 3.0 * (double)h * (1.0 + 1e-6); /* 9h^2 uses the float square */
         int64_t bx0, bx1, by0, by1;
         bin_span((double)x[j] - reach, (double)x[j] + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
         bin_span((double)y[j] - reach, (double)y[j] + reach, b.y0, b.side, b.nby, &by0, &by1);

@@ -147,13 +147,17 @@ def test_loo_batch_matches_oracle(ctx):
     b = o.mark_boundary(eg, d["edge_mask"])
     d2 = o.dist2_boundary(x, y, eg, b)
     hgrid = synth.log_h_grid(2.0, 20.0, 16)
-    ref = np.array([o.loglik_at(x, y, w, d2, eg, d["edge_mask"], float(h))[0] for h in hgrid])
+    refs = [o.loglik_at(x, y, w, d2, eg, d["edge_mask"], float(h)) for h in hgrid]
+    ref = np.array([r[0] for r in refs])
     pts = mk.Points.upload(ctx, x, y, w)
     em = mk.Raster.upload(ctx, mk.Grid.of(eg), d["edge_mask"])
     mk.calc_dist2_boundary(ctx, pts, em)
     got, am = mk.log_likelihood_batch(ctx, pts, em, hgrid)
     assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-6)
     assert am == int(np.argmax(ref))
+    assert sum(ctx.last_loo_evals) == sum(r[1] for r in refs)
+    again, _ = mk.log_likelihood_batch(ctx, pts, em, hgrid)
+    assert np.array_equal(got.view(np.uint64), again.view(np.uint64))
     hopt, it = mk.mle_fixed_bandwidth(ctx, pts, em, o.rule_of_thumb(x, y, w))
     assert abs(hopt - float(d["ref_hopt"])) <= 5e-6 * hopt + 5e-6
 
@@ -175,3 +179,34 @@ def test_errors_leave_device_usable(ctx):
     r = run_components(ctx, d, ref["h"])
     nd = d["density_mask"] == d["dg"].nodata
     assert rel_err(r["density"][~nd], ref["density"][~nd]).max() <= RTOL
+
+
+def test_bandwidth_select_grid_matches_oracle(ctx):
+    """1/10-scale batched bandwidth selection (2,000 mixture points in 500^2,
+    polygon edge mask at cell 4, 16 log-spaced h in [5, 500]): logL per h,
+    the argmax and the edge + pair eval counts against the oracle."""
+    c = synth.bandwidth_select(scale=0.1, seed=2, nh=16)
+    x, y, w = c["x"], c["y"], c["w"]
+    eg = o.grid(*c["edge_grid"].astuple())
+    b = o.mark_boundary(eg, c["edge_mask"])
+    d2 = o.dist2_boundary(x, y, eg, b)
+    refs = [o.loglik_at(x, y, w, d2, eg, c["edge_mask"], float(h)) for h in c["hgrid"]]
+    ref = np.array([r[0] for r in refs])
+    pts = mk.Points.upload(ctx, x, y, w)
+    em = mk.Raster.upload(ctx, mk.Grid.of(c["edge_grid"]), c["edge_mask"])
+    mk.calc_dist2_boundary(ctx, pts, em)
+    got, am = mk.log_likelihood_batch(ctx, pts, em, c["hgrid"])
+    assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-6)
+    assert am == int(np.argmax(ref))
+    assert sum(ctx.last_loo_evals) == sum(r[1] for r in refs)
+
+
+def test_loo_without_edge_correction(ctx):
+    d = load("loo_h1")
+    x, y, w = d["x"], d["y"], d["w"]
+    hgrid = synth.log_h_grid(2.0, 20.0, 8)
+    ref = np.array([o.loo_loglik(x, y, w, None, float(h))[0] for h in hgrid])
+    pts = mk.Points.upload(ctx, x, y, w)
+    got, am = mk.log_likelihood_batch(ctx, pts, None, hgrid)
+    assert np.all(np.abs(got - ref) <= 1e-6 * np.abs(ref) + 1e-6)
+    assert am == int(np.argmax(ref))
