@@ -519,6 +519,140 @@ def run_bandwidth_select(args):
     return 0
 
 
+# ---------------------------------------------------------- out of core (C3) --
+def run_out_of_core(args):
+    """One step = the whole out-of-core job from device-resident points and
+    edge mask: boundary, distances, edge weights, index, then the density
+    raster in 4096 x 4096 tiles streamed to a host array (the raster never
+    exists on the device as a whole: two tile buffers)."""
+    import torch
+
+    import mgpukde_tiled_b200 as mk
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    c = synth.out_of_core(scale=args.scale, seed=3 + rank)
+    dg, eg = mk.Grid.of(c["density_grid"]), mk.Grid.of(c["edge_grid"])
+    h = float(c["h"])
+    tile = int(c["tile"])
+    stream = torch.cuda.current_stream()
+    ctx = mk.Context(local, stream=stream)
+    dx = torch.from_numpy(c["x"]).cuda()
+    dy = torch.from_numpy(c["y"]).cuda()
+    dw = torch.from_numpy(c["w"]).cuda()
+    demask = torch.from_numpy(c["edge_mask"]).cuda()
+    pts = mk.Points.wrap(ctx, dx, dy, dw)
+    em = mk.Raster.wrap(ctx, eg, demask)
+    # tiles land here through the library's copy sink (page-locked: direct 2-D copies)
+    host = torch.empty((dg.nrows, dg.ncols), dtype=torch.float32, pin_memory=True).numpy()
+
+    def step(count=False):
+        mk.mark_boundary(ctx, em)
+        mk.calc_dist2_boundary(ctx, pts, em)
+        ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=count)
+        idx = mk.Index(ctx, pts, h)
+        ev_d = mk.density_stream(ctx, idx, dg, tile, host, count=count)
+        idx.close()
+        return ev_e, ev_d
+
+    ev_e, ev_d = step(count=True)
+    evals = ev_e + ev_d
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (ctx.kernel_launches - l0) / args.steps
+    ntiles = ((dg.nrows + tile - 1) // tile) * ((dg.ncols + tile - 1) // tile)
+    out = {"metric": METRIC, "value": evals * world / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
+           "config": {"workload": f"out_of_core: {len(c['x'])} points (70% from 500 Gaussians, 30% uniform) in "
+                                  f"{dg.ncols}^2, density {dg.ncols}^2 @ cell 1 in {ntiles} tiles of {tile}^2 "
+                                  f"streamed to host memory, edge mask {eg.ncols}^2 @ cell 5, h={h:g}",
+                      "scale": args.scale, "l2": "output streamed through HBM tile buffers to the host"},
+           "evals_per_step": evals, "density_evals": ev_d, "edge_evals": ev_e,
+           "output_bytes": int(host.nbytes), "output_gb_s": host.nbytes / (ms / 1e3) / 1e9,
+           "gpu_launches": launches, "clocks": clocks}
+    print(json.dumps(out))
+    pts.close()
+    em.close()
+    ctx.close()
+    return 0
+
+
+# ------------------------------------------------------------ serving (C4) --
+def run_serving(args):
+    """Poisson arrivals of whole KDE requests into the serving loop, swept
+    over arrival rates; per rate: completed requests/s, evals/s and the p50 /
+    p99 of submit-to-result latency.  The line's value is the evals/s at the
+    highest rate (saturation)."""
+    import torch
+
+    import mgpukde_tiled_b200 as mk
+
+    rank, world, local = env_rank()
+    if world > 1:
+        raise SystemExit("serving runs one server per GPU (replicas only)")
+    torch.cuda.set_device(local)
+    count = max(4, int(round(24 * args.scale)))
+    reqs = synth.serving_requests(count, seed=4)
+    rates = [8.0, 32.0, 128.0, 512.0, 2048.0]
+    rng = np.random.default_rng(7)
+
+    # page-locked result rasters, allocated once outside the arrival process
+    outs = [torch.empty((q["grid"].nrows, q["grid"].ncols), dtype=torch.float32, pin_memory=True).numpy()
+            for q in reqs]
+
+    def submit(srv, q, k=None):
+        return srv.submit(q["x"], q["y"], q["w"], q["h"], mk.Grid.of(q["grid"]), q["mask"],
+                          mk.Grid.of(q["edge_grid"]) if q["edge_grid"] is not None else None, q["edge_mask"],
+                          out=outs[k] if k is not None else None)
+
+    rows = []
+    with mk.Server(local, tile=2048, max_active=8) as srv:
+        for k, q in enumerate(reqs[:min(3, len(reqs))]):  # warm-up: kernels loaded, allocator primed
+            srv.wait(submit(srv, q, k))
+        for rate in rates:
+            arr = np.cumsum(rng.exponential(1.0 / rate, len(reqs)))
+            t0 = time.perf_counter()
+            tickets = []
+            for k, (a, q) in enumerate(zip(arr, reqs)):
+                dt = t0 + a - time.perf_counter()
+                if dt > 0:
+                    time.sleep(dt)
+                tickets.append(submit(srv, q, k))
+            res = [srv.wait(t)[1] for t in tickets]
+            wall = time.perf_counter() - t0
+            lat = np.array([r["total_ms"] for r in res])
+            ev = sum(r["evals"] for r in res)
+            rows.append({"rate_req_s": rate, "completed_req_s": len(res) / wall, "evals_s": ev / wall,
+                         "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                         "mean_queue_ms": float(np.mean([r["queue_ms"] for r in res])), "evals": int(ev)})
+        st = srv.stats()
+    top = rows[-1]
+    out = {"metric": "served evals/s at saturation (mixed-request p50/p99 ms alongside)", "value": top["evals_s"],
+           "unit": "evals/s", "n_gpus": 1, "steps": len(rates), "warmup": 3, "ms_per_step": None,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+           "data": "synthetic (seeded PCG64)",
+           "config": {"workload": f"serving: {count} requests per rate, N lognormal [1e3, 2e6], side U[256, 8192], "
+                                  f"h U[5, 100], edge correction on half; Poisson arrivals",
+                      "tile": 2048, "max_active": 8},
+           "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": rows,
+           "server": {k: st[k] for k in ("ticks", "tiles", "max_batch", "completed")}}
+    print(json.dumps(out))
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -534,6 +668,10 @@ def main():
         return run_reference_arm(args)
     if args.workload == "bandwidth_select":
         return run_bandwidth_select(args)
+    if args.workload == "serving":
+        return run_serving(args)
+    if args.workload == "out_of_core":
+        return run_out_of_core(args)
     return run_mgk(args)
 
 

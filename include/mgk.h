@@ -206,6 +206,32 @@ typedef struct mgk_tile_job {
 } mgk_tile_job;
 int mgk_density_tiles(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, int64_t* evals);
 
+/* Out-of-core density: the raster in row-major tiles of tile_side^2 cells,
+ * each handed to `sink` (on a library thread, in tile order, after its data
+ * is final) while the GPU computes the next ones; mask tiles (optional) come
+ * from `mask_src` (on the calling thread) into an nrows x ncols buffer.
+ * done (optional, one byte per tile, row-major tile order): tiles to skip,
+ * for resuming an interrupted run.  A nonzero return from a callback stops
+ * the run with MGK_ERR_IO; tiles already given to the sink stay valid.
+ * evals (optional): algorithmic pair count of the tiles computed.  The
+ * reference's tile loop is kde_cuda_kdtr_tiled.cu:1233-1517 (GeoTIFF reads
+ * and writes per tile, GeoTIFF.cpp:494-575). */
+typedef int (*mgk_tile_source)(void* user, int64_t tile, int64_t row0, int64_t col0, int64_t nrows,
+                               int64_t ncols, float* mask_out);
+typedef int (*mgk_tile_sink)(void* user, int64_t tile, int64_t row0, int64_t col0, int64_t nrows,
+                             int64_t ncols, const float* density);
+int mgk_density_stream(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t tile_side,
+                       mgk_tile_source mask_src, void* src_user, mgk_tile_sink sink, void* sink_user,
+                       const uint8_t* done, int64_t* evals);
+/* A ready-made sink: copies each tile into a whole host raster;
+ * sink_user points to an mgk_copy_target. */
+typedef struct mgk_copy_target {
+    float* base;                   /* host, nrows x ncols row-major */
+    int64_t ncols;
+} mgk_copy_target;
+int mgk_copy_sink(void* target, int64_t tile, int64_t row0, int64_t col0, int64_t nrows, int64_t ncols,
+                  const float* density);
+
 /* ---- bandwidth selection ---------------------------------------------- */
 
 /* Batched LogLikelihood (kde_cuda_kdtr_tiled.cu:3214-3299) over nh fixed
@@ -224,6 +250,31 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mas
 /* Rule-of-thumb bandwidth (kde_cuda_kdtr_tiled.cu:64-68, 1563-1595), host
  * arithmetic identical to the reference's. */
 float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w);
+
+/* ---- tuning ------------------------------------------------------------ */
+/* Launch-shape settings of a context.  bin_factor: index bin side / h when
+ * mgk_index_build gets bin_size 0 (default 0.75); split_waves: the density
+ * plan splits blocks into work items of at most total / (resident CTAs x
+ * split_waves) candidates (default 8); tile_side: density tile side used by
+ * mgk_kde_raster when its tile argument is 0 (0: the whole raster). */
+typedef struct mgk_tuning {
+    float bin_factor;
+    int32_t split_waves;
+    int64_t tile_side;
+    float density_ms;              /* autotune: time of the chosen bin side on its sample windows */
+    int32_t from_cache;            /* autotune: 1 when read from the cache file */
+} mgk_tuning;
+int mgk_ctx_get_tuning(const mgk_ctx* ctx, mgk_tuning* out);
+int mgk_ctx_set_tuning(mgk_ctx* ctx, const mgk_tuning* t);
+/* Measures the bin factor (0.5, 0.75, 1, 1.25 x h, on four 1024^2 sample
+ * windows of g) and, for rasters above 4096 cells a side, the streamed tile
+ * side (2048, 4096, 8192 over the same central area) for these points and h,
+ * applies them to ctx and appends them to cache_file (optional) under a key
+ * of GPU, point count, h in cells and point density; a later call with a
+ * matching key reads the file instead of measuring.  No reference
+ * counterpart (the reference's launch shapes are compile-time constants). */
+int mgk_autotune(mgk_ctx* ctx, const mgk_points* pts, float h, const mgk_grid* g, const char* cache_file,
+                 mgk_tuning* out);
 
 /* ---- serving loop ------------------------------------------------------ */
 /* A worker thread with its own context on `device` (HBM budget as for

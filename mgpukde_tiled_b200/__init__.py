@@ -7,14 +7,15 @@ Python host side over that ABI; the C++ host driver with the reference's
 command line is `_lib/mgkde_tiled`.
 """
 from ._native import EXPORTS, LIB_PATH, MgkError, MgkGrid, lib  # noqa: F401
-from .kde import (Context, Grid, Index, Points, Raster, calc_dist2_boundary, density_tile,  # noqa: F401
-                  density_tiles, edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
+from .kde import (Context, Grid, Index, Points, Raster, autotune, calc_dist2_boundary, density_tile,  # noqa: F401
+                  get_tuning, set_tuning,
+                  density_stream, density_tiles, edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
                   mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights)
 from .serve import Server  # noqa: F401
 
 __all__ = [
     "Context", "Grid", "Index", "Points", "Raster", "MgkError", "Server", "calc_dist2_boundary", "density_tile",
-    "density_tiles",
+    "density_stream", "density_tiles", "autotune", "get_tuning", "set_tuning",
     "edge_correction_weights", "kde_raster", "log_likelihood_batch", "mark_boundary",
     "mle_fixed_bandwidth", "rule_of_thumb", "unit_edge_weights", "lib",
 ]

@@ -27,7 +27,8 @@ EXPORTS = [
     "mgk_density_tile", "mgk_density_tile_fp64", "mgk_density_tile_noalloc", "mgk_density_tiles", "mgk_loo_loglik_batch",
     "mgk_mle_fixed_bandwidth", "mgk_rule_of_thumb", "mgk_kde_raster",
     "mgk_serve_create", "mgk_serve_submit", "mgk_serve_poll", "mgk_serve_wait", "mgk_serve_stats",
-    "mgk_serve_destroy",
+    "mgk_serve_destroy", "mgk_density_stream", "mgk_copy_sink", "mgk_ctx_get_tuning", "mgk_ctx_set_tuning",
+    "mgk_autotune",
 ]
 
 
@@ -55,6 +56,21 @@ class MgkResult(C.Structure):
 class MgkServeInfo(C.Structure):
     _fields_ = [(k, C.c_uint64) for k in ("ticks", "tiles", "max_batch", "completed", "queued", "active",
                                           "reserved_bytes", "device_bytes")]
+
+
+TILE_SOURCE = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                          C.POINTER(C.c_float))
+TILE_SINK = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int64,
+                        C.POINTER(C.c_float))
+
+
+class MgkCopyTarget(C.Structure):
+    _fields_ = [("base", C.c_void_p), ("ncols", C.c_int64)]
+
+
+class MgkTuning(C.Structure):
+    _fields_ = [("bin_factor", C.c_float), ("split_waves", C.c_int32), ("tile_side", C.c_int64),
+                ("density_ms", C.c_float), ("from_cache", C.c_int32)]
 
 
 class MgkError(RuntimeError):
@@ -115,6 +131,11 @@ def lib():
         "mgk_serve_wait": (I, [P, C.c_uint64, C.c_double, C.POINTER(MgkResult)]),
         "mgk_serve_stats": (I, [P, C.POINTER(MgkServeInfo)]),
         "mgk_serve_destroy": (I, [P]),
+        "mgk_density_stream": (I, [P, P, G, I64, TILE_SOURCE, P, TILE_SINK, P, P, C.POINTER(I64)]),
+        "mgk_copy_sink": (I, [P, I64, I64, I64, I64, I64, C.POINTER(C.c_float)]),
+        "mgk_ctx_get_tuning": (I, [P, C.POINTER(MgkTuning)]),
+        "mgk_ctx_set_tuning": (I, [P, C.POINTER(MgkTuning)]),
+        "mgk_autotune": (I, [P, P, C.c_float, G, C.c_char_p, C.POINTER(MgkTuning)]),
         "mgk_mle_fixed_bandwidth": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(I)]),
         "mgk_rule_of_thumb": (C.c_float, [I64, P, P, P]),
         "mgk_kde_raster": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, P, I64, P, P, C.POINTER(I64)]),

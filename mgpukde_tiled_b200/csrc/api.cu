@@ -603,7 +603,7 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "kde_raster ew");
     }
     // tile loop (kde_cuda_kdtr_tiled.cu:1373-1517): row-major tiles
-    const int64_t T = tile_side > 0 ? tile_side : std::max<int64_t>(dg->ncols, dg->nrows);
+    const int64_t T = tile_side > 0 ? tile_side : (c->tile_side > 0 ? c->tile_side : std::max<int64_t>(dg->ncols, dg->nrows));
     const int64_t tr = std::min<int64_t>(T, dg->nrows), tc = std::min<int64_t>(T, dg->ncols);
     const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_out, tb);

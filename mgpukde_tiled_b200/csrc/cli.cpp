@@ -16,6 +16,12 @@
 // serialized_mode must be 0 (the reference's author advises 0).
 // Extras: --device=D  --tile=N (tile side, cells)  --bin=S (index bin side)
 //         --h=H (fixed bandwidth, overrides h_option 0)  --budget=BYTES
+//         --resume (skip the density tiles listed in <denfn_cuda>.tiles by an
+//         interrupted run and write the rest into its GeoTIFF)
+//         --max-tiles=K (write at most K density tiles, then stop with exit
+//         code 2 so that a later --resume run continues: work in time slices)
+//         --autotune[=CACHE_FILE] (measure the index bin side and the density
+//         tile side for this workload first; fixed h only)
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -51,6 +57,10 @@ struct Args {
     float bin = 0.0f;
     float h_fixed = 0.0f;
     uint64_t budget = 0;
+    bool resume = false;
+    int64_t max_tiles = -1;
+    bool autotune = false;
+    std::string tune_cache;
 };
 
 void usage() {
@@ -76,6 +86,9 @@ bool parse(int argc, char** argv, Args& a) {
             else if (k == "bin") a.bin = (float)std::atof(v.c_str());
             else if (k == "h") a.h_fixed = (float)std::atof(v.c_str());
             else if (k == "budget") a.budget = std::strtoull(v.c_str(), nullptr, 10);
+            else if (k == "resume") a.resume = true;
+            else if (k == "max-tiles") a.max_tiles = std::atoll(v.c_str());
+            else if (k == "autotune") { a.autotune = true; a.tune_cache = v; }
             else { std::printf("***Unknown option %s\n", s.c_str()); return false; }
         } else {
             pos.push_back(s);
@@ -282,12 +295,24 @@ int main(int argc, char** argv) {
         }
         mgk_ctx_synchronize(ctx);
         std::printf("...CalcEdgeCorrectionWeights took %.0f ms\n", ms_since(t1));
+        mgk_tuning tuned{};
+        bool have_tuning = false;
+        if (a.autotune && hpp.empty()) {
+            t1 = Clock::now();
+            if (check(ctx, mgk_autotune(ctx, pts, hfinal, &dg, a.tune_cache.empty() ? nullptr : a.tune_cache.c_str(),
+                                        &tuned), "autotune"))
+                break;
+            have_tuning = true;
+            std::printf("...autotune: bin side %.2f h, tile side %lld%s (%.0f ms)\n", tuned.bin_factor,
+                        (long long)tuned.tile_side, tuned.from_cache ? " (cached)" : "", ms_since(t1));
+        }
         if (check(ctx, mgk_index_build(ctx, pts, hfinal, a.bin, &idx), "index build")) break;
 
         // ---- tiled density (kde_cuda_kdtr_tiled.cu:1146-1517) ----------
         size_t fr = 0, tot = 0;
         cudaMemGetInfo(&fr, &tot);
         int64_t T = a.tile;
+        if (T <= 0 && have_tuning && tuned.tile_side > 0) T = tuned.tile_side;
         if (T <= 0) {  // largest square tile whose mask + output fit in 20% of free memory
             const double cells = 0.2 * (double)fr / 8.0;
             T = (int64_t)std::sqrt(cells);
@@ -295,49 +320,74 @@ int main(int argc, char** argv) {
         }
         const int64_t tr = std::min<int64_t>(T, dg.nrows), tc = std::min<int64_t>(T, dg.ncols);
         std::printf("...TILE_XSIZE=%lld, TILE_YSIZE=%lld\n", (long long)tc, (long long)tr);
+        // Completed tiles are appended to <output>.tiles after their data is
+        // written, so --resume can skip them after an interruption.
+        const int64_t ntx = (dg.ncols + tc - 1) / tc, nty = (dg.nrows + tr - 1) / tr;
+        std::vector<uint8_t> done((size_t)(ntx * nty), 0);
+        const std::string log_fn = a.den_cuda_fn + ".tiles";
+        bool resuming = false;
+        if (a.resume) {
+            if (FILE* lf = std::fopen(log_fn.c_str(), "r")) {
+                long long t = 0;
+                while (std::fscanf(lf, "%lld", &t) == 1)
+                    if (t >= 0 && t < ntx * nty) done[(size_t)t] = 1;
+                std::fclose(lf);
+                resuming = true;
+            }
+        }
         mgk_tiff::TiledWriter wr;
-        if (!wr.open(a.den_cuda_fn, dg.ncols, dg.nrows, dens_gt, true, dg.nodata, 256)) {
+        if (!wr.open(a.den_cuda_fn, dg.ncols, dg.nrows, dens_gt, true, dg.nodata, 256, 0.0f, resuming)) {
             std::printf("***Cannot create %s\n", a.den_cuda_fn.c_str());
             break;
         }
-        float *d_out = nullptr, *d_mask = nullptr;
-        std::vector<float> hbuf((size_t)tr * tc), hmask;
-        cudaMalloc(&d_out, sizeof(float) * tr * tc);
-        if (!dmask_all_valid) cudaMalloc(&d_mask, sizeof(float) * tr * tc);
+        FILE* tile_log = std::fopen(log_fn.c_str(), resuming ? "a" : "w");
+        struct Sink {
+            mgk_tiff::TiledWriter* wr;
+            FILE* log;
+            int64_t max_tiles;
+            int64_t n = 0;
+        } sk{&wr, tile_log, a.max_tiles};
+        auto sink = [](void* u, int64_t t, int64_t r0, int64_t c0, int64_t nr, int64_t nc, const float* d) -> int {
+            Sink* s = static_cast<Sink*>(u);
+            if (s->max_tiles >= 0 && s->n >= s->max_tiles) return 1;  // this run's tile allowance is used up
+            if (!s->wr->write_region(c0, r0, nc, nr, d) || !s->wr->flush()) return 1;
+            if (s->log) {
+                std::fprintf(s->log, "%lld\n", (long long)t);
+                std::fflush(s->log);
+            }
+            std::printf("...wrote tile %lld: rows %lld+%lld cols %lld+%lld\n", (long long)t, (long long)r0,
+                        (long long)nr, (long long)c0, (long long)nc);
+            s->n++;
+            return 0;
+        };
+        struct Src {
+            const float* mask;
+            int64_t ncols;
+        } src{dmask_all_valid ? nullptr : dmask.data(), dg.ncols};
+        auto source = [](void* u, int64_t, int64_t r0, int64_t c0, int64_t nr, int64_t nc, float* out) -> int {
+            const Src* s = static_cast<const Src*>(u);
+            for (int64_t r = 0; r < nr; r++)
+                std::memcpy(out + r * nc, s->mask + (r0 + r) * s->ncols + c0, sizeof(float) * nc);
+            return 0;
+        };
         t1 = Clock::now();
         int64_t evals_total = 0;
-        bool ok = d_out && (dmask_all_valid || d_mask);
-        int tile_no = 0;
-        for (int64_t r0 = 0; ok && r0 < dg.nrows; r0 += tr) {
-            for (int64_t c0 = 0; ok && c0 < dg.ncols; c0 += tc) {
-                const int64_t nr = std::min<int64_t>(tr, dg.nrows - r0), nc = std::min<int64_t>(tc, dg.ncols - c0);
-                if (!dmask_all_valid) {
-                    hmask.resize((size_t)nr * nc);
-                    for (int64_t r = 0; r < nr; r++)
-                        std::memcpy(&hmask[r * nc], &dmask[(r0 + r) * dg.ncols + c0], sizeof(float) * nc);
-                    cudaMemcpy(d_mask, hmask.data(), sizeof(float) * nr * nc, cudaMemcpyHostToDevice);
-                }
-                int64_t ev = 0;
-                if (check(ctx, mgk_density_tile(ctx, idx, &dg, r0, c0, nr, nc, d_mask, d_out, &ev), "density")) {
-                    ok = false;
-                    break;
-                }
-                evals_total += ev;
-                cudaMemcpy(hbuf.data(), d_out, sizeof(float) * nr * nc, cudaMemcpyDeviceToHost);
-                if (!wr.write_region(c0, r0, nc, nr, hbuf.data())) {
-                    std::printf("***Unable to write tile in GeoTIFF!\n");
-                    ok = false;
-                    break;
-                }
-                wr.flush();
-                std::printf("...working on tile %d: rows %lld+%lld cols %lld+%lld, %lld kernel evaluations\n",
-                            ++tile_no, (long long)r0, (long long)nr, (long long)c0, (long long)nc, (long long)ev);
-            }
-        }
-        cudaFree(d_out);
-        if (d_mask) cudaFree(d_mask);
+        const int dst = mgk_density_stream(ctx, idx, &dg, T, dmask_all_valid ? nullptr : +source,
+                                           &src, +sink, &sk, done.data(), &evals_total);
+        if (tile_log) std::fclose(tile_log);
         wr.close();
-        if (!ok) break;
+        if (dst != MGK_OK) {
+            if (dst == MGK_ERR_IO && a.max_tiles >= 0 && sk.n >= a.max_tiles) {
+                std::printf("...stopped after %lld tiles (--max-tiles); rerun with --resume to continue\n",
+                            (long long)sk.n);
+                rc = 2;
+            } else {
+                std::printf("***density: %s (%s); rerun with --resume to continue\n", mgk_status_string(dst),
+                            mgk_ctx_last_error(ctx));
+            }
+            break;
+        }
+        std::remove(log_fn.c_str());  // complete: nothing to resume
         std::printf("KernelDensityEstimation took %.0f ms (%lld kernel evaluations)\n", ms_since(t1),
                     (long long)evals_total);
 

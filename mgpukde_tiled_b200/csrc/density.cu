@@ -20,15 +20,16 @@
 //    a common quantum, so dx = (xh - cxh) + (xl - cxl) is exact as a pair and
 //    a = dx^2 k2 is formed with error-free float products (no FP64, no
 //    conversions); E = ex2(-a_hi) (1 - a_lo ln2).  Row entries also carry the
-//    cutoff threshold T_i = cut - b_i, a flag marking rows where some column
-//    lies within a 4e-6 (log2 units) band of the cutoff, and each warp's
-//    sub-block gets an exact-enough rectangle-vs-disc test.
+//    cutoff threshold G_i = 2^-cut / 2^-b_i (a_j < cut - b_i <=> E_j > G_i),
+//    a flag marking rows where some column lies within a 4e-6 (log2 units)
+//    band of the cutoff, and each warp's sub-block gets an exact-enough
+//    rectangle-vs-disc test.
 //  phase B (each warp, its processed points): per cell one compare
-//    a_j < T_i and a predicated FFMA part += E_j F_i.  Rows flagged as
+//    E_j > G_i and a predicated FFMA part += E_j F_i.  Rows flagged as
 //    ambiguous are re-decided with the exact FP64 test of the oracle, so the
 //    summed pair set is exactly the reference's.
 //
-// Accumulation: FP32 partial sums over 8 points per cell, added into a
+// Accumulation: FP32 partial sums over 16 points per cell, added into a
 // Kahan-compensated FP32 accumulator; the epilogue forms (s - c) times the
 // kernel normalisation in FP64.  Heavy blocks are split into work items whose
 // FP64 partials are merged in a fixed order, so results are bitwise
@@ -73,7 +74,8 @@ struct DParams {
     int qexp;
     // fixed-h constants
     double h2, k0, cut_d2, reach;
-    float k2h, k2l, cutlh, cutll, cutf, epsd2;
+    float k2h, k2l, cutf, epsd2;
+    float gcut;  // 2^-(cutoff in log2 units): the in-cutoff threshold on E_j F'_i
     unsigned long long* evals;
     unsigned long long* err;
 };
@@ -181,6 +183,12 @@ __device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, floa
 __device__ __forceinline__ float exp2_pair(float ah, float al) {
     const float e = mgk_ex2(-ah);
     return __fmaf_rn(__fmul_rn(-al, MGK_LN2F), e, e);
+}
+
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
 }
 
 __device__ __forceinline__ float rsqrt_approx(float x) {
@@ -393,10 +401,11 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     const int i = ka + 8 * c;
                     float bh, bl, d2;
                     exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
-                    const float T = __fadd_rn(__fsub_rn(P.cutlh, bh), __fsub_rn(P.cutll, bl));
-                    rF[i] = __fmul_rn(r.wk, exp2_pair(bh, bl));
-                    // a_j < T_i  <=>  E_j > G_i (2^-x is decreasing); G = inf for rows off the disc
-                    rG[i] = mgk_ex2(-T);
+                    const float fb = exp2_pair(bh, bl);
+                    rF[i] = __fmul_rn(r.wk, fb);
+                    // a_j < cutl - b_i  <=>  E_j > G_i = 2^-cutl / 2^-b_i (2^-x is decreasing);
+                    // G = inf for rows off the disc (2^-b_i flushed to zero)
+                    rG[i] = __fmul_rn(P.gcut, rcp_approx(fb));
                     const float s2 = cutf - d2;
                     const unsigned a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2 ? 3u : 0u);
                     const unsigned sh = (ka + 8 * c) & 31;
@@ -513,7 +522,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     if (COUNT) cnt += __popc(inm & valid);
                 }
                 pc++;
-                if ((pc & 7u) == 0) {
+                if ((pc & 15u) == 0) {
 #pragma unroll
                     for (int k = 0; k < 16; k++) {
                         kahan_add(acc_s[k], acc_c[k], part[k]);
@@ -714,8 +723,7 @@ void fill_params(DParams& P, const mgk_index* idx, const mgk_grid* g, int64_t ro
     P.k2l = (float)(k2 - (double)P.k2h);
     // log2-unit cutoff: 9 h^2 k2 for fixed h; 4.5 log2(e) for per-point h
     const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
-    P.cutlh = (float)cutl;
-    P.cutll = (float)(cutl - (double)P.cutlh);
+    P.gcut = (float)std::exp2(-cutl);
     P.cutf = (float)idx->cut_d2;
     // ambiguity band in d^2 units: |a - T| < kAmbEps  <=>  |dx^2 - s^2| < kAmbEps / k2 (x2 margin)
     P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
@@ -733,14 +741,14 @@ struct TilePlan {
     int32_t nslots = 0;
 };
 
-void plan_tile(const int64_t* counts, int nbx_t, int nby_t, int sm_count, int job, TilePlan& T) {
+void plan_tile(const int64_t* counts, int nbx_t, int nby_t, int sm_count, int waves, int job, TilePlan& T) {
     const int nblk = nbx_t * nby_t;
     T.nbx_t = nbx_t;
     T.nby_t = nby_t;
     int64_t total = 0;
     for (int b = 0; b < nblk; b++) total += counts[b];
     const int64_t slots_resident = (int64_t)sm_count * 2;
-    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
+    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * waves));
     K = (K + kMB - 1) / kMB * kMB;
     T.items.reserve(nblk + 16);
     for (int b = 0; b < nblk; b++) {
@@ -793,7 +801,7 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     mgk_free(ctx, d_counts, sizeof(int64_t) * nblk);
     if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
     TilePlan T;
-    plan_tile(counts.data(), nbx_t, nby_t, ctx->sm_count, 0, T);
+    plan_tile(counts.data(), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
     sort_items(T.items);
     std::vector<Item>& items = T.items;
     const int32_t nslots = T.nslots;
@@ -905,7 +913,7 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     for (int j = 0; j < njobs; j++) {
         if (!nbx[j]) continue;
         TilePlan T;
-        plan_tile(counts.data() + off[j], nbx[j], nby[j], ctx->sm_count, j, T);
+        plan_tile(counts.data() + off[j], nbx[j], nby[j], ctx->sm_count, ctx->split_waves, j, T);
         slot0[j] = nslots;
         for (size_t b = 0; b < T.split_blocks.size(); b++)
             merges.push_back(make_int4(j, T.split_blocks[b], T.split_begin[b], T.split_begin[b + 1]));
@@ -1053,40 +1061,8 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     int32_t* d_sbeg = reinterpret_cast<int32_t*>(base + kNaOffSplitBegin);
     cudaStream_t s = ctx->stream;
 
-    DParams P{};
-    P.xll = g->xll;
-    P.yll = g->yll;
-    P.cs = g->cs;
-    P.g_nrows = g->nrows;
-    P.row0 = row0;
-    P.col0 = col0;
-    P.nr = nr;
-    P.nc = nc;
-    P.nodata = g->nodata;
-    P.mask = d_mask;
-    P.out = d_out;
-    P.pts = idx->pts;
-    P.bin_start = idx->bin_start;
-    P.ox = idx->ox;
-    P.oy = idx->oy;
-    P.inv_side = 1.0 / idx->side;
-    P.nbx = idx->nbx;
-    P.nby = idx->nby;
-    P.qexp = idx->qexp;
-    P.h2 = idx->h2;
-    P.k0 = idx->k0;
-    P.cut_d2 = idx->cut_d2;
-    P.reach = idx->reach;
-    {
-        const double k2 = idx->k2;
-        P.k2h = (float)k2;
-        P.k2l = (float)(k2 - (double)P.k2h);
-        const double cutl = idx->varh ? MGK_CUT * 0.5 * MGK_LOG2E : idx->cut_d2 * k2;
-        P.cutlh = (float)cutl;
-        P.cutll = (float)(cutl - (double)P.cutlh);
-        P.cutf = (float)idx->cut_d2;
-        P.epsd2 = (float)(2.0 * (double)kAmbEps / k2);
-    }
+    DParams P;
+    fill_params(P, idx, g, row0, col0, nr, nc, d_mask, d_out);
     P.evals = nullptr;
     P.err = ctx->d_counter + 7;
     P.scratch = reinterpret_cast<double*>(base + kNaOffSlots);
@@ -1101,7 +1077,7 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     int64_t total = 0;
     for (int b = 0; b < nblk; b++) total += g_na_counts[b];
     const int64_t slots_resident = (int64_t)ctx->sm_count * MGK_DENSITY_MIN_CTAS;
-    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * 8));
+    int64_t K = std::max<int64_t>(2048, total / std::max<int64_t>(1, slots_resident * ctx->split_waves));
     K = (K + kMB - 1) / kMB * kMB;
     for (;;) {  // grow the item size until the split items fit the fixed slots
         int64_t need = 0;

@@ -259,7 +259,7 @@ int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float b
     // 3h plus a margin: 9 h^2 is formed from the float square, which may
     // exceed h^2 by a relative 2^-24
     idx->reach = 3.0 * (double)hmax * (1.0 + 1e-6);
-    double side = bin_size > 0.0f ? (double)bin_size : 0.75 * (double)hmax;
+    double side = bin_size > 0.0f ? (double)bin_size : (double)ctx->bin_factor * (double)hmax;
     const double ext = std::max(xmax - xmin, ymax - ymin);
     side = std::max(side, ext / 4096.0);
     if (!(side > 0.0)) side = 1.0;

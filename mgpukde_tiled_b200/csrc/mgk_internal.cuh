@@ -40,6 +40,10 @@ struct mgk_ctx {
     float last_density_ms = 0.0f;
     int64_t last_loo_evals[2] = {0, 0};  // edge and LOO evals of the last LOO batch run
     float last_loo_ms = 0.0f;
+    // tuning (mgk_autotune / mgk_ctx_set_tuning)
+    float bin_factor = 0.75f;  // default index bin side / h
+    int split_waves = 8;       // density work items per resident CTA slot
+    int64_t tile_side = 0;     // streamed tile side (0: whole raster when it fits)
 };
 
 #define MGK_COUNT_LAUNCH(ctx, k) ((ctx)->launches += (k))

@@ -335,8 +335,10 @@ class TiledWriter {
     TiledWriter& operator=(const TiledWriter&) = delete;
     ~TiledWriter() { close(); }
 
+    // resume: reopen an existing file of the same layout (written by an
+    // earlier, interrupted run) instead of creating and pre-filling it.
     bool open(const std::string& path, int64_t ncols, int64_t nrows, const double gt[6],
-              bool has_nodata, double nodata, int tile = 256, float fill = 0.0f) {
+              bool has_nodata, double nodata, int tile = 256, float fill = 0.0f, bool resume = false) {
         close();
         ncols_ = ncols;
         nrows_ = nrows;
@@ -346,8 +348,7 @@ class TiledWriter {
         const uint64_t tile_bytes = (uint64_t)tile * tile * 4;
         const uint64_t data_bytes = tile_bytes * (uint64_t)(nbx_ * nby_);
         big_ = data_bytes > 0xF0000000ull;
-        f_ = fopen(path.c_str(), "w+b");
-        if (!f_) return false;
+        f_ = nullptr;
         // Layout: header | tag payloads | tile offsets | tile counts | IFD | tile data
         std::vector<uint8_t> head;
         auto put = [&](uint64_t v, int n) {
@@ -429,6 +430,22 @@ class TiledWriter {
                 for (int i = 0; i < osz; i++) head[toff_off + t * osz + i] = (uint8_t)(o >> (8 * i));
             }
         }
+        const uint64_t total = data_off_ + ntiles * tile_bytes;
+        if (resume) {
+            f_ = fopen(path.c_str(), "r+b");
+            if (f_) {
+                std::vector<uint8_t> have(head.size());
+                const bool same = fseeko(f_, 0, SEEK_END) == 0 && (uint64_t)ftello(f_) == total &&
+                                  fseeko(f_, 0, SEEK_SET) == 0 &&
+                                  fread(have.data(), 1, have.size(), f_) == have.size() && have == head;
+                if (same) return true;
+                fclose(f_);
+                f_ = nullptr;
+            }
+            return false;  // missing, or not the file this run would write
+        }
+        f_ = fopen(path.c_str(), "w+b");
+        if (!f_) return false;
         if (fwrite(head.data(), 1, head.size(), f_) != head.size()) return false;
         // pre-fill tile data
         std::vector<float> fillbuf((size_t)tile * tile, fill);

@@ -14,7 +14,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
-from ._native import MgkError, MgkGrid, MgkTileJob, lib
+from ._native import TILE_SINK, TILE_SOURCE, MgkCopyTarget, MgkError, MgkGrid, MgkTileJob, MgkTuning, lib
 
 
 def _ptr(a):
@@ -267,6 +267,74 @@ def density_tiles(ctx: Context, jobs, count=False):
     ev = (C.c_int64 * max(len(jobs), 1))()
     ctx.check(lib().mgk_density_tiles(ctx.handle, len(jobs), arr, ev if count else None))
     return [int(ev[k]) for k in range(len(jobs))] if count else None
+
+
+def density_stream(ctx: Context, index: Index, grid: Grid, tile: int, sink, mask=None, done=None, count=False):
+    """Out-of-core density: sink(tile_id, row0, col0, tile_array) receives
+    every finished tile (a float32 nrows x ncols view, valid during the call;
+    return False to stop), or sink is a whole host float32 array that the
+    library's own copy sink fills; mask is None, a full host array, or
+    mask(tile_id, row0, col0, nrows, ncols) -> array.  done: optional bool
+    per tile (row-major tile order) to skip.  Returns the eval count when
+    count is set."""
+    def src_cb(user, t, r0, c0, nr, nc, buf):
+        try:
+            m = mask[r0:r0 + nr, c0:c0 + nc] if isinstance(mask, np.ndarray) else mask(t, r0, c0, nr, nc)
+            dst = np.ctypeslib.as_array(buf, shape=(nr * nc,)).reshape(nr, nc)
+            dst[...] = m
+            return 0
+        except Exception:  # noqa: BLE001 - reported to the library as a failed read
+            return 1
+
+    def sink_cb(user, t, r0, c0, nr, nc, buf):
+        try:
+            arr = np.ctypeslib.as_array(buf, shape=(nr * nc,)).reshape(nr, nc)
+            return 0 if sink(int(t), int(r0), int(c0), arr) is not False else 1
+        except Exception:  # noqa: BLE001 - reported to the library as a failed write
+            return 1
+
+    src = TILE_SOURCE(src_cb) if mask is not None else TILE_SOURCE()
+    target = None
+    if isinstance(sink, np.ndarray):
+        if sink.dtype != np.float32 or not sink.flags.c_contiguous or sink.shape != (grid.nrows, grid.ncols):
+            raise ValueError("sink array must be a C-contiguous float32 nrows x ncols array")
+        target = MgkCopyTarget(sink.ctypes.data, grid.ncols)
+        snk = C.cast(lib().mgk_copy_sink, TILE_SINK)
+    else:
+        snk = TILE_SINK(sink_cb)
+    g = grid.c()
+    d = None if done is None else np.ascontiguousarray(done, dtype=np.uint8)
+    ev = C.c_int64()
+    ctx.check(lib().mgk_density_stream(ctx.handle, index._h, C.byref(g), int(tile), src, None, snk,
+                                       C.cast(C.pointer(target), C.c_void_p) if target is not None else None, _ptr(d),
+                                       C.byref(ev) if count else None))
+    return ev.value if count else None
+
+
+def _tuning_dict(t):
+    return {"bin_factor": float(t.bin_factor), "split_waves": int(t.split_waves), "tile_side": int(t.tile_side),
+            "density_ms": float(t.density_ms), "from_cache": bool(t.from_cache)}
+
+
+def autotune(ctx: Context, points: Points, h: float, grid: Grid, cache_file: str | None = None) -> dict:
+    """Measures and applies the index bin factor and the streamed tile side
+    for this workload (cached in cache_file when given)."""
+    t = MgkTuning()
+    g = grid.c()
+    ctx.check(lib().mgk_autotune(ctx.handle, points._h, float(h), C.byref(g),
+                                 cache_file.encode() if cache_file else None, C.byref(t)))
+    return _tuning_dict(t)
+
+
+def get_tuning(ctx: Context) -> dict:
+    t = MgkTuning()
+    ctx.check(lib().mgk_ctx_get_tuning(ctx.handle, C.byref(t)))
+    return _tuning_dict(t)
+
+
+def set_tuning(ctx: Context, bin_factor=0.75, split_waves=8, tile_side=0):
+    t = MgkTuning(float(bin_factor), int(split_waves), int(tile_side), 0.0, 0)
+    ctx.check(lib().mgk_ctx_set_tuning(ctx.handle, C.byref(t)))
 
 
 def log_likelihood_batch(ctx: Context, points: Points, raster: Raster | None, hgrid):

@@ -23,6 +23,16 @@ def _p(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
 
 
+def _host_raster(nrows, ncols):
+    """A page-locked host raster when torch can provide one (device-to-host
+    copies into it run at full link speed), else an ordinary array."""
+    try:
+        import torch
+        return torch.empty((nrows, ncols), dtype=torch.float32, pin_memory=True).numpy()
+    except Exception:  # noqa: BLE001 - no CUDA host allocator: pageable memory works too
+        return np.empty((nrows, ncols), np.float32)
+
+
 class Ticket:
     def __init__(self, tid, out, keep):
         self.id = tid
@@ -41,7 +51,7 @@ class Server:
                out=None) -> Ticket:
         x, y, w, mask, edge_mask = _f32(x), _f32(y), _f32(w), _f32(mask), _f32(edge_mask)
         if out is None:
-            out = np.empty((grid.nrows, grid.ncols), np.float32)
+            out = _host_raster(grid.nrows, grid.ncols)
         edge = edge_mask is not None
         req = MgkRequest(len(x), _p(x), _p(y), _p(w), float(h), grid.c(), _p(mask), int(edge),
                          edge_grid.c() if edge else Grid(1, 1, 0.0, 0.0, 1.0).c(), _p(edge_mask), _p(out))

@@ -168,6 +168,31 @@ def out_of_core(scale=1.0, seed=3):
                 edge_grid=eg, edge_mask=rasterize_polygon(poly, eg), edge=True, tile=4096)
 
 
+def serving_requests(count, seed=4, n_lo=1_000, n_hi=2_000_000, side_lo=256, side_hi=8192):
+    """The serving stream's requests: point count lognormal (median 3e4,
+    sigma 1.5) clipped to [n_lo, n_hi], Gaussian-mixture points with a
+    per-request seed, square raster side uniform in [side_lo, side_hi] at
+    cell 1, h uniform in [5, 100] cells, edge correction (polygon mask at
+    cell 4) for half of them; lognormal(0, 0.5) weights."""
+    r = _rng(seed)
+    out = []
+    for k in range(count):
+        n = int(np.clip(r.lognormal(np.log(3e4), 1.5), n_lo, n_hi))
+        side = int(r.integers(side_lo, side_hi + 1))
+        h = float(r.uniform(5.0, 100.0))
+        edge = bool(r.random() < 0.5)
+        x, y = mixture_points(n, 10, float(side), side / 40.0, side / 8.0, seed * 1000 + k)
+        w = lognormal_weights(n, seed * 1000 + k + 500)
+        g = Grid(side, side, 0.0, 0.0, 1.0)
+        q = dict(x=x, y=y, w=w, h=h, grid=g, mask=None, edge_grid=None, edge_mask=None)
+        if edge:
+            eg = Grid(max(1, side // 4), max(1, side // 4), 0.0, 0.0, 4.0)
+            q["edge_grid"] = eg
+            q["edge_mask"] = rasterize_polygon(star_polygon(float(side), seed * 1000 + k + 700), eg)
+        out.append(q)
+    return out
+
+
 def density_mask_window(poly, g: Grid, r0, c0, nr, nc):
     """Polygon mask for a window of a (possibly huge) density grid."""
     sub = Grid(nc, nr, g.xll + c0 * g.cs, g.yll + (g.nrows - r0 - nr) * g.cs, g.cs, g.nodata)

@@ -38,3 +38,40 @@ def test_cli_mode0_runs(tmp_path):
     assert p.returncode == 0, p.stdout[-2000:]
     r = tiff.read(str(tmp_path / "b.tif"))
     assert r.data.shape == (200, 200) and np.isfinite(r.data).all() and (r.data > 0).any()
+
+
+def test_cli_resume_after_a_tile_limit(tmp_path):
+    """--max-tiles stops a run after K density tiles (exit code 2, tiles
+    logged); --resume computes only the rest; the GeoTIFF equals an
+    uninterrupted run's bit for bit."""
+    write_case_files(str(tmp_path), "poly_fixed")
+    args = "1 p.csv e.tif d.tif 0 1 1 1 0 1 1 a.tif b.tif 0 --tile=32".split()
+    full = subprocess.run([CLI] + args, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert full.returncode == 0, full.stdout[-2000:]
+    ref = tiff.read(str(tmp_path / "b.tif")).data
+    os.rename(tmp_path / "b.tif", tmp_path / "full.tif")
+    p1 = subprocess.run([CLI] + args + ["--max-tiles=3"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert p1.returncode == 2, p1.stdout[-2000:]
+    logged = [int(v) for v in open(tmp_path / "b.tif.tiles").read().split()]
+    assert logged == [0, 1, 2]
+    p2 = subprocess.run([CLI] + args + ["--resume"], cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert p2.returncode == 0, p2.stdout[-2000:]
+    wrote = [int(line.split()[2].rstrip(":")) for line in p2.stdout.splitlines() if line.startswith("...wrote tile")]
+    assert wrote and not set(wrote) & set(logged)
+    assert not os.path.exists(tmp_path / "b.tif.tiles")
+    got = tiff.read(str(tmp_path / "b.tif")).data
+    assert np.array_equal(got.view(np.uint32), ref.view(np.uint32))
+
+
+def test_cli_autotune_keeps_parity(tmp_path):
+    g = write_case_files(str(tmp_path), "redwood_h0")
+    ref = oracle_run(load("redwood_h0"))
+    args = "1 p.csv e.tif d.tif 0 1 0 1 0 1 1 a.tif b.tif 0 --autotune=tune.txt".split()
+    for k in range(2):
+        p = subprocess.run([CLI] + args, cwd=tmp_path, capture_output=True, text=True, timeout=600)
+        assert p.returncode == 0, p.stdout[-2000:]
+        assert "...autotune: bin side" in p.stdout and (("(cached)" in p.stdout) == (k == 1))
+        den = tiff.read(str(tmp_path / "b.tif")).data
+        nd = g["density_mask"] == g["dg"].nodata
+        rel = np.abs(den[~nd] - ref["density"][~nd]) / np.maximum(np.abs(ref["density"][~nd]), 1e-300)
+        assert rel.max() <= 1e-6
