@@ -179,7 +179,7 @@ int mgk_density_tile_fp64(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g,
  * in which cudaMalloc/cudaFree, which may synchronise the device, are not
  * allowed).  It calls no cudaMalloc, cudaFree or other allocating routine:
  * its scratch (block counts, work items, FP64 partial sums of split blocks)
- * lives in one fixed file-scope device array of about 12.4 MiB that every GPU
+ * lives in one fixed file-scope device array of about 12.3 MiB that every GPU
  * loading the library holds until the process exits.  Limit: tiles of at most
  * 4096 x 4096 cells (MGK_ERR_INVALID beyond).  The first call on a device looks
  * up that array's device address (once per device); make that first call

@@ -44,7 +44,9 @@
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kBlk = 64;        // cells per CTA block side
+constexpr int kBR = 64;         // cell rows of a CTA block
+constexpr int kBC = 128;        // cell columns of a CTA block
+constexpr int kCells = kBR * kBC;
 constexpr int kMB = 32;         // points per mini-batch
 constexpr int kStage64 = 512;   // points staged per batch by the FP64 form
 constexpr float kAmbEps = 4e-6f;
@@ -64,7 +66,7 @@ struct DParams {
     float nodata;
     const float* mask;
     float* out;
-    double* scratch;  // [slot][kBlk*kBlk]
+    double* scratch;  // [slot][kCells]
     const Item* items;
     // index
     const MgkPt* pts;
@@ -99,10 +101,10 @@ struct BlockGeom {
 
 __device__ __forceinline__ BlockGeom block_geom(const DParams& P, int bxi, int byi) {
     BlockGeom G;
-    G.r0 = P.row0 + (int64_t)byi * kBlk;
-    G.c0 = P.col0 + (int64_t)bxi * kBlk;
-    G.nrow = (int)mgk_min64(kBlk, P.row0 + P.nr - G.r0);
-    G.ncol = (int)mgk_min64(kBlk, P.col0 + P.nc - G.c0);
+    G.r0 = P.row0 + (int64_t)byi * kBR;
+    G.c0 = P.col0 + (int64_t)bxi * kBC;
+    G.nrow = (int)mgk_min64(kBR, P.row0 + P.nr - G.r0);
+    G.ncol = (int)mgk_min64(kBC, P.col0 + P.nc - G.c0);
     const double x_lo = mgk_cell_x(P.xll, P.cs, G.c0), x_hi = mgk_cell_x(P.xll, P.cs, G.c0 + G.ncol - 1);
     const double y_hi = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0);
     const double y_lo = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + G.nrow - 1);
@@ -204,13 +206,13 @@ __device__ __forceinline__ void fma_if_less(float& acc, float a, float t, float 
         : "f"(a), "f"(t), "f"(e), "f"(f));
 }
 
-// Does some column of a regular 64-column block lie within the ambiguity
+// Does some column of a regular 128-column block lie within the ambiguity
 // band of a row?  For the row, in-disc columns satisfy dx^2 < s2 with
 // s2 = 9h^2 - dy^2 (squared half-chord); the FP32 decision a_j < T_i can
 // differ from the exact one only for columns with |dx^2 - s2| < eps_d2, i.e.
 // within eps_d2 / (2 s) of a crossing x = px +- s.  pc0 = (px - cx_0) / cs in
 // columns; margins cover the float error of the crossing positions.  Returns
-// two bits: bit 0 for columns 0-31 (warp column half 0), bit 1 for 32-63.
+// two bits: bit 0 for columns 0-63 (warp column half 0), bit 1 for 64-127.
 __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, float inv_cs) {
     const float r = rsqrt_approx(fmaxf(s2, 1e-30f));
     const float sc = s2 * r * inv_cs;  // half-chord in columns (0 when s2 <= 0)
@@ -219,9 +221,9 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
     if (wc > 0.25f) return 3u;
     const float fp = pc0 + sc, fm = pc0 - sc;
     const bool np = fabsf(fp - rintf(fp)) < wc, nm = fabsf(fm - rintf(fm)) < wc;
-    // a crossing near column position f concerns half 0 if f <= 32, half 1 if f >= 31
-    const unsigned b0 = (np && fp >= -1.0f && fp <= 32.0f) || (nm && fm >= -1.0f && fm <= 32.0f);
-    const unsigned b1 = (np && fp >= 31.0f && fp <= 64.0f) || (nm && fm >= 31.0f && fm <= 64.0f);
+    // a crossing near column position f concerns half 0 if f <= 64, half 1 if f >= 63
+    const unsigned b0 = (np && fp >= -1.0f && fp <= 64.0f) || (nm && fm >= -1.0f && fm <= 64.0f);
+    const unsigned b1 = (np && fp >= 63.0f && fp <= 128.0f) || (nm && fm >= 63.0f && fm <= 128.0f);
     return b0 | (b1 << 1);
 }
 
@@ -250,50 +252,58 @@ __device__ __forceinline__ int next_batch(const DParams& P, const BlockGeom& G, 
     return 0;
 }
 
-// Dynamic shared memory of k_density (bytes); factor tables are padded to a
-// row stride of 72 float2 so that phase-A stores of 4 points hit distinct banks.
-constexpr int kFStride = 72;  // floats; 72 = 8 (mod 32): phase-A stores of 4 points hit 32 banks
+// Dynamic shared memory of k_density (bytes): the staged points, the factor
+// tables (row strides of 136 and 72 floats, both 8 mod 32, so that the
+// phase-A stores of 4 points hit distinct banks) and the per-cell Kahan
+// accumulators (sum and compensation, 8192 floats each).
+constexpr int kFStrideC = 136;  // column table, floats per point
+constexpr int kFStride = 72;    // row tables, floats per point
 constexpr size_t kSmemStage = 2 * kMB * sizeof(MgkPt);
-constexpr size_t kSmemTab = (size_t)kMB * kFStride * sizeof(float);
-constexpr size_t kDensitySmem = kSmemStage + 3 * kSmemTab;
+constexpr size_t kSmemColTab = (size_t)kMB * kFStrideC * sizeof(float);
+constexpr size_t kSmemRowTab = (size_t)kMB * kFStride * sizeof(float);
+constexpr size_t kSmemKahan = (size_t)kCells * sizeof(float);
+constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab + 2 * kSmemKahan;
 
 #ifndef MGK_DENSITY_MIN_CTAS
-#define MGK_DENSITY_MIN_CTAS 3  // resident CTAs per SM the register budget is sized for
+#define MGK_DENSITY_MIN_CTAS 2  // resident CTAs per SM (shared memory allows two)
 #endif
 
 // One work item: the gather of the candidate range [it.k0, it.k1) of one
-// 64 x 64 block (the body of k_density and of the multi-job k_density_jobs).
+// 64 x 128 block (the body of k_density and of the multi-job k_density_jobs).
 template <bool VARH, bool COUNT>
 __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     extern __shared__ __align__(128) unsigned char dsm[];
-    MgkPt* stage = reinterpret_cast<MgkPt*>(dsm);                                  // [2][kMB]
-    float* colE = reinterpret_cast<float*>(dsm + kSmemStage);                 // [kMB][kFStride] E_j = 2^-a_j
-    float* rowF = reinterpret_cast<float*>(dsm + kSmemStage + kSmemTab);      // [kMB][kFStride] F_i = w e 2^-b_i
-    float* rowG = reinterpret_cast<float*>(dsm + kSmemStage + 2 * kSmemTab);  // [kMB][kFStride] G_i = 2^-T_i
+    MgkPt* stage = reinterpret_cast<MgkPt*>(dsm);                                    // [2][kMB]
+    float* colE = reinterpret_cast<float*>(dsm + kSmemStage);                   // [kMB][kFStrideC] E_j
+    float* rowF = reinterpret_cast<float*>(dsm + kSmemStage + kSmemColTab);     // [kMB][kFStride] F_i
+    float* rowG = reinterpret_cast<float*>(dsm + kSmemStage + kSmemColTab + kSmemRowTab);  // [kMB][kFStride] G_i
+    // Kahan sum / compensation of the thread's 32 cells: float4 [8][256] each
+    float4* ksum = reinterpret_cast<float4*>(dsm + kSmemStage + kSmemColTab + 2 * kSmemRowTab);
+    float4* kcmp = ksum + kCells / 4;
     __shared__ __align__(8) uint64_t mbar[2];
     __shared__ __align__(16) unsigned long long rowflag[kMB][2];  // per column half: 64 row bits
     __shared__ unsigned char procmask[kMB];  // warp w processes the point
     __shared__ unsigned char fullmask[kMB];  // every cell of warp w's sub-block is inside the cutoff
-    __shared__ float s_cxh[kBlk], s_cxl[kBlk], s_cyh[kBlk], s_cyl[kBlk], s_cxg[kBlk], s_cyg[kBlk];
+    __shared__ float s_cxh[kBC], s_cxl[kBC], s_cxg[kBC], s_cyh[kBR], s_cyl[kBR], s_cyg[kBR];
     __shared__ int s_abort;
 
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*32..
-    const int tr = lane >> 3, tc = lane & 7;  // lane micro-tile: rows tr*4.., cols tc*4..
+    const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*64..
+    const int tr = lane >> 3, tc = lane & 7;  // lane micro-tile: rows tr*4.. (4), cols tc*8.. (8)
 
     // cell centres of the block: global floats and their quantum split
     bool regular = true;
-    if (tid < kBlk) {
+    if (tid < kBC) {
         const float cx = mgk_cell_x(P.xll, P.cs, G.c0 + tid);
         s_cxg[tid] = cx;
         mgk_qsplit(cx, P.qexp, s_cxh[tid], s_cxl[tid]);
         const float cx0 = mgk_cell_x(P.xll, P.cs, G.c0);
         regular = ((double)cx - (double)cx0) == (double)tid * P.cs;
-    } else if (tid < 2 * kBlk) {
-        const float cy = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + tid - kBlk);
-        s_cyg[tid - kBlk] = cy;
-        mgk_qsplit(cy, P.qexp, s_cyh[tid - kBlk], s_cyl[tid - kBlk]);
+    } else if (tid < kBC + kBR) {
+        const float cy = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + tid - kBC);
+        s_cyg[tid - kBC] = cy;
+        mgk_qsplit(cy, P.qexp, s_cyh[tid - kBC], s_cyl[tid - kBC]);
     }
     if (tid == 0) {
         mbar_init(&mbar[0], 1);
@@ -301,33 +311,38 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         fence_mbar_init();
         s_abort = 0;
     }
+#pragma unroll
+    for (int q4 = 0; q4 < 8; q4++) {
+        ksum[q4 * kThreads + tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        kcmp[q4 * kThreads + tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    }
     regular = __syncthreads_and(regular);
     const float inv_cs = 1.0f / (float)P.cs;
 
-    // validity of the lane's 16 cells (inside the tile and not NoData)
+    // validity of the lane's 32 cells (inside the tile and not NoData); bit i*8+j
     unsigned valid = 0;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r = wr * 16 + tr * 4 + i, c = wc * 32 + tc * 4 + j;
+        for (int j = 0; j < 8; j++) {
+            const int r = wr * 16 + tr * 4 + i, c = wc * 64 + tc * 8 + j;
             bool v = r < G.nrow && c < G.ncol;
             if (v && P.mask) v = P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata;
-            valid |= (unsigned)v << (i * 4 + j);
+            valid |= (unsigned)v << (i * 8 + j);
         }
 
-    float part[16], acc_s[16], acc_c[16];
+    float part[32];
 #pragma unroll
-    for (int k = 0; k < 16; k++) part[k] = acc_s[k] = acc_c[k] = 0.0f;
+    for (int k = 0; k < 32; k++) part[k] = 0.0f;
     unsigned long long cnt = 0;
     unsigned pc = 0;  // points processed by this warp (warp-uniform)
 
-    // phase A roles: point q = tid / 8, part k = tid % 8: columns and rows
-    // k, k+8, ..., k+56, and the skip test of warp k
+    // phase A roles: point q = tid / 8, part k = tid % 8: columns k, k+8, ...,
+    // k+120, rows k, k+8, ..., k+56, and the skip test of warp k
     const int qa = tid >> 3, ka = tid & 7;
     const int sk_wr = ka >> 1, sk_wc = ka & 1;
-    const bool sk_on = (sk_wr * 16 < G.nrow) && (sk_wc * 32 < G.ncol);
-    const int sk_c0 = sk_wc * 32, sk_c1 = min(sk_wc * 32 + 31, G.ncol - 1);
+    const bool sk_on = (sk_wr * 16 < G.nrow) && (sk_wc * 64 < G.ncol);
+    const int sk_c0 = sk_wc * 64, sk_c1 = min(sk_wc * 64 + 63, G.ncol - 1);
     const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
 
     BatchIt bit{G.by0, 0, (int64_t)it.k0};
@@ -385,11 +400,11 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     cutf = P.cutf;
                     epsd2 = P.epsd2;
                 }
-                float* cE = colE + qa * kFStride;
+                float* cE = colE + qa * kFStrideC;
                 float* rF = rowF + qa * kFStride;
                 float* rG = rowG + qa * kFStride;
 #pragma unroll
-                for (int c = 0; c < 8; c++) {
+                for (int c = 0; c < 16; c++) {
                     const int j = ka + 8 * c;
                     float ah, al, d2;
                     exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
@@ -464,18 +479,19 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             while (todo) {
                 const int q = __ffs(todo) - 1;
                 todo &= todo - 1u;
-                const float* pE = colE + q * kFStride + wc * 32 + tc * 4;
+                const float* pE = colE + q * kFStrideC + wc * 64 + tc * 8;
                 const float* pF = rowF + q * kFStride + wr * 16 + tr * 4;
-                const float4 e4 = *reinterpret_cast<const float4*>(pE);
+                const float4 e4a = *reinterpret_cast<const float4*>(pE);
+                const float4 e4b = *reinterpret_cast<const float4*>(pE + 4);
                 const float4 f4 = *reinterpret_cast<const float4*>(pF);
-                const float ce[4] = {e4.x, e4.y, e4.z, e4.w};
+                const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                 const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
                 if (!COUNT && ((fullb >> q) & 1u)) {
                     // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
-                        for (int j = 0; j < 4; j++) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
+                        for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
                 } else {
                     const float4 g4 = *reinterpret_cast<const float4*>(rowG + q * kFStride + wr * 16 + tr * 4);
                     const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
@@ -484,16 +500,16 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
-                            for (int j = 0; j < 4; j++) {
+                            for (int j = 0; j < 8; j++) {
                                 const bool in = rg[i] < ce[j];
-                                if (in) part[i * 4 + j] = __fmaf_rn(ce[j], rv[i], part[i * 4 + j]);
-                                inm |= (unsigned)in << (i * 4 + j);
+                                if (in) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
+                                inm |= (unsigned)in << (i * 8 + j);
                             }
                     } else {
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
-                            for (int j = 0; j < 4; j++) fma_if_less(part[i * 4 + j], rg[i], ce[j], ce[j], rv[i]);
+                            for (int j = 0; j < 8; j++) fma_if_less(part[i * 8 + j], rg[i], ce[j], ce[j], rv[i]);
                     }
                     if ((ambb >> q) & 1u) {
                         // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
@@ -506,14 +522,14 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                             for (int i = 0; i < 4; i++) {
                                 if (!((fl >> i) & 1u)) continue;
 #pragma unroll
-                                for (int j = 0; j < 4; j++) {
-                                    const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 32 + tc * 4 + j],
+                                for (int j = 0; j < 8; j++) {
+                                    const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 64 + tc * 8 + j],
                                                                  s_cyg[wr * 16 + tr * 4 + i]) < cut;
                                     const bool fi = rg[i] < ce[j];
                                     if (ex != fi) {
                                         const float t = __fmul_rn(ce[j], rv[i]);
-                                        part[i * 4 + j] = __fadd_rn(part[i * 4 + j], ex ? t : -t);
-                                        if (COUNT) inm ^= 1u << (i * 4 + j);
+                                        part[i * 8 + j] = __fadd_rn(part[i * 8 + j], ex ? t : -t);
+                                        if (COUNT) inm ^= 1u << (i * 8 + j);
                                     }
                                 }
                             }
@@ -523,10 +539,17 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 }
                 pc++;
                 if ((pc & 15u) == 0) {
+                    // 16-point partials into the Kahan accumulators in shared memory
 #pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        kahan_add(acc_s[k], acc_c[k], part[k]);
-                        part[k] = 0.0f;
+                    for (int q4 = 0; q4 < 8; q4++) {
+                        float4 sv = ksum[q4 * kThreads + tid], cv = kcmp[q4 * kThreads + tid];
+                        kahan_add(sv.x, cv.x, part[q4 * 4 + 0]);
+                        kahan_add(sv.y, cv.y, part[q4 * 4 + 1]);
+                        kahan_add(sv.z, cv.z, part[q4 * 4 + 2]);
+                        kahan_add(sv.w, cv.w, part[q4 * 4 + 3]);
+                        ksum[q4 * kThreads + tid] = sv;
+                        kcmp[q4 * kThreads + tid] = cv;
+                        part[q4 * 4 + 0] = part[q4 * 4 + 1] = part[q4 * 4 + 2] = part[q4 * 4 + 3] = 0.0f;
                     }
                 }
             }
@@ -548,21 +571,27 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     // epilogue: FP64 result = (s - c) * normalisation
     const double norm = VARH ? 1.0 : P.k0;
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int q4 = 0; q4 < 8; q4++) {
+        float4 sv = ksum[q4 * kThreads + tid], cv = kcmp[q4 * kThreads + tid];
+        kahan_add(sv.x, cv.x, part[q4 * 4 + 0]);
+        kahan_add(sv.y, cv.y, part[q4 * 4 + 1]);
+        kahan_add(sv.z, cv.z, part[q4 * 4 + 2]);
+        kahan_add(sv.w, cv.w, part[q4 * 4 + 3]);
+        const float ss[4] = {sv.x, sv.y, sv.z, sv.w}, cc[4] = {cv.x, cv.y, cv.z, cv.w};
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int k = i * 4 + j;
-            kahan_add(acc_s[k], acc_c[k], part[k]);
-            const int r = wr * 16 + tr * 4 + i, c = wc * 32 + tc * 4 + j;
+        for (int u = 0; u < 4; u++) {
+            const int k = q4 * 4 + u, i = k >> 3, j = k & 7;
+            const int r = wr * 16 + tr * 4 + i, c = wc * 64 + tc * 8 + j;
             if (r >= G.nrow || c >= G.ncol) continue;
-            const double v = ((double)acc_s[k] - (double)acc_c[k]) * norm;
+            const double v = ((double)ss[u] - (double)cc[u]) * norm;
             if (it.slot >= 0) {
-                P.scratch[(size_t)it.slot * (kBlk * kBlk) + r * kBlk + c] = v;
+                P.scratch[(size_t)it.slot * kCells + r * kBC + c] = v;
             } else {
                 const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0);
                 P.out[o] = ((valid >> k) & 1u) ? (float)v : P.nodata;
             }
         }
+    }
     if (COUNT) {
         for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         if (lane == 0 && cnt) atomicAdd(P.evals, cnt);
@@ -593,14 +622,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = warp >> 1, wc = warp & 1, tr = lane >> 3, tc = lane & 7;
-    float cx[4], cy[4];
+    float cx[8], cy[4];
 #pragma unroll
-    for (int j = 0; j < 4; j++) cx[j] = mgk_cell_x(P.xll, P.cs, G.c0 + wc * 32 + tc * 4 + j);
+    for (int j = 0; j < 8; j++) cx[j] = mgk_cell_x(P.xll, P.cs, G.c0 + wc * 64 + tc * 8 + j);
 #pragma unroll
     for (int i = 0; i < 4; i++) cy[i] = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + wr * 16 + tr * 4 + i);
-    double acc[16];
+    double acc[32];
 #pragma unroll
-    for (int k = 0; k < 16; k++) acc[k] = 0.0;
+    for (int k = 0; k < 32; k++) acc[k] = 0.0;
     if (G.any) {
         int64_t seq = 0;
         for (int64_t by = G.by0; by <= G.by1 && seq < it.k1; by++) {
@@ -623,9 +652,9 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
 #pragma unroll
                     for (int i = 0; i < 4; i++)
 #pragma unroll
-                        for (int j = 0; j < 4; j++) {
+                        for (int j = 0; j < 8; j++) {
                             const double d2 = mgk_d2_exact(px, py, cx[j], cy[i]);
-                            if (d2 < cut) acc[i * 4 + j] += exp(d2 * m2h) * (double)p.wk;
+                            if (d2 < cut) acc[i * 8 + j] += exp(d2 * m2h) * (double)p.wk;
                         }
                 }
             }
@@ -636,12 +665,12 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
-        for (int j = 0; j < 4; j++) {
-            const int r = wr * 16 + tr * 4 + i, c = wc * 32 + tc * 4 + j;
+        for (int j = 0; j < 8; j++) {
+            const int r = wr * 16 + tr * 4 + i, c = wc * 64 + tc * 8 + j;
             if (r >= G.nrow || c >= G.ncol) continue;
-            const double v = acc[i * 4 + j] * norm;
+            const double v = acc[i * 8 + j] * norm;
             if (it.slot >= 0) {
-                P.scratch[(size_t)it.slot * (kBlk * kBlk) + r * kBlk + c] = v;
+                P.scratch[(size_t)it.slot * kCells + r * kBC + c] = v;
             } else {
                 const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0);
                 const bool valid = !P.mask || P.mask[o] != P.nodata;
@@ -652,16 +681,16 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
 
 // Merge of split blocks: cell value = sum over the block's slots in order.
 __device__ __forceinline__ void merge_block(const DParams& P, int32_t blk, int s0, int s1) {
-    const int nbx_t = (int)((P.nc + kBlk - 1) / kBlk);
+    const int nbx_t = (int)((P.nc + kBC - 1) / kBC);
     const int bxi = blk % nbx_t, byi = blk / nbx_t;
-    const int64_t r0 = P.row0 + (int64_t)byi * kBlk, c0 = P.col0 + (int64_t)bxi * kBlk;
-    const int nrow = (int)mgk_min64(kBlk, P.row0 + P.nr - r0);
-    const int ncol = (int)mgk_min64(kBlk, P.col0 + P.nc - c0);
-    for (int e = threadIdx.x; e < kBlk * kBlk; e += blockDim.x) {
-        const int r = e / kBlk, c = e % kBlk;
+    const int64_t r0 = P.row0 + (int64_t)byi * kBR, c0 = P.col0 + (int64_t)bxi * kBC;
+    const int nrow = (int)mgk_min64(kBR, P.row0 + P.nr - r0);
+    const int ncol = (int)mgk_min64(kBC, P.col0 + P.nc - c0);
+    for (int e = threadIdx.x; e < kCells; e += blockDim.x) {
+        const int r = e / kBC, c = e % kBC;
         if (r >= nrow || c >= ncol) continue;
         double v = 0.0;
-        for (int s = s0; s < s1; s++) v += P.scratch[(size_t)s * (kBlk * kBlk) + e];
+        for (int s = s0; s < s1; s++) v += P.scratch[(size_t)s * kCells + e];
         const int64_t o = (r0 + r - P.row0) * P.nc + (c0 + c - P.col0);
         const bool valid = !P.mask || P.mask[o] != P.nodata;
         P.out[o] = valid ? (float)v : P.nodata;
@@ -786,7 +815,7 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     P.evals = d_evals;
     P.err = ctx->d_counter + 7;
 
-    const int nbx_t = (int)((nc + kBlk - 1) / kBlk), nby_t = (int)((nr + kBlk - 1) / kBlk);
+    const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
     const int nblk = nbx_t * nby_t;
     int st;
     // ---- plan: candidates per block -> work items (split heavy blocks) ----
@@ -807,7 +836,7 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     const int32_t nslots = T.nslots;
 
     const size_t b_items = sizeof(Item) * items.size();
-    const size_t b_scr = sizeof(double) * (size_t)kBlk * kBlk * (size_t)std::max(nslots, 1);
+    const size_t b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
     const size_t b_sb = sizeof(int32_t) * (T.split_blocks.size() + 1);
     const size_t b_sbeg = sizeof(int32_t) * T.split_begin.size();
     Item* d_items = nullptr;
@@ -883,8 +912,8 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
         fill_params(P[j], J.index, &J.grid, J.row0, J.col0, J.nrows, J.ncols, J.d_mask, J.d_out);
         P[j].evals = d_evals ? d_evals + j : nullptr;
         P[j].err = ctx->d_counter + 7;
-        nbx[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.ncols + kBlk - 1) / kBlk) : 0;
-        nby[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.nrows + kBlk - 1) / kBlk) : 0;
+        nbx[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.ncols + kBC - 1) / kBC) : 0;
+        nby[j] = J.nrows > 0 && J.ncols > 0 ? (int)((J.nrows + kBR - 1) / kBR) : 0;
         off[j + 1] = off[j] + nbx[j] * nby[j];
     }
     const int nblk_all = off[njobs];
@@ -925,7 +954,7 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     sort_items(items_var);
     const size_t b_jobs = sizeof(DParams) * njobs;
     const size_t b_items = sizeof(Item) * std::max<size_t>(items_fix.size() + items_var.size(), 1);
-    const size_t b_scr = sizeof(double) * (size_t)kBlk * kBlk * (size_t)std::max(nslots, 1);
+    const size_t b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
     const size_t b_mg = sizeof(int4) * std::max<size_t>(merges.size(), 1);
     DParams* d_jobs = nullptr;
     Item* d_items = nullptr;
@@ -938,7 +967,7 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     unsigned long long err = 0;
     if (st == MGK_OK) {
         for (int j = 0; j < njobs; j++)
-            P[j].scratch = d_scr ? d_scr + (size_t)slot0[j] * kBlk * kBlk : nullptr;  // slots are job-local
+            P[j].scratch = d_scr ? d_scr + (size_t)slot0[j] * kCells : nullptr;  // slots are job-local
         std::vector<Item> all(items_fix);
         all.insert(all.end(), items_var.begin(), items_var.end());
         do {
@@ -994,18 +1023,18 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
 // up front for its own allocator or arena, or a latency-critical loop that
 // forbids cudaMalloc/cudaFree (which may synchronise the whole device) once it
 // is running.  For them this variant keeps all scratch in one fixed
-// file-scope device array, g_density_scratch (kNaScratchBytes, about 12.4 MiB),
+// file-scope device array, g_density_scratch (kNaScratchBytes, about 12.3 MiB),
 // which every GPU that loads the library holds until the process exits, and
 // its host-side plan in fixed static arrays.  Limits: a tile of at most 4096 x
-// 4096 cells (64 x 64 blocks of 64 x 64) and at most kNaMaxSlots split work
+// 4096 cells (64 x 32 blocks of 64 x 128) and at most kNaMaxSlots split work
 // items (heavy blocks get larger work items instead).  Inputs (index, mask) and
 // the output tile are the caller's as for mgk_density_tile.
 namespace {
 
-constexpr int kNaMaxBlocks = 4096;
+constexpr int kNaMaxBlocks = 2048;
 constexpr int kNaMaxItems = 12288;
-constexpr int kNaMaxSlots = 384;
-constexpr size_t kNaSlotBytes = sizeof(double) * kBlk * kBlk;
+constexpr int kNaMaxSlots = 192;
+constexpr size_t kNaSlotBytes = sizeof(double) * kCells;
 constexpr size_t na_round(size_t v) { return (v + 255) / 256 * 256; }
 constexpr size_t kNaOffCounts = 0;
 constexpr size_t kNaOffItems = na_round(kNaOffCounts + sizeof(int64_t) * kNaMaxBlocks);
@@ -1033,9 +1062,9 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     if (row0 < 0 || col0 < 0 || nr < 0 || nc < 0 || row0 + nr > g->nrows || col0 + nc > g->ncols)
         return mgk_fail(ctx, MGK_ERR_INVALID, "density_tile_noalloc: tile outside the raster");
     if (nr == 0 || nc == 0) return MGK_OK;
-    const int nbx_t = (int)((nc + kBlk - 1) / kBlk), nby_t = (int)((nr + kBlk - 1) / kBlk);
+    const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
     const int nblk = nbx_t * nby_t;
-    if (nblk > kNaMaxBlocks)
+    if (nr > 4096 || nc > 4096 || nblk > kNaMaxBlocks)
         return mgk_fail(ctx, MGK_ERR_INVALID,
                         "density_tile_noalloc: tile of " + std::to_string(nr) + " x " + std::to_string(nc) +
                             " cells exceeds the fixed scratch (at most 4096 x 4096 cells)");

@@ -56,7 +56,7 @@ def test_stream_matches_oracle_and_is_deterministic(setup):
     ref, rev = o.density(c["x"], c["y"], c["w"], ew, c["h"], o.grid(*c["density_grid"].astuple()), mask)
     nd = mask == dg.nodata
     assert np.array_equal(out[nd], mask[nd])
-    rel = np.abs(out[~nd].astype(np.float64) - ref[~nd]) / np.abs(ref[~nd])
+    rel = np.abs(out[~nd].astype(np.float64) - ref[~nd]) / np.maximum(np.abs(ref[~nd]), 1e-300)
     assert rel.max() <= RTOL
     assert ev == rev
     again, _, _ = run(ctx, idx, dg, mask, 192)
