@@ -268,6 +268,11 @@ constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab + 2 *
 #define MGK_DENSITY_MIN_CTAS 2  // resident CTAs per SM (shared memory allows two)
 #endif
 
+// Block column of cell j (0..7) of lane column tc in warp column wc.
+__device__ __forceinline__ int lane_col(int wc, int tc, int j) {
+    return wc * 64 + (j < 4 ? tc * 4 + j : 32 + tc * 4 + (j - 4));
+}
+
 // One work item: the gather of the candidate range [it.k0, it.k1) of one
 // 64 x 128 block (the body of k_density and of the multi-job k_density_jobs).
 template <bool VARH, bool COUNT>
@@ -290,7 +295,9 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*64..
-    const int tr = lane >> 3, tc = lane & 7;  // lane micro-tile: rows tr*4.. (4), cols tc*8.. (8)
+    // lane micro-tile: rows tr*4.. (4); columns tc*4.. and 32+tc*4.. (2 x 4) of
+    // the warp's 64, so the 8 lanes of a row read 128 contiguous bytes of E
+    const int tr = lane >> 3, tc = lane & 7;
 
     // cell centres of the block: global floats and their quantum split
     bool regular = true;
@@ -325,7 +332,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            const int r = wr * 16 + tr * 4 + i, c = wc * 64 + tc * 8 + j;
+            const int r = wr * 16 + tr * 4 + i, c = lane_col(wc, tc, j);
             bool v = r < G.nrow && c < G.ncol;
             if (v && P.mask) v = P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata;
             valid |= (unsigned)v << (i * 8 + j);
@@ -479,10 +486,10 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             while (todo) {
                 const int q = __ffs(todo) - 1;
                 todo &= todo - 1u;
-                const float* pE = colE + q * kFStrideC + wc * 64 + tc * 8;
+                const float* pE = colE + q * kFStrideC + wc * 64 + tc * 4;
                 const float* pF = rowF + q * kFStride + wr * 16 + tr * 4;
                 const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                const float4 e4b = *reinterpret_cast<const float4*>(pE + 4);
+                const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
                 const float4 f4 = *reinterpret_cast<const float4*>(pF);
                 const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                 const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
@@ -523,7 +530,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                                 if (!((fl >> i) & 1u)) continue;
 #pragma unroll
                                 for (int j = 0; j < 8; j++) {
-                                    const bool ex = mgk_d2_exact(px, py, s_cxg[wc * 64 + tc * 8 + j],
+                                    const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
                                                                  s_cyg[wr * 16 + tr * 4 + i]) < cut;
                                     const bool fi = rg[i] < ce[j];
                                     if (ex != fi) {
@@ -581,7 +588,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
         for (int u = 0; u < 4; u++) {
             const int k = q4 * 4 + u, i = k >> 3, j = k & 7;
-            const int r = wr * 16 + tr * 4 + i, c = wc * 64 + tc * 8 + j;
+            const int r = wr * 16 + tr * 4 + i, c = lane_col(wc, tc, j);
             if (r >= G.nrow || c >= G.ncol) continue;
             const double v = ((double)ss[u] - (double)cc[u]) * norm;
             if (it.slot >= 0) {
