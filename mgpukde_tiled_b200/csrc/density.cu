@@ -7,16 +7,16 @@
 //
 //   den(c) = sum_p [d^2 < 9 h_p^2] exp(-d^2 / 2 h_p^2) / (h_p^2 TWO_PI) w_p e_p
 //
-// Layout: a CTA (256 threads) owns a 64 x 64 block of cells; warp w owns a
-// 16 x 32 sub-block, lane l a 4 x 4 micro-tile.  Candidates (points of the
+// Layout: a CTA (256 threads) owns a 64 x 128 block of cells; warp w owns a
+// 16 x 64 sub-block, lane l a 4 x 8 micro-tile.  Candidates (points of the
 // bins within 3h of the block, one contiguous range per bin row) arrive in
-// mini-batches of 32 through a double-buffered TMA bulk copy
-// (cp.async.bulk + mbarrier) into shared memory.  Per mini-batch:
+// mini-batches of 32, taken across bin rows, through a double-buffered TMA
+// bulk copy (cp.async.bulk + mbarrier) into shared memory.  Per mini-batch:
 //
 //  phase A (all 256 threads, 8 per point): the Gaussian factorises over the
 //    grid, exp2(-(a_j + b_i)) = E_j F_i with a_j = dx_j^2 k2, b_i = dy_i^2 k2,
-//    k2 = log2(e) / (2 h^2).  The 64 column factors and 64 row factors of the
-//    block are computed once per point.  Coordinates are hi/lo float pairs on
+//    k2 = log2(e) / (2 h^2).  The 128 column factors and 64 row factors of
+//    the block are computed once per point.  Coordinates are hi/lo float pairs on
 //    a common quantum, so dx = (xh - cxh) + (xl - cxl) is exact as a pair and
 //    a = dx^2 k2 is formed with error-free float products (no FP64, no
 //    conversions); E = ex2(-a_hi) (1 - a_lo ln2).  Row entries also carry the
@@ -29,8 +29,10 @@
 //    ambiguous are re-decided with the exact FP64 test of the oracle, so the
 //    summed pair set is exactly the reference's.
 //
-// Accumulation: FP32 partial sums over 16 points per cell, added into a
-// Kahan-compensated FP32 accumulator; the epilogue forms (s - c) times the
+// Accumulation: FP32 partial sums over 16 points per cell (registers), added
+// into a Kahan-compensated FP32 accumulator (shared memory, 64 KB per CTA,
+// which with the 128 registers per thread leaves two CTAs per SM); the
+// epilogue forms (s - c) times the
 // kernel normalisation in FP64.  Heavy blocks are split into work items whose
 // FP64 partials are merged in a fixed order, so results are bitwise
 // reproducible.
@@ -231,25 +233,30 @@ struct BatchIt {
     int64_t by, seq, pos;
 };
 
-// Next mini-batch of the block's candidate sequence (never spans two bin
-// rows): returns its size (0 at the end) and its first global index.
-__device__ __forceinline__ int next_batch(const DParams& P, const BlockGeom& G, const Item& it, BatchIt& s,
-                                          int64_t& src) {
+// Stages the next mini-batch of the block's candidate sequence into dst: up
+// to kMB candidates, taken across bin rows (one bulk copy per row segment,
+// all completing on the buffer's mbarrier; the issuing thread then arrives
+// with the batch's byte count).  Returns the batch size (0 at the end).
+__device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, const Item& it, BatchIt& s,
+                                          MgkPt* dst, uint64_t* bar, bool issuer) {
     if (!G.any) return 0;
-    while (s.by <= G.by1 && s.pos < it.k1) {
+    int m = 0;
+    while (m < kMB && s.by <= G.by1 && s.pos < it.k1) {
         const int64_t sb = P.bin_start[s.by * P.nbx + G.bx0];
         const int64_t len = (int64_t)P.bin_start[s.by * P.nbx + G.bx1 + 1] - sb;
         const int64_t lo = mgk_max64(s.pos, s.seq), hi = mgk_min64(s.seq + len, (int64_t)it.k1);
         if (lo < hi) {
-            const int m = (int)mgk_min64(kMB, hi - lo);
-            src = sb + (lo - s.seq);
-            s.pos = lo + m;
-            return m;
+            const int n = (int)mgk_min64(kMB - m, hi - lo);
+            if (issuer) bulk_g2s(dst + m, P.pts + sb + (lo - s.seq), (unsigned)(n * sizeof(MgkPt)), bar);
+            s.pos = lo + n;
+            m += n;
+        } else {
+            s.seq += len;
+            s.by++;
         }
-        s.seq += len;
-        s.by++;
     }
-    return 0;
+    if (issuer && m > 0) mbar_arrive_tx(bar, (unsigned)(m * sizeof(MgkPt)));
+    return m;
 }
 
 // Dynamic shared memory of k_density (bytes): the staged points, the factor
@@ -353,24 +360,14 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
 
     BatchIt bit{G.by0, 0, (int64_t)it.k0};
-    int64_t src = 0;
-    int m = next_batch(P, G, it, bit, src);
-    if (m > 0 && tid == 0) {
-        mbar_arrive_tx(&mbar[0], (unsigned)(m * sizeof(MgkPt)));
-        bulk_g2s(&stage[0], P.pts + src, (unsigned)(m * sizeof(MgkPt)), &mbar[0]);
-    }
+    int m = fill_batch(P, G, it, bit, &stage[0], &mbar[0], tid == 0);
     unsigned phase0 = 0, phase1 = 0;
     int buf = 0;
     // outstanding copies at an abort: (buffer, parity) pairs to drain
     int drain_n = 0, drain_b[2] = {0, 0};
     unsigned drain_p[2] = {0, 0};
     while (m > 0) {
-        int64_t nsrc = 0;
-        const int nm = next_batch(P, G, it, bit, nsrc);
-        if (nm > 0 && tid == 0) {
-            mbar_arrive_tx(&mbar[buf ^ 1], (unsigned)(nm * sizeof(MgkPt)));
-            bulk_g2s(&stage[(buf ^ 1) * kMB], P.pts + nsrc, (unsigned)(nm * sizeof(MgkPt)), &mbar[buf ^ 1]);
-        }
+        const int nm = fill_batch(P, G, it, bit, &stage[(buf ^ 1) * kMB], &mbar[buf ^ 1], tid == 0);
         const unsigned par = buf ? phase1 : phase0;
         if (!mbar_wait(&mbar[buf], par)) {
             atomicExch(P.err, 1ull);
@@ -563,7 +560,6 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         }
         __syncthreads();  // factor tables and stage[buf] are reused next
         m = nm;
-        src = nsrc;
         buf ^= 1;
     }
     if (drain_n) {
