@@ -73,7 +73,7 @@ struct DParams {
     // index
     const MgkPt* pts;
     const int32_t* bin_start;
-    double ox, oy, inv_side;
+    double ox, oy, side, inv_side;
     int64_t nbx, nby;
     int qexp;
     // fixed-h constants
@@ -98,6 +98,7 @@ struct BlockGeom {
     int64_t r0, c0;   // global first row / col of the block
     int nrow, ncol;   // cells of the block inside the tile
     int64_t bx0, bx1, by0, by1;
+    double x_lo, x_hi, y_lo, y_hi;  // extent of the block's cell centres
     bool any;
 };
 
@@ -107,12 +108,37 @@ __device__ __forceinline__ BlockGeom block_geom(const DParams& P, int bxi, int b
     G.c0 = P.col0 + (int64_t)bxi * kBC;
     G.nrow = (int)mgk_min64(kBR, P.row0 + P.nr - G.r0);
     G.ncol = (int)mgk_min64(kBC, P.col0 + P.nc - G.c0);
-    const double x_lo = mgk_cell_x(P.xll, P.cs, G.c0), x_hi = mgk_cell_x(P.xll, P.cs, G.c0 + G.ncol - 1);
-    const double y_hi = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0);
-    const double y_lo = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + G.nrow - 1);
-    G.any = bin_range(x_lo - P.reach, x_hi + P.reach, P.ox, P.inv_side, P.nbx, G.bx0, G.bx1) &&
-            bin_range(y_lo - P.reach, y_hi + P.reach, P.oy, P.inv_side, P.nby, G.by0, G.by1);
+    G.x_lo = mgk_cell_x(P.xll, P.cs, G.c0);
+    G.x_hi = mgk_cell_x(P.xll, P.cs, G.c0 + G.ncol - 1);
+    G.y_hi = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0);
+    G.y_lo = mgk_cell_y(P.yll, P.cs, P.g_nrows, G.r0 + G.nrow - 1);
+    G.any = bin_range(G.x_lo - P.reach, G.x_hi + P.reach, P.ox, P.inv_side, P.nbx, G.bx0, G.bx1) &&
+            bin_range(G.y_lo - P.reach, G.y_hi + P.reach, P.oy, P.inv_side, P.nby, G.by0, G.by1);
     return G;
+}
+
+// Candidates of bin row `by` for the block: a point of the row can be within
+// reach of a cell centre only if |x - [x_lo, x_hi]| <= sqrt(reach^2 - dy^2),
+// dy the distance from the row's y-extent to [y_lo, y_hi] (a lower bound on
+// the point's), so the row's bin range narrows away from the block (the
+// candidate region is the block rectangle grown by a disc, not by a square).
+// Returns the row's contiguous range [sb, sb + len) of the index.
+__device__ __forceinline__ void row_span(const DParams& P, const BlockGeom& G, int64_t by, int64_t& sb,
+                                         int64_t& len) {
+    const double rlo = P.oy + (double)by * P.side, rhi = rlo + P.side;
+    const double dy = fmax(0.0, fmax(rlo - G.y_hi, G.y_lo - rhi)) * (1.0 - 1e-9);
+    const double rr = P.reach * P.reach - dy * dy;
+    int64_t b0, b1;
+    if (rr >= 0.0) {
+        const double hw = sqrt(rr) * (1.0 + 1e-9) + 1e-9 * P.reach;
+        if (bin_range(G.x_lo - hw, G.x_hi + hw, P.ox, P.inv_side, P.nbx, b0, b1)) {
+            sb = P.bin_start[by * P.nbx + b0];
+            len = (int64_t)P.bin_start[by * P.nbx + b1 + 1] - sb;
+            return;
+        }
+    }
+    sb = 0;
+    len = 0;
 }
 
 // Candidate count of every block of the tile (planning).
@@ -122,8 +148,11 @@ __global__ void k_block_counts(DParams P, int nbx_t, int nby_t, int64_t* __restr
     const BlockGeom G = block_geom(P, i % nbx_t, i / nbx_t);
     int64_t c = 0;
     if (G.any)
-        for (int64_t by = G.by0; by <= G.by1; by++)
-            c += (int64_t)P.bin_start[by * P.nbx + G.bx1 + 1] - (int64_t)P.bin_start[by * P.nbx + G.bx0];
+        for (int64_t by = G.by0; by <= G.by1; by++) {
+            int64_t sb, len;
+            row_span(P, G, by, sb, len);
+            c += len;
+        }
     counts[i] = c;
 }
 
@@ -230,7 +259,8 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
 }
 
 struct BatchIt {
-    int64_t by, seq, pos;
+    int64_t by, seq, pos;  // current bin row, its offset in the block's sequence, next candidate
+    int64_t sb, len;       // the current row's range of the index
 };
 
 // Stages the next mini-batch of the block's candidate sequence into dst: up
@@ -242,17 +272,15 @@ __device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, 
     if (!G.any) return 0;
     int m = 0;
     while (m < kMB && s.by <= G.by1 && s.pos < it.k1) {
-        const int64_t sb = P.bin_start[s.by * P.nbx + G.bx0];
-        const int64_t len = (int64_t)P.bin_start[s.by * P.nbx + G.bx1 + 1] - sb;
-        const int64_t lo = mgk_max64(s.pos, s.seq), hi = mgk_min64(s.seq + len, (int64_t)it.k1);
+        const int64_t lo = mgk_max64(s.pos, s.seq), hi = mgk_min64(s.seq + s.len, (int64_t)it.k1);
         if (lo < hi) {
             const int n = (int)mgk_min64(kMB - m, hi - lo);
-            if (issuer) bulk_g2s(dst + m, P.pts + sb + (lo - s.seq), (unsigned)(n * sizeof(MgkPt)), bar);
+            if (issuer) bulk_g2s(dst + m, P.pts + s.sb + (lo - s.seq), (unsigned)(n * sizeof(MgkPt)), bar);
             s.pos = lo + n;
             m += n;
         } else {
-            s.seq += len;
-            s.by++;
+            s.seq += s.len;
+            if (++s.by <= G.by1) row_span(P, G, s.by, s.sb, s.len);
         }
     }
     if (issuer && m > 0) mbar_arrive_tx(bar, (unsigned)(m * sizeof(MgkPt)));
@@ -359,7 +387,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     const int sk_c0 = sk_wc * 64, sk_c1 = min(sk_wc * 64 + 63, G.ncol - 1);
     const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
 
-    BatchIt bit{G.by0, 0, (int64_t)it.k0};
+    BatchIt bit{G.by0, 0, (int64_t)it.k0, 0, 0};
+    if (G.any) row_span(P, G, G.by0, bit.sb, bit.len);
     int m = fill_batch(P, G, it, bit, &stage[0], &mbar[0], tid == 0);
     unsigned phase0 = 0, phase1 = 0;
     int buf = 0;
@@ -636,9 +665,8 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
     if (G.any) {
         int64_t seq = 0;
         for (int64_t by = G.by0; by <= G.by1 && seq < it.k1; by++) {
-            const int64_t sb = P.bin_start[by * P.nbx + G.bx0];
-            const int64_t se = P.bin_start[by * P.nbx + G.bx1 + 1];
-            const int64_t len = se - sb;
+            int64_t sb, len;
+            row_span(P, G, by, sb, len);
             const int64_t lo = mgk_max64(seq, it.k0), hi = mgk_min64(seq + len, it.k1);
             for (int64_t base = lo; base < hi; base += kStage64) {
                 const int m = (int)mgk_min64(kStage64, hi - base);
@@ -742,6 +770,7 @@ void fill_params(DParams& P, const mgk_index* idx, const mgk_grid* g, int64_t ro
     P.bin_start = idx->bin_start;
     P.ox = idx->ox;
     P.oy = idx->oy;
+    P.side = idx->side;
     P.inv_side = 1.0 / idx->side;
     P.nbx = idx->nbx;
     P.nby = idx->nby;
