@@ -419,7 +419,7 @@ def run_mgk(args):
     if os.path.exists(tp) and args.scale == 1.0:
         with open(tp) as f:
             for line in f:
-                if line.startswith("bytes_per_launch_scaled:"):
+                if line.startswith("bytes_per_launch:"):
                     traffic = int(line.split(":", 1)[1].split()[0])
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
