@@ -429,3 +429,148 @@ float orc_mle_fixed_bandwidth(int64_t n, const float* x, const float* y, const f
     if (iterations) *iterations = it;
     return (hA + hD) / 2;
 }
+
+/* ---- adaptive bandwidths (h_option 2) ---- */
+
+void orc_point_density(int64_t n, const float* x, const float* y, const float* w,
+                       const double* ew, const float* hs, float h, int self,
+                       double* out, int64_t* evals) {
+    float hmax = h;
+    if (hs)
+        for (int64_t i = 0; i < n; i++)
+            if (hs[i] > hmax) hmax = hs[i];
+    bins_t b;
+    bins_build(&b, n, x, y, 3.0 * (double)hmax * (1.0 + 1e-6));
+    int64_t total = 0;
+#pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 64) reduction(+ : total)
+    for (int64_t j = 0; j < n; j++) {
+        const double reach = 3.0 * (double)hmax * (1.0 + 1e-6);
+        int64_t bx0, bx1, by0, by1;
+        bin_span((double)x[j] - reach, (double)x[j] + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
+        bin_span((double)y[j] - reach, (double)y[j] + reach, b.y0, b.side, b.nby, &by0, &by1);
+        double den = 0.0;
+        int64_t cnt = 0;
+        for (int64_t by = by0; by <= by1; by++)
+            for (int64_t bx = bx0; bx <= bx1; bx++) {
+                const int64_t k = by * b.nbx + bx;
+                for (int64_t t = b.start[k]; t < b.start[k + 1]; t++) {
+                    const int64_t i = b.idx[t];
+                    if (i == j && !self) continue;
+                    const double h2 = orc_h2(hs ? hs[i] : h);
+                    const double d2 = d2_exact(x[i], y[i], x[j], y[j]);
+                    if (d2 < kCut * h2) {
+                        den += kern(h2, d2) * (double)(w ? w[i] : 1.0f) * (ew ? ew[i] : 1.0);
+                        cnt++;
+                    }
+                }
+            }
+        out[j] = den;
+        total += cnt;
+    }
+    bins_free(&b);
+    if (evals) *evals = total;
+}
+
+void orc_adaptive_bandwidths(int64_t n, const double* den0, float h, float alpha, float* hs) {
+    double s = 0.0;
+    for (int64_t i = 0; i < n; i++) s += log(den0[i]);
+    const double gml = exp(s / (double)n);
+    for (int64_t i = 0; i < n; i++) hs[i] = (float)((double)h * pow(den0[i] / gml, (double)alpha));
+}
+
+double orc_loglik_adaptive(int64_t n, const float* x, const float* y, const float* w,
+                           const double* dist2, const orc_grid* g, const float* mask,
+                           float h, float alpha, float* hs_out) {
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    double* ew = dist2 ? (double*)malloc(sizeof(double) * nn) : NULL;
+    double* den = (double*)malloc(sizeof(double) * nn);
+    float* hs = (float*)malloc(sizeof(float) * nn);
+    if (dist2) orc_edge_weights(n, x, y, NULL, h, dist2, g, mask, ew, NULL);
+    orc_point_density(n, x, y, w, ew, NULL, h, 1, den, NULL);
+    orc_adaptive_bandwidths(n, den, h, alpha, hs);
+    if (dist2) orc_edge_weights(n, x, y, hs, 0.0f, dist2, g, mask, ew, NULL);
+    orc_point_density(n, x, y, w, ew, hs, 0.0f, 0, den, NULL);
+    double logl = 0.0;
+    for (int64_t j = 0; j < n; j++) logl += log(den[j] > kEpsDensity ? den[j] : kEpsDensity);
+    if (hs_out) memcpy(hs_out, hs, sizeof(float) * (size_t)n);
+    free(ew);
+    free(den);
+    free(hs);
+    return logl;
+}
+
+/* hj_likelihood, kde_cuda_kdtr_tiled.cu:3677-3720: the likelihoods of the
+ * centre and its four neighbours, skipping the ones the last move kept. */
+static void hj_likelihoods(int64_t n, const float* x, const float* y, const float* w, const double* dist2,
+                           const orc_grid* g, const float* mask, float h0, float a0, float sh, float sa,
+                           int last, double* L) {
+    if (last == -1) L[0] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0, NULL);
+    if (last != 2) L[1] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 - sh, a0, NULL);
+    if (last != 1) L[2] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 + sh, a0, NULL);
+    if (last != 4) L[3] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 + sa, NULL);
+    if (last != 3) L[4] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 - sa, NULL);
+}
+
+void orc_adaptive_search(int64_t n, const float* x, const float* y, const float* w,
+                         const double* dist2, const orc_grid* g, const float* mask,
+                         float h0, float* out3, float* hs, int* iterations) {
+    float alpha0 = -0.5f;
+    float stepH = h0 / 10;
+    float stepA = 0.1f;
+    double L[5];
+    hj_likelihoods(n, x, y, w, dist2, g, mask, h0, alpha0, stepH, stepA, -1, L);
+    double Lmax = L[0];
+    const float s = stepH / 10;
+    const float a = stepA / 10;
+    int it = 0;
+    while ((stepH > s || stepA > a) && (h0 - stepH > 0) && it <= 30) { /* MAX_NUM_ITERATIONS */
+        int dmax = 0;
+        for (int i = 0; i < 5; i++)
+            if (L[i] > Lmax) {
+                Lmax = L[i];
+                dmax = i;
+            }
+        if (dmax == 0) {
+            stepH = stepH / 2;
+            stepA = stepA / 2;
+        } else {
+            /* the moves and likelihood bookkeeping of hooke_jeeves (:3750-3778),
+             * including its handling of a move to +stepA */
+            if (dmax == 1) {
+                h0 = h0 - stepH;
+                L[2] = L[0];
+                L[0] = L[1];
+            }
+            if (dmax == 2) {
+                h0 = h0 + stepH;
+                L[1] = L[0];
+                L[0] = L[2];
+            }
+            if (dmax == 3) {
+                alpha0 = alpha0 + stepA;
+                L[3] = L[0];
+                L[0] = L[4];
+            }
+            if (dmax == 4) {
+                alpha0 = alpha0 - stepA;
+                L[3] = L[0];
+                L[0] = L[4];
+            }
+        }
+        hj_likelihoods(n, x, y, w, dist2, g, mask, h0, alpha0, stepH, stepA, dmax, L);
+        it++;
+    }
+    out3[0] = h0;
+    out3[1] = alpha0;
+    out3[2] = (float)Lmax;
+    if (iterations) *iterations = it;
+    /* final bandwidths, main :566-572 */
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    double* ew = dist2 ? (double*)malloc(sizeof(double) * nn) : NULL;
+    double* den = (double*)malloc(sizeof(double) * nn);
+    if (dist2) orc_edge_weights(n, x, y, NULL, h0, dist2, g, mask, ew, NULL);
+    orc_point_density(n, x, y, w, ew, NULL, h0, 1, den, NULL);
+    orc_adaptive_bandwidths(n, den, h0, alpha0, hs);
+    free(ew);
+    free(den);
+}

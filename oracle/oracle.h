@@ -110,6 +110,39 @@ float orc_mle_fixed_bandwidth(int64_t n, const float* x, const float* y, const f
                               const double* dist2, const orc_grid* g, const float* mask,
                               float h0, int* iterations);
 
+/* Density at the points themselves with per-source bandwidths:
+ *   den_j = sum_{i, d_ij^2 < 9 h_i^2} K_{h_i}(d_ij) w_i e_i   (i = j included when self != 0)
+ * hs == NULL -> fixed h.  ComputeFixedDensityAtPoints
+ * (kde_cuda_kdtr_tiled.cu:3096-3133) with self, and the leave-one-out sums of
+ * the adaptive LogLikelihood (CPU branch, :3604-3636) without. */
+void orc_point_density(int64_t n, const float* x, const float* y, const float* w,
+                       const double* ew, const float* hs, float h, int self,
+                       double* out, int64_t* evals);
+
+/* Adaptive bandwidths from a pilot density, kde_cuda_kdtr_tiled.cu:3581-3590:
+ * gml = exp(mean log den0) (compGML, :3807-3814) and
+ * hs_i = h (den0_i / gml)^alpha, stored as float. */
+void orc_adaptive_bandwidths(int64_t n, const double* den0, float h, float alpha, float* hs);
+
+/* Log likelihood of the adaptive bandwidths for (h, alpha), CPU branch of
+ * LogLikelihood(h, alpha) (kde_cuda_kdtr_tiled.cu:3553-3650): edge weights at
+ * the fixed h, pilot density with self, hs, edge weights at hs, and the
+ * leave-one-out sum with per-source bandwidths.  dist2 == NULL: no edge
+ * correction.  hs_out (optional) receives the bandwidths. */
+double orc_loglik_adaptive(int64_t n, const float* x, const float* y, const float* w,
+                           const double* dist2, const orc_grid* g, const float* mask,
+                           float h, float alpha, float* hs_out);
+
+/* Hooke-Jeeves search over (h, alpha), hooke_jeeves / hj_likelihood
+ * (kde_cuda_kdtr_tiled.cu:3677-3785), with the reference's start
+ * (alpha0 = -0.5, stepH = h0 / 10, stepA = 0.1, main :550-555), its float
+ * step arithmetic and its bookkeeping of the five likelihoods, then the final
+ * bandwidths of main (:566-572): pilot density at the optimum h with edge
+ * weights at h, compGML, hs.  out: h_opt, alpha_opt, Lmax; hs (n floats). */
+void orc_adaptive_search(int64_t n, const float* x, const float* y, const float* w,
+                         const double* dist2, const orc_grid* g, const float* mask,
+                         float h0, float* out3, float* hs, int* iterations);
+
 /* Number of OpenMP threads the oracle uses (0 = library default). */
 void orc_set_threads(int n);
 int orc_get_threads(void);

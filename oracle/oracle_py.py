@@ -50,6 +50,12 @@ def lib():
         L.orc_mle_fixed_bandwidth.restype = C.c_float
         L.orc_mle_fixed_bandwidth.argtypes = [C.c_int64, P, P, P, P, C.POINTER(OrcGrid), P, C.c_float,
                                               C.POINTER(C.c_int)]
+        L.orc_point_density.argtypes = [C.c_int64, P, P, P, P, P, C.c_float, C.c_int, P, P]
+        L.orc_adaptive_bandwidths.argtypes = [C.c_int64, P, C.c_float, C.c_float, P]
+        L.orc_loglik_adaptive.restype = C.c_double
+        L.orc_loglik_adaptive.argtypes = [C.c_int64, P, P, P, P, C.POINTER(OrcGrid), P, C.c_float, C.c_float, P]
+        L.orc_adaptive_search.argtypes = [C.c_int64, P, P, P, P, C.POINTER(OrcGrid), P, C.c_float, P, P,
+                                          C.POINTER(C.c_int)]
         L.orc_set_threads.argtypes = [C.c_int]
         L.orc_get_threads.restype = C.c_int
         _lib = L
@@ -156,3 +162,41 @@ def mle_fixed_bandwidth(x, y, w, dist2, g: OrcGrid, mask, h0):
     h = lib().orc_mle_fixed_bandwidth(len(x), _p(x), _p(y), _p(w), _p(d), C.byref(g), _p(m),
                                       float(h0), C.byref(it))
     return float(h), it.value
+
+
+def point_density(x, y, w, ew, h, hs=None, self_term=True):
+    x, y, w, ew, hs = _f32(x), _f32(y), _f32(w), _f64(ew), _f32(hs)
+    out = np.zeros(len(x), np.float64)
+    ev = C.c_int64(0)
+    lib().orc_point_density(len(x), _p(x), _p(y), _p(w), _p(ew), _p(hs), float(h), int(bool(self_term)),
+                            _p(out), C.byref(ev))
+    return out, ev.value
+
+
+def adaptive_bandwidths(den0, h, alpha):
+    den0 = _f64(den0)
+    hs = np.zeros(len(den0), np.float32)
+    lib().orc_adaptive_bandwidths(len(den0), _p(den0), float(h), float(alpha), _p(hs))
+    return hs
+
+
+def loglik_adaptive(x, y, w, dist2, g, mask, h, alpha):
+    x, y, w, d = _f32(x), _f32(y), _f32(w), _f64(dist2)
+    m = None if mask is None else _f32(mask).reshape(-1)
+    hs = np.zeros(len(x), np.float32)
+    ll = lib().orc_loglik_adaptive(len(x), _p(x), _p(y), _p(w), _p(d), C.byref(g) if g is not None else None,
+                                   _p(m), float(h), float(alpha), _p(hs))
+    return float(ll), hs
+
+
+def adaptive_search(x, y, w, dist2, g, mask, h0):
+    """Hooke-Jeeves over (h, alpha) and the final per-point bandwidths;
+    returns (h_opt, alpha_opt, Lmax, hs, iterations)."""
+    x, y, w, d = _f32(x), _f32(y), _f32(w), _f64(dist2)
+    m = None if mask is None else _f32(mask).reshape(-1)
+    out3 = np.zeros(3, np.float32)
+    hs = np.zeros(len(x), np.float32)
+    it = C.c_int(0)
+    lib().orc_adaptive_search(len(x), _p(x), _p(y), _p(w), _p(d), C.byref(g) if g is not None else None, _p(m),
+                              float(h0), _p(out3), _p(hs), C.byref(it))
+    return float(out3[0]), float(out3[1]), float(out3[2]), hs, it.value

@@ -83,8 +83,12 @@ def make_case(name, x, y, w, h_pp, eg, emask, dg, dmask, hoption, edge, sw):
     print(f"{name}: n={len(x)} h0={h0} hopt={hopt} density {den.shape}")
 
 
-def main():
+def main(only=()):
     ensure_ref()
+
+    def want(name):
+        return not only or name in only
+
     # 1-2: the reference's own sample data (62 redwood seedlings, 128x128 mask at 1/128).
     if os.path.isdir(REF_SAMPLE):
         pts = np.loadtxt(os.path.join(REF_SAMPLE, "pntsRedwood.csv"), delimiter=",", skiprows=1)
@@ -92,12 +96,15 @@ def main():
         r = tiff.read(os.path.join(REF_SAMPLE, "redwood_edgecorrection.tif"))
         g = synth.Grid(r.data.shape[1], r.data.shape[0], np.float32(r.xll), np.float32(r.yll),
                        np.float32(r.cell_size), np.float32(r.nodata))
-        make_case("redwood_h0", x, y, w, None, g, r.data, g, r.data, 0, True, False)
-        make_case("redwood_h1", x, y, w, None, g, r.data, g, r.data, 1, True, False)
+        if want("redwood_h0"):
+            make_case("redwood_h0", x, y, w, None, g, r.data, g, r.data, 0, True, False)
+        if want("redwood_h1"):
+            make_case("redwood_h1", x, y, w, None, g, r.data, g, r.data, 1, True, False)
     # 3: 10,000 uniform points in 100 x 100, h = 2 (per-point column), all cells valid.
     c = synth.small_uniform(seed=0)
     hpp = np.full(len(c["x"]), 2.0, np.float32)
-    make_case("uniform_c0", c["x"], c["y"], c["w"], hpp, c["edge_grid"], c["edge_mask"],
+    if want("uniform_c0"):
+        make_case("uniform_c0", c["x"], c["y"], c["w"], hpp, c["edge_grid"], c["edge_mask"],
               c["density_grid"], c["density_mask"], -1, True, True)
     # 4-5: mixture points with lognormal weights under a polygon mask.
     x, y = synth.mixture_points(3000, 6, 100.0, 4.0, 15.0, seed=11)
@@ -106,23 +113,45 @@ def main():
     dg = synth.Grid(100, 100, 0.0, 0.0, 1.0)
     eg = synth.Grid(50, 50, 0.0, 0.0, 2.0)
     dm, em = synth.rasterize_polygon(poly, dg), synth.rasterize_polygon(poly, eg)
-    make_case("poly_fixed", x, y, w, np.full(3000, 3.0, np.float32), eg, em, dg, dm, -1, True, True)
+    if want("poly_fixed"):
+        make_case("poly_fixed", x, y, w, np.full(3000, 3.0, np.float32), eg, em, dg, dm, -1, True, True)
     hv = np.random.Generator(np.random.PCG64(14)).uniform(1.5, 5.0, 3000).astype(np.float32)
-    make_case("poly_varh", x, y, w, hv, eg, em, dg, dm, -1, True, True)
+    if want("poly_varh"):
+        make_case("poly_varh", x, y, w, hv, eg, em, dg, dm, -1, True, True)
     # 6: rule-of-thumb bandwidth, edge correction off, offset origin and fractional cells.
     x, y = synth.uniform_points(2000, 10.0, 60.0, seed=21)
     dg = synth.Grid(80, 64, np.float32(5.0), np.float32(7.5), np.float32(0.75))
     dm = synth.all_valid(dg)
     dm[:5, :] = dg.nodata
     dm[:, -3:] = dg.nodata
-    make_case("uniform_h0_noedge", x, y, np.ones_like(x), None, dg, dm, dg, dm, 0, False, False)
+    if want("uniform_h0_noedge"):
+        make_case("uniform_h0_noedge", x, y, np.ones_like(x), None, dg, dm, dg, dm, 0, False, False)
     # 7: golden-section LOO bandwidth search with edge correction.
     x, y = synth.mixture_points(1500, 4, 100.0, 5.0, 12.0, seed=31)
     eg = synth.Grid(50, 50, 0.0, 0.0, 2.0)
     em = synth.rasterize_polygon(synth.star_polygon(100.0, seed=33), eg)
     dg = synth.Grid(25, 25, 0.0, 0.0, 4.0)
-    make_case("loo_h1", x, y, np.ones_like(x), None, eg, em, dg, synth.all_valid(dg), 1, True, False)
+    if want("loo_h1"):
+        make_case("loo_h1", x, y, np.ones_like(x), None, eg, em, dg, synth.all_valid(dg), 1, True, False)
+
+
+    # 8-9: adaptive bandwidths (h_option 2): Hooke-Jeeves over (h0, alpha).
+    if os.path.isdir(REF_SAMPLE) and want("redwood_h2"):
+        pts = np.loadtxt(os.path.join(REF_SAMPLE, "pntsRedwood.csv"), delimiter=",", skiprows=1)
+        x, y, w = (pts[:, 0].astype(np.float32), pts[:, 1].astype(np.float32), pts[:, 2].astype(np.float32))
+        r = tiff.read(os.path.join(REF_SAMPLE, "redwood_edgecorrection.tif"))
+        g = synth.Grid(r.data.shape[1], r.data.shape[0], np.float32(r.xll), np.float32(r.yll),
+                       np.float32(r.cell_size), np.float32(r.nodata))
+        make_case("redwood_h2", x, y, w, None, g, r.data, g, r.data, 2, True, False)
+    if want("poly_h2"):
+        x, y = synth.mixture_points(800, 4, 100.0, 4.0, 14.0, seed=41)
+        w = synth.lognormal_weights(800, seed=42)
+        poly = synth.star_polygon(100.0, seed=43)
+        eg = synth.Grid(50, 50, 0.0, 0.0, 2.0)
+        dg = synth.Grid(50, 50, 0.0, 0.0, 2.0)
+        em = synth.rasterize_polygon(poly, eg)
+        make_case("poly_h2", x, y, w, None, eg, em, dg, synth.rasterize_polygon(poly, dg), 2, True, True)
 
 
 if __name__ == "__main__":
-    main()
+    main(tuple(sys.argv[1:]))

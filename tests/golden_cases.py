@@ -36,15 +36,20 @@ def oracle_run(d):
         d2 = o.dist2_boundary(x, y, eg, b)
         out["boundary"], out["dist2"] = b, d2
     h = out["h0"]
+    hs = d["hs"]
     if int(d["hoption"]) == 1:
         h, _ = o.mle_fixed_bandwidth(x, y, w, d2, eg, em, out["h0"])
+    if int(d["hoption"]) == 2:
+        # adaptive bandwidths (Hooke-Jeeves over h0, alpha; main :548-573)
+        h, alpha, lmax, hs, it = o.adaptive_search(x, y, w, d2 if int(d["edge"]) else None, eg, em, out["h0"])
+        out["alpha"], out["lmax"], out["hj_iterations"], out["hs"] = alpha, lmax, it, hs
     out["h"] = h
     if int(d["edge"]):
-        ew, out["edge_evals"] = o.edge_weights(x, y, h, d2, eg, em, hs=d["hs"])
+        ew, out["edge_evals"] = o.edge_weights(x, y, h, d2, eg, em, hs=hs)
     else:
         ew, out["edge_evals"] = np.ones(len(x)), 0
     out["ew"] = ew
-    out["density"], out["density_evals"] = o.density(x, y, w, ew, h, d["dg"], d["density_mask"], hs=d["hs"])
+    out["density"], out["density_evals"] = o.density(x, y, w, ew, h, d["dg"], d["density_mask"], hs=hs)
     return out
 
 
