@@ -247,6 +247,28 @@ int mgk_loo_loglik_batch(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask,
  * iteration (each one batched launch of nh=2); returns the bracket midpoint. */
 int mgk_mle_fixed_bandwidth(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h0,
                             float* h_opt, int* iterations);
+/* LogLikelihood with adaptive bandwidths (kde_cuda_kdtr_tiled.cu:3553-3650,
+ * the CPU branch of the h_option 2 likelihood): edge weights at h, pilot
+ * density at every point (itself included), hs_i = h (den_i / gml)^alpha with
+ * gml the geometric mean of the pilot densities (compGML, :3655-3672), edge
+ * weights at hs, then
+ *   logL = sum_j log(max(sum_{i != j, d^2 < 9 hs_i^2} K_{hs_i}(d) w_i e_i(hs), 1e-14f)).
+ * mask NULL: no edge correction (mask != NULL needs mgk_boundary_dist).
+ * Leaves hs in the points' per-point bandwidths (points that wrap caller
+ * memory get a buffer of their own; the caller's h array is not written). */
+int mgk_loglik_adaptive(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h, float alpha,
+                        double* logL);
+/* h_option 2 (main, kde_cuda_kdtr_tiled.cu:548-573): Hooke-Jeeves search
+ * (hooke_jeeves / hj_likelihood, :3677-3785) of (h, alpha) from (h0, -0.5)
+ * with steps h0/10 and 0.1, at most 30 iterations, maximising
+ * mgk_loglik_adaptive; then the bandwidths of the optimum, hs_i = h (den_i /
+ * gml)^alpha, from the pilot density at the fixed h.  hs are left in the
+ * points' per-point bandwidths and copied to hs_out (host, n floats; may be
+ * NULL).  The points' edge weights are invalidated: compute them at hs
+ * (mgk_edge_weights with h = 0) before the density.  h_opt, alpha_opt, lmax
+ * (the largest logL seen), iterations: host, each may be NULL. */
+int mgk_adaptive_bandwidths(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h0, float* h_opt,
+                            float* alpha_opt, double* lmax, int* iterations, float* hs_out);
 /* Rule-of-thumb bandwidth (kde_cuda_kdtr_tiled.cu:64-68, 1563-1595), host
  * arithmetic identical to the reference's. */
 float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* w);

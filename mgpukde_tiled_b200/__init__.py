@@ -10,12 +10,12 @@ from ._native import EXPORTS, LIB_PATH, MgkError, MgkGrid, lib  # noqa: F401
 from .kde import (Context, Grid, Index, Points, Raster, autotune, calc_dist2_boundary, density_tile,  # noqa: F401
                   get_tuning, set_tuning,
                   density_stream, density_tiles, edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
-                  mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights)
+                  mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights, loglik_adaptive, adaptive_bandwidths)
 from .serve import Server  # noqa: F401
 
 __all__ = [
     "Context", "Grid", "Index", "Points", "Raster", "MgkError", "Server", "calc_dist2_boundary", "density_tile",
     "density_stream", "density_tiles", "autotune", "get_tuning", "set_tuning",
     "edge_correction_weights", "kde_raster", "log_likelihood_batch", "mark_boundary",
-    "mle_fixed_bandwidth", "rule_of_thumb", "unit_edge_weights", "lib",
+    "mle_fixed_bandwidth", "rule_of_thumb", "unit_edge_weights", "loglik_adaptive", "adaptive_bandwidths", "lib",
 ]

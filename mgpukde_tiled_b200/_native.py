@@ -28,7 +28,7 @@ EXPORTS = [
     "mgk_mle_fixed_bandwidth", "mgk_rule_of_thumb", "mgk_kde_raster",
     "mgk_serve_create", "mgk_serve_submit", "mgk_serve_poll", "mgk_serve_wait", "mgk_serve_stats",
     "mgk_serve_destroy", "mgk_density_stream", "mgk_copy_sink", "mgk_ctx_get_tuning", "mgk_ctx_set_tuning",
-    "mgk_autotune",
+    "mgk_autotune", "mgk_loglik_adaptive", "mgk_adaptive_bandwidths",
 ]
 
 
@@ -137,6 +137,9 @@ def lib():
         "mgk_ctx_set_tuning": (I, [P, C.POINTER(MgkTuning)]),
         "mgk_autotune": (I, [P, P, C.c_float, G, C.c_char_p, C.POINTER(MgkTuning)]),
         "mgk_mle_fixed_bandwidth": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(I)]),
+        "mgk_loglik_adaptive": (I, [P, P, P, C.c_float, C.c_float, C.POINTER(C.c_double)]),
+        "mgk_adaptive_bandwidths": (I, [P, P, P, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float),
+                                        C.POINTER(C.c_double), C.POINTER(I), P]),
         "mgk_rule_of_thumb": (C.c_float, [I64, P, P, P]),
         "mgk_kde_raster": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, P, I64, P, P, C.POINTER(I64)]),
     }

@@ -20,7 +20,7 @@ REPO = os.path.dirname(PKG)
 CSRC = os.path.join(PKG, "csrc")
 LIB = os.path.join(PKG, "_lib")
 OBJ = os.path.join(PKG, "_build")
-CU_SOURCES = ["api.cu", "index.cu", "density.cu", "boundary.cu", "edge.cu", "loo.cu", "serve.cu", "stream.cu", "tune.cu"]
+CU_SOURCES = ["api.cu", "index.cu", "density.cu", "boundary.cu", "edge.cu", "loo.cu", "serve.cu", "stream.cu", "tune.cu", "adaptive.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1,0 +1,343 @@
+// Adaptive bandwidths (h_option 2): Hooke-Jeeves search over (h0, alpha).
+//
+// The reference (main, kde_cuda_kdtr_tiled.cu:548-573) starts from the
+// rule-of-thumb h0 with alpha0 = -0.5 and searches (hooke_jeeves /
+// hj_likelihood, :3677-3785) for the (h, alpha) maximising
+// LogLikelihood(h, alpha) (CPU branch :3553-3650):
+//   1. edge weights e(h) at the fixed h,
+//   2. pilot density at every point, itself included:
+//        den0_j = sum_{i, d^2 < 9h^2} K_h(d) w_i e_i(h),
+//   3. hs_i = h (den0_i / gml)^alpha, gml the geometric mean of den0 (compGML),
+//   4. edge weights e(hs) at the per-point bandwidths,
+//   5. leave-one-out density with the bandwidth of each source point:
+//        den1_j = sum_{i != j, d^2 < 9 hs_i^2} K_{hs_i}(d) w_i e_i(hs),
+//   6. logL = sum_j log max(den1_j, EPSILONDENSITY).
+// After the search the bandwidths of the optimum are computed once more
+// (steps 1-3) and used for the density raster.
+//
+// On the device: steps 1 and 4 are k_edge_rows; steps 2 and 5 are
+// k_point_density over a cell-binned index of the points (fixed-h index for
+// the pilot, per-point-h index for the LOO sum), one thread per query, the
+// candidates staged through shared memory, the cutoff decided in FP32 with a
+// band re-decided by the oracle's FP64 test, terms from the unbiased
+// polynomial exp2, Kahan-compensated FP32 partials and an FP64 result per
+// point; the geometric mean, the bandwidths and the log sum are FP64 on the
+// device (fixed-order reductions).  The search itself runs on the host with
+// the reference's float step arithmetic and its bookkeeping of the five
+// likelihoods.
+#include <algorithm>
+#include <cfloat>
+#include <cmath>
+
+#include "mgk_internal.cuh"
+
+namespace {
+
+constexpr int kPdQ = 128;  // queries (threads) per CTA
+constexpr int kPdB = 32;   // candidates per staged batch
+
+// den[perm[q]] = sum over candidates i (all points of the index within reach
+// of the CTA's 128 consecutive queries) of [in cutoff] K w_i e_i; the query
+// itself is included when SELF.  Fixed h: terms exp2(-d^2 k2) w e, times
+// 1/(h^2 TWO_PI) at the end; per-point h (VARH): the candidate's own k2 and
+// cutoff, weights already carry 1/(h_i^2 TWO_PI).
+template <bool VARH, bool SELF>
+__global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* __restrict__ pts,
+                                                        const int32_t* __restrict__ perm,
+                                                        const int32_t* __restrict__ bin_start, double ox,
+                                                        double oy, double inv_side, int64_t nbx, int64_t nby,
+                                                        double reach, double h2, double* __restrict__ den,
+                                                        unsigned long long* __restrict__ evals) {
+    __shared__ __align__(16) MgkPt st[kPdB];
+    __shared__ float bb[4][kPdQ / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t qpos = (int64_t)blockIdx.x * kPdQ + tid;
+    const bool qv = qpos < n;
+    MgkPt q{};
+    if (qv) q = pts[qpos];
+    const float qx = q.xh + q.xl, qy = q.yh + q.yl;
+    float mnx = qv ? qx : FLT_MAX, mxx = qv ? qx : -FLT_MAX, mny = qv ? qy : FLT_MAX, mxy = qv ? qy : -FLT_MAX;
+    for (int o = 16; o; o >>= 1) {
+        mnx = fminf(mnx, __shfl_xor_sync(0xffffffffu, mnx, o));
+        mxx = fmaxf(mxx, __shfl_xor_sync(0xffffffffu, mxx, o));
+        mny = fminf(mny, __shfl_xor_sync(0xffffffffu, mny, o));
+        mxy = fmaxf(mxy, __shfl_xor_sync(0xffffffffu, mxy, o));
+    }
+    if (lane == 0) {
+        bb[0][warp] = mnx;
+        bb[1][warp] = mxx;
+        bb[2][warp] = mny;
+        bb[3][warp] = mxy;
+    }
+    __syncthreads();
+    for (int i = 0; i < kPdQ / 32; i++) {
+        mnx = fminf(mnx, bb[0][i]);
+        mxx = fmaxf(mxx, bb[1][i]);
+        mny = fminf(mny, bb[2][i]);
+        mxy = fmaxf(mxy, bb[3][i]);
+    }
+    const int64_t bx0 = mgk_max64(0, (int64_t)floor(((double)mnx - reach - ox) * inv_side));
+    const int64_t bx1 = mgk_min64(nbx - 1, (int64_t)floor(((double)mxx + reach - ox) * inv_side));
+    const int64_t by0 = mgk_max64(0, (int64_t)floor(((double)mny - reach - oy) * inv_side));
+    const int64_t by1 = mgk_min64(nby - 1, (int64_t)floor(((double)mxy + reach - oy) * inv_side));
+    // fixed-h constants
+    const double cut = MGK_CUT * h2;
+    const float cutf = (float)cut;
+    const double k2 = MGK_LOG2E / (2.0 * h2);
+    const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
+    float s = 0.0f, c = 0.0f;
+    unsigned cnt = 0;
+    for (int64_t by = by0; by <= by1 && bx0 <= bx1; by++) {
+        const int64_t sb = bin_start[by * nbx + bx0], se = bin_start[by * nbx + bx1 + 1];
+        for (int64_t base = sb; base < se; base += kPdB) {
+            const int m = (int)mgk_min64(kPdB, se - base);
+            __syncthreads();
+            if (tid < m) st[tid] = pts[base + tid];
+            __syncthreads();
+            if (!qv) continue;
+            float part = 0.0f;
+            for (int t = 0; t < m; t++) {
+                const MgkPt p = st[t];
+                const float dx = __fadd_rn(__fsub_rn(p.xh, q.xh), __fsub_rn(p.xl, q.xl));
+                const float dy = __fadd_rn(__fsub_rn(p.yh, q.yh), __fsub_rn(p.yl, q.yl));
+                const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
+                const float cf = VARH ? 9.0f * p.hh : cutf;
+                bool in = d2 < cf;
+                if (fabsf(d2 - cf) <= cf * 4e-6f)  // near the cutoff: the oracle's FP64 decision
+                    in = mgk_d2_exact(qx, qy, p.xh + p.xl, p.yh + p.yl) < (VARH ? MGK_CUT * (double)p.hh : cut);
+                if (!SELF && base + t == qpos) in = false;
+                if (in) {
+                    const float a = VARH ? __fmaf_rn(d2, p.k2h, __fmul_rn(d2, p.k2l))
+                                         : __fmaf_rn(d2, k2h, __fmul_rn(d2, k2l));
+                    part = __fmaf_rn(mgk_exp2_neg_poly(a), p.wk, part);
+                    cnt++;
+                }
+            }
+            const float y = part - c;
+            const float tt = s + y;
+            c = (tt - s) - y;
+            s = tt;
+        }
+    }
+    if (qv) {
+        const double v = (double)s - (double)c;
+        den[perm[qpos]] = VARH ? v : v / (h2 * (double)MGK_TWO_PI_F);
+    }
+    if (evals) {
+        for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
+        if (lane == 0 && cnt) atomicAdd(evals, (unsigned long long)cnt);
+    }
+}
+
+// out[0] = sum_i log(max(v_i, floor)) in a fixed order (one CTA).
+__global__ void k_log_sum(int64_t n, const double* __restrict__ v, double floor_v, double* __restrict__ out) {
+    __shared__ double sh[256];
+    double a = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += log(v[i] > floor_v ? v[i] : floor_v);
+    sh[threadIdx.x] = a;
+    __syncthreads();
+    for (int o = 128; o; o >>= 1) {
+        if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = sh[0];
+}
+
+// hs_i = h (den0_i / gml)^alpha with gml = exp(logsum / n).
+__global__ void k_adaptive_h(int64_t n, const double* __restrict__ den0, const double* __restrict__ logsum, float h,
+                             float alpha, float* __restrict__ hs) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const double gml = exp(logsum[0] / (double)n);
+    hs[i] = (float)((double)h * pow(den0[i] / gml, (double)alpha));
+}
+
+int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den) {
+    if (idx->n == 0) return MGK_OK;
+    const unsigned grid = (unsigned)((idx->n + kPdQ - 1) / kPdQ);
+    cudaStream_t s = c->stream;
+    if (idx->varh)
+        k_point_density<true, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
+                                                           idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
+                                                           idx->h2, d_den, nullptr);
+    else if (self)
+        k_point_density<false, true><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
+                                                           idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
+                                                           idx->h2, d_den, nullptr);
+    else
+        k_point_density<false, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
+                                                            idx->oy, 1.0 / idx->side, idx->nbx, idx->nby,
+                                                            idx->reach, idx->h2, d_den, nullptr);
+    MGK_CHECK_LAUNCH(c, "k_point_density");
+    MGK_COUNT_LAUNCH(c, 1);
+    return MGK_OK;
+}
+
+// Steps 1-3: e(h), the pilot density with self, and hs into p->h.
+int pilot_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* d_den,
+                     double* d_scal) {
+    int st;
+    if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, h, p->dist2, r, p->ew, nullptr);
+    else st = mgk_edge_weights_unit(c, p);
+    if (st) return st;
+    p->has_ew = true;
+    mgk_index* idx = nullptr;
+    if ((st = mgk_index_build(c, p, h, 0.0f, &idx))) return st;  // h > 0: fixed-h index
+    st = point_density(c, idx, true, d_den);
+    if (st == MGK_OK) {
+        k_log_sum<<<1, 256, 0, c->stream>>>(p->n, d_den, 0.0, d_scal);
+        k_adaptive_h<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->n, d_den, d_scal, h, alpha, p->h);
+        MGK_COUNT_LAUNCH(c, 2);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths");
+    }
+    mgk_index_destroy(idx);
+    return st;
+}
+
+// LogLikelihood(h, alpha): steps 1-6.
+int loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* d_den,
+                    double* d_scal, double* logl) {
+    int st = pilot_bandwidths(c, p, r, h, alpha, d_den, d_scal);
+    if (st) return st;
+    if (r && (st = mgk_launch_edge_weights(c, p->n, p->x, p->y, p->h, 0.0f, p->dist2, r, p->ew, nullptr))) return st;
+    mgk_index* idx = nullptr;
+    if ((st = mgk_index_build(c, p, 0.0f, 0.0f, &idx))) return st;  // per-point h
+    st = point_density(c, idx, false, d_den);
+    mgk_index_destroy(idx);
+    if (st) return st;
+    k_log_sum<<<1, 256, 0, c->stream>>>(p->n, d_den, (double)MGK_EPS_DENSITY_F, d_scal + 1);
+    MGK_COUNT_LAUNCH(c, 1);
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(c->h_sum, d_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    *logl = c->h_sum[0];
+    return MGK_OK;
+}
+
+// The search writes the bandwidths into p->h.  Points that wrap caller
+// memory get a buffer of their own, so the caller's array is never written.
+int ensure_h(mgk_ctx* c, mgk_points* p) {
+    if (p->h && (p->owns_xywh || p->owns_h)) return MGK_OK;
+    float* h = nullptr;
+    const int st = mgk_alloc(c, (void**)&h, sizeof(float) * (size_t)std::max<int64_t>(p->n, 1));
+    if (st) return st;
+    p->h = h;
+    if (!p->owns_xywh) p->owns_h = true;
+    return MGK_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int mgk_loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* logl) {
+    if (!c || !p || !logl || !(h > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "loglik_adaptive: bad arguments");
+    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loglik_adaptive: run mgk_boundary_dist first");
+    int st;
+    if ((st = ensure_h(c, p))) return st;
+    double *d_den = nullptr, *d_scal = nullptr;
+    const size_t bd = sizeof(double) * (size_t)std::max<int64_t>(p->n, 1);
+    if ((st = mgk_alloc(c, (void**)&d_den, bd))) return st;
+    if ((st = mgk_alloc(c, (void**)&d_scal, 2 * sizeof(double)))) {
+        mgk_free(c, d_den, bd);
+        return st;
+    }
+    st = loglik_adaptive(c, p, r, h, alpha, d_den, d_scal, logl);
+    mgk_free(c, d_den, bd);
+    mgk_free(c, d_scal, 2 * sizeof(double));
+    return st;
+}
+
+int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h0, float* h_opt,
+                            float* alpha_opt, double* lmax, int* iterations, float* hs_out) {
+    if (!c || !p || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "adaptive_bandwidths: bad arguments");
+    if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "adaptive_bandwidths: run mgk_boundary_dist first");
+    int st;
+    if ((st = ensure_h(c, p))) return st;
+    double *d_den = nullptr, *d_scal = nullptr;
+    const size_t bd = sizeof(double) * (size_t)std::max<int64_t>(p->n, 1);
+    if ((st = mgk_alloc(c, (void**)&d_den, bd))) return st;
+    if ((st = mgk_alloc(c, (void**)&d_scal, 2 * sizeof(double)))) {
+        mgk_free(c, d_den, bd);
+        return st;
+    }
+    // hooke_jeeves (kde_cuda_kdtr_tiled.cu:3726-3785): float steps, five likelihoods
+    float alpha0 = -0.5f;
+    float stepH = h0 / 10;
+    float stepA = 0.1f;
+    double L[5] = {0, 0, 0, 0, 0};
+    auto ll = [&](float h, float a, double* out) { return loglik_adaptive(c, p, r, h, a, d_den, d_scal, out); };
+    // hj_likelihood (:3677-3720): the centre and the neighbours the last move did not keep
+    auto around = [&](int last) {
+        int s2 = MGK_OK;
+        if (s2 == MGK_OK && last == -1) s2 = ll(h0, alpha0, &L[0]);
+        if (s2 == MGK_OK && last != 2) s2 = ll(h0 - stepH, alpha0, &L[1]);
+        if (s2 == MGK_OK && last != 1) s2 = ll(h0 + stepH, alpha0, &L[2]);
+        if (s2 == MGK_OK && last != 4) s2 = ll(h0, alpha0 + stepA, &L[3]);
+        if (s2 == MGK_OK && last != 3) s2 = ll(h0, alpha0 - stepA, &L[4]);
+        return s2;
+    };
+    st = around(-1);
+    double Lm = L[0];
+    const float sH = stepH / 10, sA = stepA / 10;
+    int it = 0;
+    while (st == MGK_OK && (stepH > sH || stepA > sA) && (h0 - stepH > 0) && it <= 30) {  // MAX_NUM_ITERATIONS
+        int dmax = 0;
+        for (int i = 0; i < 5; i++)
+            if (L[i] > Lm) {
+                Lm = L[i];
+                dmax = i;
+            }
+        if (dmax == 0) {
+            stepH = stepH / 2;
+            stepA = stepA / 2;
+        } else {
+            // the reference's moves and its bookkeeping of the kept likelihoods
+            // (:3750-3778), the move to +stepA included
+            if (dmax == 1) {
+                h0 = h0 - stepH;
+                L[2] = L[0];
+                L[0] = L[1];
+            }
+            if (dmax == 2) {
+                h0 = h0 + stepH;
+                L[1] = L[0];
+                L[0] = L[2];
+            }
+            if (dmax == 3) {
+                alpha0 = alpha0 + stepA;
+                L[3] = L[0];
+                L[0] = L[4];
+            }
+            if (dmax == 4) {
+                alpha0 = alpha0 - stepA;
+                L[3] = L[0];
+                L[0] = L[4];
+            }
+        }
+        st = around(dmax);
+        it++;
+    }
+    // final bandwidths at the optimum (main :566-572)
+    if (st == MGK_OK) st = pilot_bandwidths(c, p, r, h0, alpha0, d_den, d_scal);
+    if (st == MGK_OK && hs_out && p->n > 0) {
+        const cudaError_t e = cudaMemcpyAsync(hs_out, p->h, sizeof(float) * (size_t)p->n, cudaMemcpyDeviceToHost,
+                                              c->stream);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths download");
+    }
+    if (st == MGK_OK) {
+        const cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths");
+    }
+    mgk_free(c, d_den, bd);
+    mgk_free(c, d_scal, 2 * sizeof(double));
+    if (st) return st;
+    p->has_ew = false;  // the weights left behind belong to the fixed h0; recompute at hs
+    if (h_opt) *h_opt = h0;
+    if (alpha_opt) *alpha_opt = alpha0;
+    if (lmax) *lmax = Lm;
+    if (iterations) *iterations = it;
+    return MGK_OK;
+}
+
+}  // extern "C"

@@ -253,6 +253,8 @@ int mgk_points_destroy(mgk_points* p) {
         mgk_free(c, p->y, b);
         mgk_free(c, p->w, b);
         mgk_free(c, p->h, b);
+    } else if (p->owns_h) {
+        mgk_free(c, p->h, b);
     }
     mgk_free(c, p->dist2, sizeof(double) * (size_t)std::max<int64_t>(p->n, 1));
     mgk_free(c, p->ew, b);

@@ -9,7 +9,7 @@
 //
 // The 14 positional arguments keep their meaning.  h_option: 0 rule of thumb,
 // 1 leave-one-out maximum likelihood (golden section), -1 per-point h from
-// the CSV.  h_option 2 (adaptive) is not part of this build and is rejected.
+// the CSV, 2 adaptive bandwidths (Hooke-Jeeves over h0 and alpha).
 // The OpenMP CPU path (skip_omp_parallel = 0) is not part of this build: only
 // the GPU path runs and writes denfn_cuda and pntsCUDA.csv.  num_gpu > 1 runs
 // on one GPU (this build is single-GPU; tiles need no exchange).
@@ -186,10 +186,6 @@ int main(int argc, char** argv) {
         std::printf("***Error - should never use bandwidth option -1 in mode 0 (i.e., randomly generately points). Exiting...");
         return 1;
     }
-    if (a.hoption == 2) {
-        std::printf("***Error - h_option 2 (adaptive bandwidth) is not part of this build. Exiting...\n");
-        return 1;
-    }
     if (a.hoption < -1 || a.hoption > 2) {
         std::printf("***Error - unknown h_option %d\n", a.hoption);
         return 1;
@@ -285,7 +281,20 @@ int main(int argc, char** argv) {
                         ms_since(t1));
             h = hopt;
         }
-        const float hfinal = a.hoption == -1 ? 0.0f : h;
+        if (a.hoption == 2) {  // adaptive bandwidths (main, kde_cuda_kdtr_tiled.cu:548-573)
+            float hopt = h, aopt = -0.5f;
+            double lmax = 0.0;
+            int it = 0;
+            hpp.assign((size_t)n, 0.0f);
+            t1 = Clock::now();
+            if (check(ctx, mgk_adaptive_bandwidths(ctx, pts, em, h, &hopt, &aopt, &lmax, &it, hpp.data()),
+                      "adaptive bandwidth search"))
+                break;
+            std::printf("h0: %.5f alpha0: %.5f Lmax: %.5f (%d iterations, %.0f ms)\n", hopt, aopt, lmax, it,
+                        ms_since(t1));
+            h = hopt;
+        }
+        const float hfinal = (a.hoption == -1 || a.hoption == 2) ? 0.0f : h;
         (void)hcall;
         t1 = Clock::now();
         if (a.edge) {

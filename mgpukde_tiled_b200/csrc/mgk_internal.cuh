@@ -53,6 +53,7 @@ struct mgk_points {
     int64_t n = 0;
     float *x = nullptr, *y = nullptr, *w = nullptr, *h = nullptr;
     bool owns_xywh = false;
+    bool owns_h = false;  // h allocated by the adaptive search on points that do not own x/y/w/h
     double* dist2 = nullptr;
     bool has_dist2 = false;
     float* ew = nullptr;

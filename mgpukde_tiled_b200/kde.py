@@ -356,6 +356,23 @@ def mle_fixed_bandwidth(ctx: Context, points: Points, raster: Raster | None, h0:
     return h.value, it.value
 
 
+def loglik_adaptive(ctx: Context, points: Points, raster: Raster | None, h: float, alpha: float) -> float:
+    """LogLikelihood(h, alpha) with adaptive bandwidths (h_option 2)."""
+    v = C.c_double()
+    ctx.check(lib().mgk_loglik_adaptive(ctx.handle, points._h, raster._h if raster else None, float(h),
+                                        float(alpha), C.byref(v)))
+    return v.value
+
+
+def adaptive_bandwidths(ctx: Context, points: Points, raster: Raster | None, h0: float):
+    """h_option 2: Hooke-Jeeves over (h, alpha); returns (h, alpha, lmax, iterations, hs[n])."""
+    h, a, lm, it = C.c_float(), C.c_float(), C.c_double(), C.c_int()
+    hs = np.empty(points.n, np.float32)
+    ctx.check(lib().mgk_adaptive_bandwidths(ctx.handle, points._h, raster._h if raster else None, float(h0),
+                                            C.byref(h), C.byref(a), C.byref(lm), C.byref(it), _ptr(hs)))
+    return h.value, a.value, lm.value, it.value, hs
+
+
 def rule_of_thumb(x, y, w=None) -> float:
     x, y, w = _f32(x), _f32(y), _f32(w)
     return float(lib().mgk_rule_of_thumb(len(x), _ptr(x), _ptr(y), _ptr(w)))

@@ -33,8 +33,8 @@ def run_cli(args, cwd):
 def test_cli_rejects_bad_arguments(tmp_path):
     p = run_cli(["0", "100"], tmp_path)
     assert p.returncode == 1 and "Incorrect arguments" in p.stdout
-    p = run_cli("0 100 1 1 2 1 0 1 0 1 1 a.tif b.tif 0".split(), tmp_path)
-    assert p.returncode == 1 and "h_option 2" in p.stdout
+    p = run_cli("0 100 1 1 3 1 0 1 0 1 1 a.tif b.tif 0".split(), tmp_path)
+    assert p.returncode == 1 and "unknown h_option 3" in p.stdout
     p = run_cli("0 100 1 1 -1 1 0 1 0 1 1 a.tif b.tif 0".split(), tmp_path)
     assert p.returncode == 1 and "bandwidth option -1 in mode 0" in p.stdout
 

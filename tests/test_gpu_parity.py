@@ -32,10 +32,11 @@ def rel_err(got, ref):
     return np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
 
 
-def run_components(ctx, d, h, count=True):
-    """boundary -> distance -> edge weights -> index -> one-tile density through the C ABI."""
+def run_components(ctx, d, h, count=True, hs=None):
+    """boundary -> distance -> edge weights -> index -> one-tile density through the C ABI.
+    hs: per-point bandwidths (default: the case's own, if any)."""
     x, y, w = d["x"], d["y"], d["w"]
-    hs = d["hs"]
+    hs = d["hs"] if hs is None else hs
     eg, dg = mk.Grid.of(d["eg"]), mk.Grid.of(d["dg"])
     pts = mk.Points.upload(ctx, x, y, w, hs)
     res = {}
@@ -64,7 +65,7 @@ def run_components(ctx, d, h, count=True):
 def test_golden_case_components(ctx, case):
     d = load(case)
     ref = oracle_run(d)
-    r = run_components(ctx, d, ref["h"])
+    r = run_components(ctx, d, ref["h"], hs=ref.get("hs"))  # h_option 2: the oracle's adaptive h
     nd = d["density_mask"] == d["dg"].nodata
     assert np.array_equal(r["density"][nd], d["density_mask"][nd])
     assert rel_err(r["density"][~nd], ref["density"][~nd]).max() <= RTOL
@@ -176,7 +177,7 @@ def test_errors_leave_device_usable(ctx):
     # the device still works
     d = load("uniform_h0_noedge")
     ref = oracle_run(d)
-    r = run_components(ctx, d, ref["h"])
+    r = run_components(ctx, d, ref["h"], hs=ref.get("hs"))  # h_option 2: the oracle's adaptive h
     nd = d["density_mask"] == d["dg"].nodata
     assert rel_err(r["density"][~nd], ref["density"][~nd]).max() <= RTOL
 
