@@ -266,7 +266,8 @@ int mgk_loglik_adaptive(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, f
  * points' per-point bandwidths and copied to hs_out (host, n floats; may be
  * NULL).  The points' edge weights are invalidated: compute them at hs
  * (mgk_edge_weights with h = 0) before the density.  h_opt, alpha_opt, lmax
- * (the largest logL seen), iterations: host, each may be NULL. */
+ * (the largest logL seen, held as a float like the reference's), iterations:
+ * host, each may be NULL. */
 int mgk_adaptive_bandwidths(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, float h0, float* h_opt,
                             float* alpha_opt, double* lmax, int* iterations, float* hs_out);
 /* Rule-of-thumb bandwidth (kde_cuda_kdtr_tiled.cu:64-68, 1563-1595), host

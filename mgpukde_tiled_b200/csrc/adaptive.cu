@@ -265,8 +265,15 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
     float alpha0 = -0.5f;
     float stepH = h0 / 10;
     float stepA = 0.1f;
-    double L[5] = {0, 0, 0, 0, 0};
-    auto ll = [&](float h, float a, double* out) { return loglik_adaptive(c, p, r, h, a, d_den, d_scal, out); };
+    // the likelihoods are kept as floats, the type of the reference's Ls array,
+    // so that ties and near-ties compare as they do there
+    float L[5] = {0, 0, 0, 0, 0};
+    auto ll = [&](float h, float a, float* out) {
+        double v = 0.0;
+        const int s1 = loglik_adaptive(c, p, r, h, a, d_den, d_scal, &v);
+        *out = (float)v;
+        return s1;
+    };
     // hj_likelihood (:3677-3720): the centre and the neighbours the last move did not keep
     auto around = [&](int last) {
         int s2 = MGK_OK;
@@ -278,7 +285,7 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
         return s2;
     };
     st = around(-1);
-    double Lm = L[0];
+    float Lm = L[0];
     const float sH = stepH / 10, sA = stepA / 10;
     int it = 0;
     while (st == MGK_OK && (stepH > sH || stepA > sA) && (h0 - stepH > 0) && it <= 30) {  // MAX_NUM_ITERATIONS

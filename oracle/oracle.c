@@ -500,15 +500,17 @@ double orc_loglik_adaptive(int64_t n, const float* x, const float* y, const floa
 }
 
 /* hj_likelihood, kde_cuda_kdtr_tiled.cu:3677-3720: the likelihoods of the
- * centre and its four neighbours, skipping the ones the last move kept. */
+ * centre and its four neighbours, skipping the ones the last move kept.
+ * They are kept as floats, the type of the reference's Ls array, so ties and
+ * near-ties compare as they do there. */
 static void hj_likelihoods(int64_t n, const float* x, const float* y, const float* w, const double* dist2,
                            const orc_grid* g, const float* mask, float h0, float a0, float sh, float sa,
-                           int last, double* L) {
-    if (last == -1) L[0] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0, NULL);
-    if (last != 2) L[1] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 - sh, a0, NULL);
-    if (last != 1) L[2] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 + sh, a0, NULL);
-    if (last != 4) L[3] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 + sa, NULL);
-    if (last != 3) L[4] = orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 - sa, NULL);
+                           int last, float* L) {
+    if (last == -1) L[0] = (float)orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0, NULL);
+    if (last != 2) L[1] = (float)orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 - sh, a0, NULL);
+    if (last != 1) L[2] = (float)orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0 + sh, a0, NULL);
+    if (last != 4) L[3] = (float)orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 + sa, NULL);
+    if (last != 3) L[4] = (float)orc_loglik_adaptive(n, x, y, w, dist2, g, mask, h0, a0 - sa, NULL);
 }
 
 void orc_adaptive_search(int64_t n, const float* x, const float* y, const float* w,
@@ -517,9 +519,9 @@ void orc_adaptive_search(int64_t n, const float* x, const float* y, const float*
     float alpha0 = -0.5f;
     float stepH = h0 / 10;
     float stepA = 0.1f;
-    double L[5];
+    float L[5];
     hj_likelihoods(n, x, y, w, dist2, g, mask, h0, alpha0, stepH, stepA, -1, L);
-    double Lmax = L[0];
+    float Lmax = L[0];
     const float s = stepH / 10;
     const float a = stepA / 10;
     int it = 0;
@@ -562,7 +564,7 @@ void orc_adaptive_search(int64_t n, const float* x, const float* y, const float*
     }
     out3[0] = h0;
     out3[1] = alpha0;
-    out3[2] = (float)Lmax;
+    out3[2] = Lmax;
     if (iterations) *iterations = it;
     /* final bandwidths, main :566-572 */
     const size_t nn = (size_t)(n > 0 ? n : 1);
