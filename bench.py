@@ -1,7 +1,7 @@
 """Benchmark: kernel evaluations/s of the tiled fixed-bandwidth KDE on B200.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl mgk|reference]
-                  [--workload single_large] [--scale S]
+                  [--workload single_large|bandwidth_select|out_of_core|serving|adaptive] [--scale S]
 
 Workload (default): the single large KDE — 1,000,000 points from a
 50-component Gaussian mixture in a 10,000 x 10,000 domain with lognormal(0,
@@ -519,6 +519,132 @@ def run_bandwidth_select(args):
     return 0
 
 
+# ------------------------------------------------- adaptive bandwidths (h_option 2) --
+def adaptive_cpu_baseline(scale):
+    """One adaptive likelihood evaluation of the FP64 oracle port, all host
+    threads, on the workload's points and mask: edge weights at h, pilot
+    density, bandwidths, edge weights at hs, leave-one-out density."""
+    import oracle_py as o
+
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    c = synth.bandwidth_select(scale=scale, seed=5, nh=2)
+    x, y, w = c["x"], c["y"], c["w"]
+    eg, em = o.grid(*c["edge_grid"].astuple()), c["edge_mask"]
+    d2 = o.dist2_boundary(x, y, eg, o.mark_boundary(eg, em))
+    h = o.rule_of_thumb(x, y, w)
+    t0 = time.perf_counter()
+    ew1, e1 = o.edge_weights(x, y, h, d2, eg, em)
+    den0, p0 = o.point_density(x, y, w, ew1, h, self_term=True)
+    hs = o.adaptive_bandwidths(den0, h, -0.5)
+    ew2, e2 = o.edge_weights(x, y, 0.0, d2, eg, em, hs=hs)
+    _, p1 = o.point_density(x, y, w, ew2, 0.0, hs=hs, self_term=False)
+    t = time.perf_counter() - t0
+    ev = e1 + e2 + p0 + p1
+    return {"value": ev / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"one adaptive likelihood evaluation (h = rule of thumb {h:.3f}, alpha = -0.5) of the FP64 "
+                      f"oracle on the workload ({len(x)} points, edge mask "
+                      f"{c['edge_grid'].ncols}^2): {e1 + e2} edge-mask cells, {p0 + p1} pairs",
+            "seconds": t}
+
+
+def run_adaptive(args):
+    """One step = one adaptive-bandwidth search (h_option 2) on device-resident
+    points and edge mask: point-to-boundary distances, the Hooke-Jeeves search
+    over (h, alpha) from the rule-of-thumb h0 (each likelihood: edge weights
+    at h, pilot density, bandwidths, edge weights at hs, leave-one-out density
+    at hs), then the bandwidths of the optimum, copied to the host.
+    Evals = edge-mask cells plus point pairs inside the cutoffs, summed over
+    every likelihood the search evaluates.  e2e: the same search through the
+    public API from host arrays (points and mask uploaded every step)."""
+    import torch
+
+    import mgpukde_tiled_b200 as mk
+
+    rank, world, local = env_rank()
+    if world > 1:
+        raise SystemExit("adaptive runs on one GPU (replicas only)")
+    torch.cuda.set_device(local)
+    c = synth.bandwidth_select(scale=0.5 * args.scale, seed=5, nh=2)
+    eg = mk.Grid.of(c["edge_grid"])
+    h0 = mk.rule_of_thumb(c["x"], c["y"], c["w"])
+    stream = torch.cuda.current_stream()
+    ctx = mk.Context(local, stream=stream)
+    dx = torch.from_numpy(c["x"]).cuda()
+    dy = torch.from_numpy(c["y"]).cuda()
+    dw = torch.from_numpy(c["w"]).cuda()
+    demask = torch.from_numpy(c["edge_mask"]).cuda()
+    pts = mk.Points.wrap(ctx, dx, dy, dw)
+    em = mk.Raster.wrap(ctx, eg, demask)
+    mk.mark_boundary(ctx, em)
+
+    def step():
+        mk.calc_dist2_boundary(ctx, pts, em)
+        return mk.adaptive_bandwidths(ctx, pts, em, h0)
+
+    h, alpha, lmax, iters, _ = step()
+    edge_ev, pair_ev = ctx.last_loo_evals
+    evals = edge_ev + pair_ev
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = ctx.kernel_launches
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    launches = (ctx.kernel_launches - l0) / args.steps
+
+    # end to end from host arrays: upload points and mask, boundary, search, hs to host
+    hx, hy, hw = (torch.from_numpy(c[k]).pin_memory() for k in ("x", "y", "w"))
+    hmask = torch.from_numpy(c["edge_mask"]).pin_memory()
+
+    def e2e_step():
+        p = mk.Points.upload(ctx, hx.numpy(), hy.numpy(), hw.numpy())
+        r = mk.Raster.upload(ctx, eg, hmask.numpy())
+        mk.mark_boundary(ctx, r)
+        mk.calc_dist2_boundary(ctx, p, r)
+        out = mk.adaptive_bandwidths(ctx, p, r, h0)
+        p.close()
+        r.close()
+        return out
+
+    e2e_step()
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1) / args.steps
+    n = len(c["x"])
+    out = {"metric": METRIC, "value": evals / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+           "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
+           "config": {"workload": f"adaptive: {n} mixture points (20 comps) in {eg.ncols * 4}^2, unit weights, "
+                                  f"edge mask {eg.ncols}^2 @ cell 4, Hooke-Jeeves over (h, alpha) from the "
+                                  f"rule-of-thumb h0 = {h0:.3f}, alpha0 = -0.5",
+                      "scale": args.scale, "l2": "point records and edge weights stay L2-resident"},
+           "evals_per_step": evals, "edge_evals": edge_ev, "pair_evals": pair_ev,
+           "search": {"h": h, "alpha": alpha, "lmax": lmax, "iterations": iters},
+           "e2e": {"value": evals / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
+                   "h2d_bytes_per_step": int(3 * 4 * n + c["edge_mask"].nbytes), "d2h_bytes_per_step": int(4 * n)},
+           "gpu_launches": launches, "clocks": clocks}
+    if not args.no_cpu_baseline:
+        out["cpu_baseline"] = adaptive_cpu_baseline(0.5 * args.scale)
+    print(json.dumps(out))
+    pts.close()
+    em.close()
+    ctx.close()
+    return 0
+
+
 # ---------------------------------------------------------- out of core (C3) --
 def run_out_of_core(args):
     """One step = the whole out-of-core job from device-resident points and
@@ -672,6 +798,8 @@ def main():
         return run_serving(args)
     if args.workload == "out_of_core":
         return run_out_of_core(args)
+    if args.workload == "adaptive":
+        return run_adaptive(args)
     return run_mgk(args)
 
 

@@ -75,10 +75,13 @@ const char* mgk_status_string(int status);
  * kernel (CUDA events on the context stream around that one launch). */
 uint64_t mgk_ctx_kernel_launches(const mgk_ctx* ctx);
 float mgk_ctx_last_density_ms(const mgk_ctx* ctx);
-/* Instrumentation of the last mgk_loo_loglik_batch / golden-section step: the
- * device time in ms of the batch (CUDA events on the context stream around
- * the edge weights, the gather, the sums and the argmax) and its algorithmic
- * eval counts (edge-mask cells in the cutoff, point pairs in the cutoff).
+/* Instrumentation of the last likelihood computation: an
+ * mgk_loo_loglik_batch / golden-section step (the device time in ms of the
+ * batch: CUDA events on the context stream around the edge weights, the
+ * gather, the sums and the argmax), or a whole mgk_loglik_adaptive /
+ * mgk_adaptive_bandwidths call (events around all of its work, host waits
+ * included); and its algorithmic eval counts (edge-mask cells in the cutoff,
+ * point pairs in the cutoff, summed over every likelihood evaluated).
  * No reference counterpart. */
 float mgk_ctx_last_loo_ms(const mgk_ctx* ctx);
 int mgk_ctx_last_loo_evals(const mgk_ctx* ctx, int64_t* edge_evals, int64_t* loo_evals);

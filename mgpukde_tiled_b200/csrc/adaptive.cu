@@ -152,6 +152,30 @@ __global__ void k_adaptive_h(int64_t n, const double* __restrict__ den0, const d
     hs[i] = (float)((double)h * pow(den0[i] / gml, (double)alpha));
 }
 
+// Counters of a likelihood computation: context counter slots 5 (edge-mask
+// cells) and 6 (point pairs inside the cutoff), accumulated over all steps.
+unsigned long long* edge_count(mgk_ctx* c) { return c->d_counter + 5; }
+unsigned long long* pair_count(mgk_ctx* c) { return c->d_counter + 6; }
+
+int count_begin(mgk_ctx* c) {
+    MGK_CHECK_CUDA(c, cudaMemsetAsync(c->d_counter + 5, 0, 2 * sizeof(unsigned long long), c->stream));
+    MGK_CHECK_CUDA(c, cudaEventRecord(c->ev_a, c->stream));
+    return MGK_OK;
+}
+
+// Reads the counters and the time since count_begin into the context
+// (mgk_ctx_last_loo_evals / mgk_ctx_last_loo_ms).
+int count_end(mgk_ctx* c) {
+    MGK_CHECK_CUDA(c, cudaEventRecord(c->ev_b, c->stream));
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(c->h_counter + 5, c->d_counter + 5, 2 * sizeof(unsigned long long),
+                                      cudaMemcpyDeviceToHost, c->stream));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    c->last_loo_evals[0] = (int64_t)c->h_counter[5];
+    c->last_loo_evals[1] = (int64_t)c->h_counter[6];
+    MGK_CHECK_CUDA(c, cudaEventElapsedTime(&c->last_loo_ms, c->ev_a, c->ev_b));
+    return MGK_OK;
+}
+
 int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den) {
     if (idx->n == 0) return MGK_OK;
     const unsigned grid = (unsigned)((idx->n + kPdQ - 1) / kPdQ);
@@ -159,15 +183,15 @@ int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den) {
     if (idx->varh)
         k_point_density<true, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
                                                            idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, d_den, nullptr);
+                                                           idx->h2, d_den, pair_count(c));
     else if (self)
         k_point_density<false, true><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
                                                            idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, d_den, nullptr);
+                                                           idx->h2, d_den, pair_count(c));
     else
         k_point_density<false, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
                                                             idx->oy, 1.0 / idx->side, idx->nbx, idx->nby,
-                                                            idx->reach, idx->h2, d_den, nullptr);
+                                                            idx->reach, idx->h2, d_den, pair_count(c));
     MGK_CHECK_LAUNCH(c, "k_point_density");
     MGK_COUNT_LAUNCH(c, 1);
     return MGK_OK;
@@ -177,7 +201,7 @@ int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den) {
 int pilot_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* d_den,
                      double* d_scal) {
     int st;
-    if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, h, p->dist2, r, p->ew, nullptr);
+    if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, h, p->dist2, r, p->ew, edge_count(c));
     else st = mgk_edge_weights_unit(c, p);
     if (st) return st;
     p->has_ew = true;
@@ -200,7 +224,8 @@ int loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, flo
                     double* d_scal, double* logl) {
     int st = pilot_bandwidths(c, p, r, h, alpha, d_den, d_scal);
     if (st) return st;
-    if (r && (st = mgk_launch_edge_weights(c, p->n, p->x, p->y, p->h, 0.0f, p->dist2, r, p->ew, nullptr))) return st;
+    if (r && (st = mgk_launch_edge_weights(c, p->n, p->x, p->y, p->h, 0.0f, p->dist2, r, p->ew, edge_count(c))))
+        return st;
     mgk_index* idx = nullptr;
     if ((st = mgk_index_build(c, p, 0.0f, 0.0f, &idx))) return st;  // per-point h
     st = point_density(c, idx, false, d_den);
@@ -242,7 +267,9 @@ int mgk_loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h,
         mgk_free(c, d_den, bd);
         return st;
     }
-    st = loglik_adaptive(c, p, r, h, alpha, d_den, d_scal, logl);
+    st = count_begin(c);
+    if (st == MGK_OK) st = loglik_adaptive(c, p, r, h, alpha, d_den, d_scal, logl);
+    if (st == MGK_OK) st = count_end(c);
     mgk_free(c, d_den, bd);
     mgk_free(c, d_scal, 2 * sizeof(double));
     return st;
@@ -284,7 +311,8 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
         if (s2 == MGK_OK && last != 3) s2 = ll(h0, alpha0 - stepA, &L[4]);
         return s2;
     };
-    st = around(-1);
+    st = count_begin(c);
+    if (st == MGK_OK) st = around(-1);
     float Lm = L[0];
     const float sH = stepH / 10, sA = stepA / 10;
     int it = 0;
@@ -332,10 +360,7 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
                                               c->stream);
         if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths download");
     }
-    if (st == MGK_OK) {
-        const cudaError_t e = cudaStreamSynchronize(c->stream);
-        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths");
-    }
+    if (st == MGK_OK) st = count_end(c);
     mgk_free(c, d_den, bd);
     mgk_free(c, d_scal, 2 * sizeof(double));
     if (st) return st;

@@ -72,10 +72,30 @@ def test_loglik_adaptive_matches_oracle(ctx, case):
     h0 = o.rule_of_thumb(x, y, w)
     pts, em, d2 = setup(ctx, d)
     mask = d["edge_mask"] if int(d["edge"]) else None
+    eg = d["eg"] if mask is not None else None
     for h, a in ((h0, -0.5), (0.7 * h0, -0.2), (1.4 * h0, -0.8)):
-        ref, _ = o.loglik_adaptive(x, y, w, d2, d["eg"] if mask is not None else None, mask, h, a)
+        ref, _ = o.loglik_adaptive(x, y, w, d2, eg, mask, h, a)
         got = mk.loglik_adaptive(ctx, pts, em, h, a)
         assert abs(got - ref) <= 1e-8 * abs(ref), (h, a, got, ref)
+        # eval counts of the same steps in the oracle: edge-mask cells at h and
+        # at hs, pilot pairs (self included) and leave-one-out pairs
+        if mask is not None:
+            ew1, e1 = o.edge_weights(x, y, h, d2, eg, mask)
+        else:
+            ew1, e1 = np.ones(len(x)), 0
+        den0, p0 = o.point_density(x, y, w, ew1, h, self_term=True)
+        hs = o.adaptive_bandwidths(den0, h, a)
+        if mask is not None:
+            ew2, e2 = o.edge_weights(x, y, 0.0, d2, eg, mask, hs=hs)
+        else:
+            ew2, e2 = np.ones(len(x)), 0
+        _, p1 = o.point_density(x, y, w, ew2, 0.0, hs=hs, self_term=False)
+        edge_ev, pair_ev = ctx.last_loo_evals
+        # the device's hs may differ from the oracle's by one float ulp, which
+        # can move a pair or a cell lying exactly at a cutoff
+        assert abs(edge_ev - (e1 + e2)) <= 1e-6 * (e1 + e2)
+        assert abs(pair_ev - (p0 + p1)) <= 1e-6 * (p0 + p1)
+        assert ctx.last_loo_ms > 0.0
 
 
 @pytest.mark.parametrize("case", ["redwood_h2", "poly_h2"])
