@@ -78,6 +78,31 @@ int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes) {
     return MGK_OK;
 }
 
+int mgk_host_stage(mgk_ctx* c, size_t bytes, void** host, void** dev) {
+    if (bytes > c->h_stage_bytes) {
+        if (c->h_stage) cudaFreeHost(c->h_stage);
+        c->h_stage = nullptr;
+        c->d_stage = nullptr;
+        c->h_stage_bytes = 0;
+        const size_t want = std::max<size_t>(bytes + bytes / 4, 1 << 16);
+        cudaError_t e = cudaHostAlloc(&c->h_stage, want, cudaHostAllocMapped);
+        if (e != cudaSuccess) {
+            c->h_stage = nullptr;
+            return mgk_cuda_fail(c, e, "mapped page-locked staging");
+        }
+        e = cudaHostGetDevicePointer(&c->d_stage, c->h_stage, 0);
+        if (e != cudaSuccess) {
+            cudaFreeHost(c->h_stage);
+            c->h_stage = nullptr;
+            return mgk_cuda_fail(c, e, "mapped page-locked staging address");
+        }
+        c->h_stage_bytes = want;
+    }
+    *host = c->h_stage;
+    *dev = c->d_stage;
+    return MGK_OK;
+}
+
 void mgk_free(mgk_ctx* ctx, void* p, size_t bytes) {
     if (!p) return;
     ctx->pool.emplace(size_class(bytes ? bytes : 16), p);
@@ -145,6 +170,7 @@ int mgk_ctx_destroy(mgk_ctx* c) {
     if (c->d_sum) cudaFree(c->d_sum);
     if (c->h_counter) cudaFreeHost(c->h_counter);
     if (c->h_sum) cudaFreeHost(c->h_sum);
+    if (c->h_stage) cudaFreeHost(c->h_stage);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -578,22 +604,99 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
 }
 
 // ---------------------------------------------------------- whole raster --
+// The tiles go through a three-stream pipeline: the mask of tile k+1 is
+// copied in (stream h2d) and the density of tile k-1 copied out (stream d2h)
+// while tile k is computed on the context stream, with two device buffers
+// of each kind and events between the stages.  Without an explicit tile
+// side the raster is cut into full-width bands of about an eighth of its
+// rows (at least 256, a multiple of the 64-row density block), so that the
+// copies in and out hide under the density of the neighbouring bands.
+namespace {
+struct RasterPipe {
+    cudaStream_t h2d = nullptr, d2h = nullptr;
+    cudaEvent_t mask_ready[2] = {}, done[2] = {}, out_free[2] = {};
+    ~RasterPipe() {
+        for (int i = 0; i < 2; i++) {
+            if (mask_ready[i]) cudaEventDestroy(mask_ready[i]);
+            if (done[i]) cudaEventDestroy(done[i]);
+            if (out_free[i]) cudaEventDestroy(out_free[i]);
+        }
+        if (h2d) cudaStreamDestroy(h2d);
+        if (d2h) cudaStreamDestroy(d2h);
+    }
+    cudaError_t init() {
+        cudaError_t e = cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking);
+        for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+            e = cudaEventCreateWithFlags(&mask_ready[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&out_free[i], cudaEventDisableTiming);
+        }
+        return e;
+    }
+};
+}  // namespace
+
 int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp, float h,
                    int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
                    const float* dmask, int64_t tile_side, float* out_density, float* out_ew, int64_t* evals) {
     if (!c || !grid_ok(dg) || !out_density || (edge_correction && (!grid_ok(eg) || !emask)) ||
         (!h_pp && !(h > 0.0f)))
         return mgk_fail(c, MGK_ERR_INVALID, "kde_raster: bad arguments");
+    // tile grid (kde_cuda_kdtr_tiled.cu:1373-1517 walks tiles row-major)
+    int64_t tr, tc;
+    const int64_t T = tile_side > 0 ? tile_side : c->tile_side;
+    if (T > 0) {
+        tr = std::min<int64_t>(T, dg->nrows);
+        tc = std::min<int64_t>(T, dg->ncols);
+    } else {
+        tr = std::max<int64_t>(256, ((dg->nrows + 7) / 8 + 63) / 64 * 64);
+        tr = std::min<int64_t>(tr, dg->nrows);
+        tc = dg->ncols;
+    }
+    const int64_t ntr = (dg->nrows + tr - 1) / tr, ntc = (dg->ncols + tc - 1) / tc, ntiles = ntr * ntc;
+    const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
+    RasterPipe pipe;
+    cudaError_t ce = pipe.init();
+    if (ce != cudaSuccess) return mgk_cuda_fail(c, ce, "kde_raster streams");
     mgk_points* p = nullptr;
     mgk_raster* em = nullptr;
     mgk_index* idx = nullptr;
-    float *d_mask = nullptr, *d_out = nullptr;
+    float* d_mask[2] = {nullptr, nullptr};
+    float* d_out[2] = {nullptr, nullptr};
     int64_t ev_edge = 0, ev_den = 0;
     const float hfix = h_pp ? 0.0f : h;
-    int st = mgk_points_upload(c, n, x, y, w, h_pp, &p);
+    int st = MGK_OK;
+    for (int i = 0; i < (ntiles > 1 ? 2 : 1) && st == MGK_OK; i++) {
+        st = mgk_alloc(c, (void**)&d_out[i], tb);
+        if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask[i], tb);
+    }
+    auto tile_of = [&](int64_t k, int64_t& r0, int64_t& c0, int64_t& nr, int64_t& nc) {
+        r0 = (k / ntc) * tr;
+        c0 = (k % ntc) * tc;
+        nr = std::min<int64_t>(tr, dg->nrows - r0);
+        nc = std::min<int64_t>(tc, dg->ncols - c0);
+    };
+    // mask of tile k into buffer k % 2, after the density of tile k - 2 read it
+    auto mask_in = [&](int64_t k) -> cudaError_t {
+        if (!dmask || k >= ntiles) return cudaSuccess;
+        int64_t r0, c0, nr, nc;
+        tile_of(k, r0, c0, nr, nc);
+        const int b = (int)(k & 1);
+        cudaError_t e = k >= 2 ? cudaStreamWaitEvent(pipe.h2d, pipe.done[b], 0) : cudaSuccess;
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(d_mask[b], sizeof(float) * nc, dmask + r0 * dg->ncols + c0,
+                                  sizeof(float) * dg->ncols, sizeof(float) * nc, nr, cudaMemcpyHostToDevice, pipe.h2d);
+        if (e == cudaSuccess) e = cudaEventRecord(pipe.mask_ready[b], pipe.h2d);
+        return e;
+    };
+    if (st == MGK_OK) st = mgk_points_upload(c, n, x, y, w, h_pp, &p);
+    if (st == MGK_OK && edge_correction) st = mgk_raster_upload(c, eg, emask, &em);
+    // the first tile's mask travels while the points are prepared
+    if (st == MGK_OK && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
     if (st == MGK_OK) {
         if (edge_correction) {
-            if ((st = mgk_raster_upload(c, eg, emask, &em)) == MGK_OK && (st = mgk_boundary_dist(c, p, em)) == MGK_OK)
+            if ((st = mgk_boundary_dist(c, p, em)) == MGK_OK)
                 st = mgk_edge_weights(c, p, em, hfix, evals ? &ev_edge : nullptr);
         } else {
             st = mgk_edge_weights_unit(c, p);
@@ -601,35 +704,64 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
     }
     if (st == MGK_OK) st = mgk_index_build(c, p, hfix, 0.0f, &idx);
     if (st == MGK_OK && out_ew) {
-        cudaError_t e = cudaMemcpyAsync(out_ew, p->ew, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
-        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "kde_raster ew");
+        ce = cudaMemcpyAsync(out_ew, p->ew, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
+        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster ew");
     }
-    // tile loop (kde_cuda_kdtr_tiled.cu:1373-1517): row-major tiles
-    const int64_t T = tile_side > 0 ? tile_side : (c->tile_side > 0 ? c->tile_side : std::max<int64_t>(dg->ncols, dg->nrows));
-    const int64_t tr = std::min<int64_t>(T, dg->nrows), tc = std::min<int64_t>(T, dg->ncols);
-    const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
-    if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_out, tb);
-    if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask, tb);
-    for (int64_t r0 = 0; st == MGK_OK && r0 < dg->nrows; r0 += tr) {
-        for (int64_t c0 = 0; st == MGK_OK && c0 < dg->ncols; c0 += tc) {
-            const int64_t nr = std::min<int64_t>(tr, dg->nrows - r0), nc = std::min<int64_t>(tc, dg->ncols - c0);
-            cudaError_t e = cudaSuccess;
-            if (dmask)
-                e = cudaMemcpy2DAsync(d_mask, sizeof(float) * nc, dmask + r0 * dg->ncols + c0, sizeof(float) * dg->ncols,
-                                      sizeof(float) * nc, nr, cudaMemcpyHostToDevice, c->stream);
-            if (e != cudaSuccess) { st = mgk_cuda_fail(c, e, "kde_raster mask"); break; }
-            int64_t ev = 0;
-            st = mgk_density_tile(c, idx, dg, r0, c0, nr, nc, d_mask, d_out, evals ? &ev : nullptr);
-            if (st) break;
-            ev_den += ev;
-            e = cudaMemcpy2DAsync(out_density + r0 * dg->ncols + c0, sizeof(float) * dg->ncols, d_out,
-                                  sizeof(float) * nc, sizeof(float) * nc, nr, cudaMemcpyDeviceToHost, c->stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
-            if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "kde_raster tile");
+    if (st == MGK_OK && evals) {
+        ce = cudaMemsetAsync(c->d_counter + 4, 0, sizeof(unsigned long long), c->stream);
+        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster counter");
+    }
+    // density of tile k - 1 out, after its kernels (event done) and into the host raster
+    auto out_copy = [&](int64_t k) -> cudaError_t {
+        if (k < 0) return cudaSuccess;
+        int64_t r0, c0, nr, nc;
+        tile_of(k, r0, c0, nr, nc);
+        const int b = (int)(k & 1);
+        cudaError_t e = cudaStreamWaitEvent(pipe.d2h, pipe.done[b], 0);
+        if (e == cudaSuccess)
+            e = cudaMemcpy2DAsync(out_density + r0 * dg->ncols + c0, sizeof(float) * dg->ncols, d_out[b],
+                                  sizeof(float) * nc, sizeof(float) * nc, nr, cudaMemcpyDeviceToHost, pipe.d2h);
+        if (e == cudaSuccess) e = cudaEventRecord(pipe.out_free[b], pipe.d2h);
+        return e;
+    };
+    // Per tile: plan it (this waits on the context stream and sends the small
+    // work list while no large copy is queued ahead of it), then queue the
+    // previous tile's density out and the next tile's mask in, then run the
+    // kernels, which the two large copies overlap.
+    for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
+        int64_t r0, c0, nr, nc;
+        tile_of(k, r0, c0, nr, nc);
+        const int b = (int)(k & 1);
+        mgk_dplan* plan = nullptr;
+        if ((st = mgk_density_prepare(c, idx, dg, r0, c0, nr, nc, d_mask[b], d_out[b],
+                                      evals ? c->d_counter + 4 : nullptr, false, &plan)))
+            break;
+        ce = out_copy(k - 1);
+        if (ce == cudaSuccess) ce = mask_in(k + 1);
+        if (ce == cudaSuccess && dmask) ce = cudaStreamWaitEvent(c->stream, pipe.mask_ready[b], 0);
+        if (ce == cudaSuccess && k >= 2) ce = cudaStreamWaitEvent(c->stream, pipe.out_free[b], 0);
+        if (ce != cudaSuccess) {
+            mgk_density_discard(c, plan);
+            st = mgk_cuda_fail(c, ce, "kde_raster tile");
+            break;
         }
+        if ((st = mgk_density_execute(c, plan))) break;
+        if ((ce = cudaEventRecord(pipe.done[b], c->stream)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster");
     }
-    if (d_out) mgk_free(c, d_out, tb);
-    if (d_mask) mgk_free(c, d_mask, tb);
+    if (st == MGK_OK && (ce = out_copy(ntiles - 1)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster tile");
+    // every copy and kernel of this call ends before its buffers are released
+    if ((ce = cudaStreamSynchronize(pipe.h2d)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
+    if ((ce = cudaStreamSynchronize(pipe.d2h)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
+    if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
+    if (st == MGK_OK && evals) {
+        ce = cudaMemcpy(c->h_counter + 4, c->d_counter + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster counter");
+        else ev_den = (int64_t)c->h_counter[4];
+    }
+    for (int i = 0; i < 2; i++) {
+        if (d_out[i]) mgk_free(c, d_out[i], tb);
+        if (d_mask[i]) mgk_free(c, d_mask[i], tb);
+    }
     mgk_index_destroy(idx);
     mgk_raster_destroy(em);
     mgk_points_destroy(p);

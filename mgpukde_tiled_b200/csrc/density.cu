@@ -37,6 +37,7 @@
 // FP64 partials are merged in a fixed order, so results are bitwise
 // reproducible.
 #include <algorithm>
+#include <cstring>
 #include <cmath>
 #include <mutex>
 #include <vector>
@@ -144,6 +145,7 @@ __device__ __forceinline__ void row_span(const DParams& P, const BlockGeom& G, i
 // Candidate count of every block of the tile (planning).
 __global__ void k_block_counts(DParams P, int nbx_t, int nby_t, int64_t* __restrict__ counts) {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i == 0 && P.err) *P.err = 0;  // the staging-wait flag of the launch this plan is for
     if (i >= nbx_t * nby_t) return;
     const BlockGeom G = block_geom(P, i % nbx_t, i / nbx_t);
     int64_t c = 0;
@@ -732,6 +734,11 @@ __global__ void k_merge(DParams P, const int32_t* __restrict__ blocks, const int
     merge_block(P, blocks[blockIdx.x], slot_begin[blockIdx.x], slot_begin[blockIdx.x + 1]);
 }
 
+// The launch's staging-wait flag into mapped host memory (no copy engine).
+__global__ void k_store_flag(const unsigned long long* __restrict__ src, volatile unsigned long long* dst) {
+    *dst = *src;
+}
+
 // Merges of several jobs: entry b = {job, block, first slot, end slot}.
 __global__ void k_merge_jobs(const DParams* __restrict__ jobs, const int4* __restrict__ list) {
     const int4 m = list[blockIdx.x];
@@ -837,12 +844,39 @@ void sort_items(std::vector<Item>& items) {
 
 }  // namespace
 
-int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
-                       int64_t nr, int64_t nc, const float* d_mask, float* d_out,
-                       unsigned long long* d_evals, bool fp64) {
+// A planned density launch: work items and split tables in the context's
+// mapped staging (read by the kernels in place), scratch allocated, kernels
+// not yet launched.
+struct mgk_dplan {
+    const mgk_index* idx = nullptr;
+    bool fp64 = false, count = false;
+    DParams P{};
+    TilePlan T;
+    const int32_t *d_sb = nullptr, *d_sbeg = nullptr;
+    unsigned long long *h_err = nullptr, *d_err = nullptr;
+    size_t b_scr = 0;
+};
+
+static void dplan_release(mgk_ctx* ctx, mgk_dplan* D) {
+    if (!D) return;
+    if (D->T.nslots) mgk_free(ctx, D->P.scratch, D->b_scr);
+    delete D;
+}
+
+void mgk_density_discard(mgk_ctx* ctx, mgk_dplan* D) { dplan_release(ctx, D); }
+
+int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                        int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
+                        bool fp64, mgk_dplan** out) {
+    *out = nullptr;
     if (nr <= 0 || nc <= 0) return MGK_OK;
     cudaStream_t s = ctx->stream;
-    DParams P;
+    mgk_dplan* D = new (std::nothrow) mgk_dplan();
+    if (!D) return mgk_fail(ctx, MGK_ERR_INVALID, "density plan: out of host memory");
+    D->idx = idx;
+    D->fp64 = fp64;
+    D->count = d_evals != nullptr;
+    DParams& P = D->P;
     fill_params(P, idx, g, row0, col0, nr, nc, d_mask, d_out);
     P.evals = d_evals;
     P.err = ctx->d_counter + 7;
@@ -850,54 +884,68 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
     const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
     const int nblk = nbx_t * nby_t;
     int st;
-    // ---- plan: candidates per block -> work items (split heavy blocks) ----
-    int64_t* d_counts = nullptr;
-    if ((st = mgk_alloc(ctx, (void**)&d_counts, sizeof(int64_t) * nblk))) return st;
-    k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, d_counts);
-    std::vector<int64_t> counts(nblk);
-    cudaError_t ce = cudaMemsetAsync(P.err, 0, sizeof(unsigned long long), s);
-    if (ce == cudaSuccess)
-        ce = cudaMemcpyAsync(counts.data(), d_counts, sizeof(int64_t) * nblk, cudaMemcpyDeviceToHost, s);
+    // ---- plan: candidates per block (written straight into host memory) ->
+    // work items (heavy blocks split) ----
+    char *h_st = nullptr, *d_st = nullptr;
+    if ((st = mgk_host_stage(ctx, sizeof(int64_t) * nblk, (void**)&h_st, (void**)&d_st))) {
+        delete D;
+        return st;
+    }
+    k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, reinterpret_cast<int64_t*>(d_st));
+    cudaError_t ce = cudaGetLastError();
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    mgk_free(ctx, d_counts, sizeof(int64_t) * nblk);
-    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
-    TilePlan T;
-    plan_tile(counts.data(), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
+    if (ce != cudaSuccess) {
+        delete D;
+        return mgk_cuda_fail(ctx, ce, "density plan");
+    }
+    TilePlan& T = D->T;
+    plan_tile(reinterpret_cast<const int64_t*>(h_st), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
     sort_items(T.items);
-    std::vector<Item>& items = T.items;
     const int32_t nslots = T.nslots;
+    D->b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
+    if (nslots && (st = mgk_alloc(ctx, (void**)&P.scratch, D->b_scr))) {
+        delete D;
+        return st;
+    }
+    // the work list, the split tables and the error flag in the staging:
+    // [items | split blocks | split begins | err]
+    auto up16 = [](size_t b) { return (b + 15) & ~(size_t)15; };
+    const size_t b_items = sizeof(Item) * T.items.size();
+    const size_t b_sb = sizeof(int32_t) * T.split_blocks.size(), b_sbeg = sizeof(int32_t) * T.split_begin.size();
+    const size_t o_sb = up16(b_items), o_sbeg = o_sb + up16(b_sb), o_err = o_sbeg + up16(b_sbeg);
+    if ((st = mgk_host_stage(ctx, o_err + sizeof(unsigned long long), (void**)&h_st, (void**)&d_st))) {
+        dplan_release(ctx, D);
+        return st;
+    }
+    memcpy(h_st, T.items.data(), b_items);
+    if (nslots) {
+        memcpy(h_st + o_sb, T.split_blocks.data(), b_sb);
+        memcpy(h_st + o_sbeg, T.split_begin.data(), b_sbeg);
+    }
+    P.items = reinterpret_cast<const Item*>(d_st);
+    D->d_sb = reinterpret_cast<const int32_t*>(d_st + o_sb);
+    D->d_sbeg = reinterpret_cast<const int32_t*>(d_st + o_sbeg);
+    D->h_err = reinterpret_cast<unsigned long long*>(h_st + o_err);
+    D->d_err = reinterpret_cast<unsigned long long*>(d_st + o_err);
+    *D->h_err = 0;
+    *out = D;
+    return MGK_OK;
+}
 
-    const size_t b_items = sizeof(Item) * items.size();
-    const size_t b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
-    const size_t b_sb = sizeof(int32_t) * (T.split_blocks.size() + 1);
-    const size_t b_sbeg = sizeof(int32_t) * T.split_begin.size();
-    Item* d_items = nullptr;
-    int32_t *d_sb = nullptr, *d_sbeg = nullptr;
-    if ((st = mgk_alloc(ctx, (void**)&d_items, b_items))) return st;
-    if (nslots && (st = mgk_alloc(ctx, (void**)&P.scratch, b_scr))) { mgk_free(ctx, d_items, b_items); return st; }
-    if (nslots && (st = mgk_alloc(ctx, (void**)&d_sb, b_sb))) {
-        mgk_free(ctx, d_items, b_items); mgk_free(ctx, P.scratch, b_scr); return st;
-    }
-    if (nslots && (st = mgk_alloc(ctx, (void**)&d_sbeg, b_sbeg))) {
-        mgk_free(ctx, d_items, b_items); mgk_free(ctx, P.scratch, b_scr); mgk_free(ctx, d_sb, b_sb); return st;
-    }
+int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* D) {
+    if (!D) return MGK_OK;
+    cudaStream_t s = ctx->stream;
+    DParams& P = D->P;
+    const mgk_index* idx = D->idx;
+    cudaError_t ce = cudaSuccess;
     int rc = MGK_OK;
-    unsigned long long err = 0;
     do {
-        if ((ce = cudaMemcpyAsync(d_items, items.data(), b_items, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
-        if (nslots) {
-            if ((ce = cudaMemcpyAsync(d_sb, T.split_blocks.data(), sizeof(int32_t) * T.split_blocks.size(),
-                                      cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
-            if ((ce = cudaMemcpyAsync(d_sbeg, T.split_begin.data(), b_sbeg, cudaMemcpyHostToDevice, s)) != cudaSuccess)
-                break;
-        }
-        P.items = d_items;
-        const unsigned grid = (unsigned)items.size();
+        const unsigned grid = (unsigned)D->T.items.size();
         cudaEventRecord(ctx->ev_a, s);
-        if (fp64) {
+        if (D->fp64) {
             if (idx->varh) k_density_fp64<true><<<grid, kThreads, 0, s>>>(P);
             else k_density_fp64<false><<<grid, kThreads, 0, s>>>(P);
-        } else if (d_evals) {
+        } else if (D->count) {
             if (idx->varh) launch_density<true, true>(grid, s, P);
             else launch_density<false, true>(grid, s, P);
         } else {
@@ -907,25 +955,31 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
         cudaEventRecord(ctx->ev_b, s);
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
         MGK_COUNT_LAUNCH(ctx, 2);  // plan + density
-        if (nslots) {
-            k_merge<<<(unsigned)T.split_blocks.size(), 256, 0, s>>>(P, d_sb, d_sbeg);
+        if (D->T.nslots) {
+            k_merge<<<(unsigned)D->T.split_blocks.size(), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
             if ((ce = cudaGetLastError()) != cudaSuccess) break;
             MGK_COUNT_LAUNCH(ctx, 1);
         }
-        // the work list and scratch are freed below: wait for the kernels
-        if ((ce = cudaMemcpyAsync(&err, P.err, sizeof(err), cudaMemcpyDeviceToHost, s)) != cudaSuccess) break;
+        k_store_flag<<<1, 1, 0, s>>>(P.err, D->d_err);
+        if ((ce = cudaGetLastError()) != cudaSuccess) break;
+        MGK_COUNT_LAUNCH(ctx, 1);
+        // the work list and scratch are released below: wait for the kernels
         ce = cudaStreamSynchronize(s);
         if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
     } while (0);
     if (ce != cudaSuccess) rc = mgk_cuda_fail(ctx, ce, "density");
-    else if (err) rc = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
-    mgk_free(ctx, d_items, b_items);
-    if (nslots) {
-        mgk_free(ctx, P.scratch, b_scr);
-        mgk_free(ctx, d_sb, b_sb);
-        mgk_free(ctx, d_sbeg, b_sbeg);
-    }
+    else if (*D->h_err) rc = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    dplan_release(ctx, D);
     return rc;
+}
+
+int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                       int64_t nr, int64_t nc, const float* d_mask, float* d_out,
+                       unsigned long long* d_evals, bool fp64) {
+    mgk_dplan* D = nullptr;
+    const int st = mgk_density_prepare(ctx, idx, g, row0, col0, nr, nc, d_mask, d_out, d_evals, fp64, &D);
+    if (st) return st;
+    return mgk_density_execute(ctx, D);
 }
 
 // Several tiles in one density launch (plus one merge launch): the tiles

@@ -34,6 +34,9 @@ struct mgk_ctx {
     unsigned long long* h_counter = nullptr;  // pinned mirror
     double* d_sum = nullptr;                  // 256 doubles
     double* h_sum = nullptr;                  // pinned mirror
+    void* h_stage = nullptr;                  // mapped page-locked staging of plans and counts (mgk_host_stage)
+    void* d_stage = nullptr;                  // its device address
+    size_t h_stage_bytes = 0;
     std::multimap<size_t, void*> pool;        // cached device blocks by size class
     uint64_t launches = 0;                    // kernels launched by this context
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
@@ -119,6 +122,13 @@ struct mgk_index {
 int mgk_fail(mgk_ctx* ctx, int status, const std::string& msg);
 int mgk_cuda_fail(mgk_ctx* ctx, cudaError_t e, const char* what);
 int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes);
+// Mapped page-locked host memory of at least `bytes` owned by the context
+// (grown on demand, previous contents not kept): *host and *dev address the
+// same bytes.  Kernels read and write it directly over the bus, so small
+// per-launch tables and flags need no copy-engine transfer and never queue
+// behind large copies that other streams have in flight.  One user at a time:
+// kernels using it must have finished before the next call.
+int mgk_host_stage(mgk_ctx* ctx, size_t bytes, void** host, void** dev);
 void mgk_free(mgk_ctx* ctx, void* p, size_t bytes);
 
 #define MGK_CHECK_CUDA(ctx, expr)                                   \
@@ -212,6 +222,19 @@ int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, in
                        int64_t col0, int64_t nr, int64_t nc, const float* d_mask, float* d_out,
                        unsigned long long* d_evals, bool fp64);
 int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, unsigned long long* d_evals);
+// mgk_launch_density in two halves, so a caller can put its own copies
+// between the plan (which synchronises the context stream and uploads the
+// work list) and the kernels: prepare plans and uploads; execute launches,
+// waits and releases the plan (also on failure); discard releases an unrun
+// plan.  One plan at a time per context (the work list shares the context's
+// page-locked staging).  A tile with no cells gives a null plan, which
+// execute accepts.
+struct mgk_dplan;
+int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                        int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
+                        bool fp64, mgk_dplan** out);
+int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* plan);
+void mgk_density_discard(mgk_ctx* ctx, mgk_dplan* plan);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
 int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r);

@@ -379,8 +379,9 @@ def rule_of_thumb(x, y, w=None) -> float:
 
 
 def kde_raster(ctx: Context, x, y, w, h, dens_grid: Grid, dens_mask=None, edge_grid: Grid | None = None,
-               edge_mask=None, h_pp=None, tile=0, out=None, return_ew=False):
-    """The whole path from host buffers; returns (density[nrows, ncols], edge weights|None, evals)."""
+               edge_mask=None, h_pp=None, tile=0, out=None, return_ew=False, count=False):
+    """The whole path from host buffers; returns (density[nrows, ncols], edge weights|None, evals|None).
+    count: also count the in-cutoff pairs (the counting kernels run somewhat slower)."""
     x, y, w, h_pp = _f32(x), _f32(y), _f32(w), _f32(h_pp)
     dm = None if dens_mask is None else _f32(dens_mask).reshape(-1)
     em = None if edge_mask is None else _f32(edge_mask).reshape(-1)
@@ -393,5 +394,5 @@ def kde_raster(ctx: Context, x, y, w, h, dens_grid: Grid, dens_mask=None, edge_g
     ctx.check(lib().mgk_kde_raster(ctx.handle, len(x), _ptr(x), _ptr(y), _ptr(w), _ptr(h_pp),
                                    float(h if h is not None else 0.0), int(edge_grid is not None),
                                    C.byref(eg), _ptr(em), C.byref(dg), _ptr(dm), int(tile), _ptr(out), _ptr(ew),
-                                   C.byref(ev)))
-    return out, ew, ev.value
+                                   C.byref(ev) if count else None))
+    return out, ew, (ev.value if count else None)

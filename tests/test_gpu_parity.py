@@ -87,7 +87,7 @@ def test_golden_case_end_to_end(ctx, case):
     ref = oracle_run(d)
     eg, dg = mk.Grid.of(d["eg"]), mk.Grid.of(d["dg"])
     den, ew, ev = mk.kde_raster(ctx, d["x"], d["y"], d["w"], ref["h"], dg, d["density_mask"], eg,
-                                d["edge_mask"], h_pp=d["hs"], tile=37, return_ew=True)
+                                d["edge_mask"], h_pp=d["hs"], tile=37, return_ew=True, count=True)
     nd = d["density_mask"] == dg.nodata
     assert np.array_equal(den[nd], d["density_mask"][nd])
     assert rel_err(den[~nd], ref["density"][~nd]).max() <= RTOL
@@ -115,13 +115,16 @@ def test_single_large_crop(ctx):
     d2 = o.dist2_boundary(c["x"], c["y"], og_e, b)
     ew, eev = o.edge_weights(c["x"], c["y"], c["h"], d2, og_e, c["edge_mask"])
     ref, rev = o.density(c["x"], c["y"], c["w"], ew, c["h"], og_d, dmask)
-    den, gew, gev = mk.kde_raster(ctx, c["x"], c["y"], c["w"], c["h"], mk.Grid.of(dg), dmask,
-                                  mk.Grid.of(c["edge_grid"]), c["edge_mask"], tile=512, return_ew=True)
-    nd = dmask == dg.nodata
-    assert np.array_equal(den[nd], dmask[nd])
-    assert rel_err(den[~nd], ref[~nd]).max() <= RTOL
-    assert rel_err(gew, ew).max() <= RTOL
-    assert gev == rev + eev
+    # 512^2 tiles, then the default full-width bands (256 rows: 4 bands through the copy pipeline)
+    for tile in (512, 0):
+        den, gew, gev = mk.kde_raster(ctx, c["x"], c["y"], c["w"], c["h"], mk.Grid.of(dg), dmask,
+                                      mk.Grid.of(c["edge_grid"]), c["edge_mask"], tile=tile, return_ew=True,
+                                      count=True)
+        nd = dmask == dg.nodata
+        assert np.array_equal(den[nd], dmask[nd])
+        assert rel_err(den[~nd], ref[~nd]).max() <= RTOL
+        assert rel_err(gew, ew).max() <= RTOL
+        assert gev == rev + eev
 
 
 def test_boundary_distance_exact_large(ctx):
