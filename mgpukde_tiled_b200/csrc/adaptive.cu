@@ -27,6 +27,7 @@
 // likelihoods.
 #include <algorithm>
 #include <cfloat>
+#include <climits>
 #include <cmath>
 
 #include "mgk_internal.cuh"
@@ -36,20 +37,30 @@ namespace {
 constexpr int kPdQ = 128;  // queries (threads) per CTA
 constexpr int kPdB = 32;   // candidates per staged batch
 
-// den[perm[q]] = sum over candidates i (all points of the index within reach
-// of the CTA's 128 consecutive queries) of [in cutoff] K w_i e_i; the query
-// itself is included when SELF.  Fixed h: terms exp2(-d^2 k2) w e, times
-// 1/(h^2 TWO_PI) at the end; per-point h (VARH): the candidate's own k2 and
-// cutoff, weights already carry 1/(h_i^2 TWO_PI).
+// psum[y][q] = sum over candidates i (the points of the index within reach
+// of the CTA's 128 consecutive queries, in the bin rows y, y + nsplit, ... of
+// the window, y = blockIdx.y) of [in cutoff] K w_i e_i, unnormalised; the
+// query itself is included when SELF.  Fixed h: terms exp2(-d^2 k2) w e;
+// per-point h (VARH): the candidate's own k2 and cutoff, weights already
+// carry 1/(h_i^2 TWO_PI).  Splitting the rows over nsplit CTAs gives a
+// launch enough CTAs for the whole GPU when there are few queries.
+//
+// Per-point h: the window is the group's bounding box grown by the largest
+// reach of all points, but in each bin row only the span from the first to
+// the last bin whose own largest reach (bin_r2: 9 h^2 of its widest point)
+// can touch the box is read, so points with small h far from the group are
+// never tested.
 template <bool VARH, bool SELF>
 __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* __restrict__ pts,
-                                                        const int32_t* __restrict__ perm,
                                                         const int32_t* __restrict__ bin_start, double ox,
-                                                        double oy, double inv_side, int64_t nbx, int64_t nby,
-                                                        double reach, double h2, double* __restrict__ den,
+                                                        double oy, double side, int64_t nbx, int64_t nby,
+                                                        double reach, double h2, const float* __restrict__ bin_r2,
+                                                        double* __restrict__ psum,
                                                         unsigned long long* __restrict__ evals) {
     __shared__ __align__(16) MgkPt st[kPdB];
     __shared__ float bb[4][kPdQ / 32];
+    __shared__ int s_span[2];
+    const double inv_side = 1.0 / side;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t qpos = (int64_t)blockIdx.x * kPdQ + tid;
     const bool qv = qpos < n;
@@ -87,8 +98,34 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
     const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
     float s = 0.0f, c = 0.0f;
     unsigned cnt = 0;
-    for (int64_t by = by0; by <= by1 && bx0 <= bx1; by++) {
-        const int64_t sb = bin_start[by * nbx + bx0], se = bin_start[by * nbx + bx1 + 1];
+    for (int64_t by = by0 + blockIdx.y; by <= by1 && bx0 <= bx1; by += gridDim.y) {
+        int64_t lo = bx0, hi = bx1;
+        if (VARH) {
+            __syncthreads();  // s_span of the previous row has been read
+            if (tid == 0) {
+                s_span[0] = INT_MAX;
+                s_span[1] = -1;
+            }
+            __syncthreads();
+            const double ry0 = oy + (double)by * side, ry1 = ry0 + side;
+            const double ddy = fmax(0.0, fmax(ry0 - (double)mxy, (double)mny - ry1));
+            for (int64_t bx = bx0 + tid; bx <= bx1; bx += kPdQ) {
+                const float r2 = bin_r2[by * nbx + bx];
+                if (r2 < 0.0f) continue;  // empty bin
+                const double rx0 = ox + (double)bx * side, rx1 = rx0 + side;
+                const double ddx = fmax(0.0, fmax(rx0 - (double)mxx, (double)mnx - rx1));
+                // a margin over the bin edges' rounding and the float h^2
+                if (ddx * ddx + ddy * ddy <= (double)r2 * (1.0 + 1e-5) + 1e-6 * side * side) {
+                    atomicMin(&s_span[0], (int)(bx - bx0));
+                    atomicMax(&s_span[1], (int)(bx - bx0));
+                }
+            }
+            __syncthreads();
+            if (s_span[1] < 0) continue;  // no bin of the row reaches the group (uniform)
+            lo = bx0 + s_span[0];
+            hi = bx0 + s_span[1];
+        }
+        const int64_t sb = bin_start[by * nbx + lo], se = bin_start[by * nbx + hi + 1];
         for (int64_t base = sb; base < se; base += kPdB) {
             const int m = (int)mgk_min64(kPdB, se - base);
             __syncthreads();
@@ -119,21 +156,46 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
             s = tt;
         }
     }
-    if (qv) {
-        const double v = (double)s - (double)c;
-        den[perm[qpos]] = VARH ? v : v / (h2 * (double)MGK_TWO_PI_F);
-    }
+    if (qv) psum[(int64_t)blockIdx.y * n + qpos] = (double)s - (double)c;
     if (evals) {
         for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
         if (lane == 0 && cnt) atomicAdd(evals, (unsigned long long)cnt);
     }
 }
 
-// out[0] = sum_i log(max(v_i, floor)) in a fixed order (one CTA).
-__global__ void k_log_sum(int64_t n, const double* __restrict__ v, double floor_v, double* __restrict__ out) {
+// den[perm[q]] = the nsplit partials of query q summed in order (times
+// 1/(h^2 TWO_PI) for a fixed h), and part[CTA] = the CTA's fixed-order sum of
+// log(max(den, floor_v)).
+__global__ void __launch_bounds__(kPdQ) k_pd_combine(int64_t n, int nsplit, const double* __restrict__ psum,
+                                                     const int32_t* __restrict__ perm, bool varh, double h2,
+                                                     double floor_v, double* __restrict__ den,
+                                                     double* __restrict__ part) {
+    __shared__ double s_lg[kPdQ / 32];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t q = (int64_t)blockIdx.x * kPdQ + tid;
+    double lg = 0.0;
+    if (q < n) {
+        double v = 0.0;
+        for (int y = 0; y < nsplit; y++) v += psum[(int64_t)y * n + q];
+        if (!varh) v /= h2 * (double)MGK_TWO_PI_F;
+        den[perm[q]] = v;
+        lg = log(v > floor_v ? v : floor_v);
+    }
+    for (int o = 16; o; o >>= 1) lg += __shfl_xor_sync(0xffffffffu, lg, o);
+    if (lane == 0) s_lg[warp] = lg;
+    __syncthreads();
+    if (tid == 0) {
+        double t = 0.0;
+        for (int i = 0; i < kPdQ / 32; i++) t += s_lg[i];
+        part[blockIdx.x] = t;
+    }
+}
+
+// out[0] = sum of the per-CTA partials in a fixed order (one CTA).
+__global__ void k_sum_parts(int64_t g, const double* __restrict__ part, double* __restrict__ out) {
     __shared__ double sh[256];
     double a = 0.0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) a += log(v[i] > floor_v ? v[i] : floor_v);
+    for (int64_t i = threadIdx.x; i < g; i += blockDim.x) a += part[i];
     sh[threadIdx.x] = a;
     __syncthreads();
     for (int o = 128; o; o >>= 1) {
@@ -150,6 +212,16 @@ __global__ void k_adaptive_h(int64_t n, const double* __restrict__ den0, const d
     if (i >= n) return;
     const double gml = exp(logsum[0] / (double)n);
     hs[i] = (float)((double)h * pow(den0[i] / gml, (double)alpha));
+}
+
+// Per bin: 9 h^2 of its widest point (-1 for an empty bin).
+__global__ void k_bin_reach2(int64_t nbins, const int32_t* __restrict__ bin_start, const MgkPt* __restrict__ pts,
+                             float* __restrict__ r2) {
+    const int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (b >= nbins) return;
+    float m = -1.0f;
+    for (int64_t t = bin_start[b]; t < bin_start[b + 1]; t++) m = fmaxf(m, pts[t].hh);
+    r2[b] = m < 0.0f ? -1.0f : 9.0f * m;
 }
 
 // Counters of a likelihood computation: context counter slots 5 (edge-mask
@@ -176,24 +248,57 @@ int count_end(mgk_ctx* c) {
     return MGK_OK;
 }
 
-int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den) {
-    if (idx->n == 0) return MGK_OK;
-    const unsigned grid = (unsigned)((idx->n + kPdQ - 1) / kPdQ);
+// den[input order] and logsum[0] = sum_j log(max(den_j, floor_v)).
+int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den, double floor_v, double* d_logsum) {
     cudaStream_t s = c->stream;
-    if (idx->varh)
-        k_point_density<true, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
-                                                           idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, d_den, pair_count(c));
-    else if (self)
-        k_point_density<false, true><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
-                                                           idx->oy, 1.0 / idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, d_den, pair_count(c));
-    else
-        k_point_density<false, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->perm, idx->bin_start, idx->ox,
-                                                            idx->oy, 1.0 / idx->side, idx->nbx, idx->nby,
-                                                            idx->reach, idx->h2, d_den, pair_count(c));
-    MGK_CHECK_LAUNCH(c, "k_point_density");
-    MGK_COUNT_LAUNCH(c, 1);
+    const int64_t g = (idx->n + kPdQ - 1) / kPdQ;
+    if (g == 0) {
+        MGK_CHECK_CUDA(c, cudaMemsetAsync(d_logsum, 0, sizeof(double), s));
+        return MGK_OK;
+    }
+    // bin rows split over enough CTAs to give every SM about 8 of them
+    const int nsplit = (int)std::min<int64_t>(8, std::max<int64_t>(1, (8 * (int64_t)c->sm_count + g - 1) / g));
+    const int64_t nbins = idx->varh ? idx->nbx * idx->nby : 0;
+    const size_t b_part = sizeof(double) * (size_t)g, b_r2 = sizeof(float) * (size_t)std::max<int64_t>(nbins, 1);
+    const size_t b_psum = sizeof(double) * (size_t)idx->n * (size_t)nsplit;
+    double *part = nullptr, *psum = nullptr;
+    float* r2 = nullptr;
+    int st = mgk_alloc(c, (void**)&part, b_part);
+    if (st) return st;
+    if ((st = mgk_alloc(c, (void**)&psum, b_psum))) {
+        mgk_free(c, part, b_part);
+        return st;
+    }
+    if (idx->varh && (st = mgk_alloc(c, (void**)&r2, b_r2))) {
+        mgk_free(c, part, b_part);
+        mgk_free(c, psum, b_psum);
+        return st;
+    }
+    const dim3 grid((unsigned)g, (unsigned)nsplit);
+    if (idx->varh) {
+        k_bin_reach2<<<(unsigned)((nbins + 255) / 256), 256, 0, s>>>(nbins, idx->bin_start, idx->pts, r2);
+        k_point_density<true, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
+                                                           idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
+                                                           idx->h2, r2, psum, pair_count(c));
+    } else if (self) {
+        k_point_density<false, true><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
+                                                           idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
+                                                           idx->h2, nullptr, psum, pair_count(c));
+    } else {
+        k_point_density<false, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
+                                                            idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
+                                                            idx->h2, nullptr, psum, pair_count(c));
+    }
+    k_pd_combine<<<(unsigned)g, kPdQ, 0, s>>>(idx->n, nsplit, psum, idx->perm, idx->varh, idx->h2, floor_v, d_den,
+                                              part);
+    k_sum_parts<<<1, 256, 0, s>>>(g, part, d_logsum);
+    const cudaError_t e = cudaGetLastError();
+    // pooled blocks: a later allocation of them is ordered on the same stream
+    mgk_free(c, part, b_part);
+    mgk_free(c, psum, b_psum);
+    if (r2) mgk_free(c, r2, b_r2);
+    if (e != cudaSuccess) return mgk_cuda_fail(c, e, "k_point_density");
+    MGK_COUNT_LAUNCH(c, idx->varh ? 4 : 3);
     return MGK_OK;
 }
 
@@ -207,11 +312,10 @@ int pilot_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, fl
     p->has_ew = true;
     mgk_index* idx = nullptr;
     if ((st = mgk_index_build(c, p, h, 0.0f, &idx))) return st;  // h > 0: fixed-h index
-    st = point_density(c, idx, true, d_den);
-    if (st == MGK_OK) {
-        k_log_sum<<<1, 256, 0, c->stream>>>(p->n, d_den, 0.0, d_scal);
+    st = point_density(c, idx, true, d_den, 0.0, d_scal);
+    if (st == MGK_OK && p->n > 0) {
         k_adaptive_h<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->n, d_den, d_scal, h, alpha, p->h);
-        MGK_COUNT_LAUNCH(c, 2);
+        MGK_COUNT_LAUNCH(c, 1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths");
     }
@@ -226,13 +330,13 @@ int loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, flo
     if (st) return st;
     if (r && (st = mgk_launch_edge_weights(c, p->n, p->x, p->y, p->h, 0.0f, p->dist2, r, p->ew, edge_count(c))))
         return st;
+    // per-point h; bins of 0.75 h (the geometric mean of hs is h), not of the
+    // widest h, so that the per-bin reach can cut the window down
     mgk_index* idx = nullptr;
-    if ((st = mgk_index_build(c, p, 0.0f, 0.0f, &idx))) return st;  // per-point h
-    st = point_density(c, idx, false, d_den);
+    if ((st = mgk_index_build(c, p, 0.0f, 0.75f * h, &idx))) return st;
+    st = point_density(c, idx, false, d_den, (double)MGK_EPS_DENSITY_F, d_scal + 1);
     mgk_index_destroy(idx);
     if (st) return st;
-    k_log_sum<<<1, 256, 0, c->stream>>>(p->n, d_den, (double)MGK_EPS_DENSITY_F, d_scal + 1);
-    MGK_COUNT_LAUNCH(c, 1);
     MGK_CHECK_CUDA(c, cudaMemcpyAsync(c->h_sum, d_scal + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
     *logl = c->h_sum[0];
