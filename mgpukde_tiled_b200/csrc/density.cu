@@ -260,32 +260,68 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
     return b0 | (b1 << 1);
 }
 
-struct BatchIt {
-    int64_t by, seq, pos;  // current bin row, its offset in the block's sequence, next candidate
-    int64_t sb, len;       // the current row's range of the index
+// A mini-batch takes its points from kNCur cursors over equal consecutive
+// parts of the item's candidate range (round robin, up to kMB / kNCur from
+// each, then whatever is left), so that the points of one batch come from
+// bin rows spread over the candidate window.  Points from one bin row all
+// touch the same warp rows of the block; mixing rows keeps the eight warps'
+// phase-B work per batch even and shortens the waits at the batch barriers.
+constexpr int kNCur = 2;
+struct BatchCur {
+    long long by, seq, pos, end;  // bin row, its offset in the block's sequence, next and end candidate
+    long long sb, len;            // the current row's range of the index
 };
 
-// Stages the next mini-batch of the block's candidate sequence into dst: up
-// to kMB candidates, taken across bin rows (one bulk copy per row segment,
-// all completing on the buffer's mbarrier; the issuing thread then arrives
-// with the batch's byte count).  Returns the batch size (0 at the end).
-__device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, const Item& it, BatchIt& s,
-                                          MgkPt* dst, uint64_t* bar, bool issuer) {
-    if (!G.any) return 0;
-    int m = 0;
-    while (m < kMB && s.by <= G.by1 && s.pos < it.k1) {
-        const int64_t lo = mgk_max64(s.pos, s.seq), hi = mgk_min64(s.seq + s.len, (int64_t)it.k1);
+// Cursor c of an item: candidates [k0 + (k1 - k0) c / kNCur, ...) of the block's sequence.
+__device__ __forceinline__ void cur_init(const DParams& P, const BlockGeom& G, const Item& it, int c, BatchCur& s) {
+    const long long k0 = it.k0, k1 = it.k1;
+    s.by = G.by0;
+    s.seq = 0;
+    s.pos = k0 + (k1 - k0) * c / kNCur;
+    s.end = k0 + (k1 - k0) * (c + 1) / kNCur;
+    s.sb = s.len = 0;
+    if (G.any) {
+        int64_t sb, len;
+        row_span(P, G, G.by0, sb, len);
+        s.sb = sb;
+        s.len = len;
+    }
+}
+
+// Up to `limit` more candidates from cursor s into dst[m..] (one bulk copy per
+// row segment, completing on bar); returns the new m.
+__device__ __forceinline__ int cur_take(const DParams& P, const BlockGeom& G, BatchCur& s, int m, int limit,
+                                        MgkPt* dst, uint64_t* bar) {
+    while (m < limit && s.by <= G.by1 && s.pos < s.end) {
+        const long long lo = s.pos > s.seq ? s.pos : s.seq;
+        const long long hi = (s.seq + s.len) < s.end ? (s.seq + s.len) : s.end;
         if (lo < hi) {
-            const int n = (int)mgk_min64(kMB - m, hi - lo);
-            if (issuer) bulk_g2s(dst + m, P.pts + s.sb + (lo - s.seq), (unsigned)(n * sizeof(MgkPt)), bar);
+            const int n = (int)((limit - m) < (hi - lo) ? (limit - m) : (hi - lo));
+            bulk_g2s(dst + m, P.pts + s.sb + (lo - s.seq), (unsigned)(n * sizeof(MgkPt)), bar);
             s.pos = lo + n;
             m += n;
         } else {
             s.seq += s.len;
-            if (++s.by <= G.by1) row_span(P, G, s.by, s.sb, s.len);
+            if (++s.by <= G.by1) {
+                int64_t sb, len;
+                row_span(P, G, s.by, sb, len);
+                s.sb = sb;
+                s.len = len;
+            }
         }
     }
-    if (issuer && m > 0) mbar_arrive_tx(bar, (unsigned)(m * sizeof(MgkPt)));
+    return m;
+}
+
+// Stages the next mini-batch of the item into dst (called by one thread; the
+// cursors live in shared memory).  Returns the batch size (0 at the end).
+__device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, BatchCur* cur, MgkPt* dst,
+                                          uint64_t* bar) {
+    if (!G.any) return 0;
+    int m = 0;
+    for (int c = 0; c < kNCur; c++) m = cur_take(P, G, cur[c], m, m + kMB / kNCur, dst, bar);
+    for (int c = 0; c < kNCur && m < kMB; c++) m = cur_take(P, G, cur[c], m, kMB, dst, bar);
+    if (m > 0) mbar_arrive_tx(bar, (unsigned)(m * sizeof(MgkPt)));
     return m;
 }
 
@@ -328,6 +364,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     __shared__ unsigned char fullmask[kMB];  // every cell of warp w's sub-block is inside the cutoff
     __shared__ float s_cxh[kBC], s_cxl[kBC], s_cxg[kBC], s_cyh[kBR], s_cyl[kBR], s_cyg[kBR];
     __shared__ int s_abort;
+    __shared__ BatchCur s_cur[kNCur];  // the item's candidate cursors (thread 0)
+    __shared__ int s_nm;               // size of the batch being staged
 
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -389,22 +427,27 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     const int sk_c0 = sk_wc * 64, sk_c1 = min(sk_wc * 64 + 63, G.ncol - 1);
     const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
 
-    BatchIt bit{G.by0, 0, (int64_t)it.k0, 0, 0};
-    if (G.any) row_span(P, G, G.by0, bit.sb, bit.len);
-    int m = fill_batch(P, G, it, bit, &stage[0], &mbar[0], tid == 0);
+    if (tid == 0) {
+        for (int c = 0; c < kNCur; c++) cur_init(P, G, it, c, s_cur[c]);
+        s_nm = fill_batch(P, G, s_cur, &stage[0], &mbar[0]);
+    }
+    __syncthreads();
+    int m = s_nm;
     unsigned phase0 = 0, phase1 = 0;
     int buf = 0;
     // outstanding copies at an abort: (buffer, parity) pairs to drain
     int drain_n = 0, drain_b[2] = {0, 0};
     unsigned drain_p[2] = {0, 0};
     while (m > 0) {
-        const int nm = fill_batch(P, G, it, bit, &stage[(buf ^ 1) * kMB], &mbar[buf ^ 1], tid == 0);
+        if (tid == 0) s_nm = fill_batch(P, G, s_cur, &stage[(buf ^ 1) * kMB], &mbar[buf ^ 1]);
         const unsigned par = buf ? phase1 : phase0;
         if (!mbar_wait(&mbar[buf], par)) {
             atomicExch(P.err, 1ull);
             s_abort = 1;
         }
-        if (__syncthreads_or(s_abort)) {
+        const bool abort_now = __syncthreads_or(s_abort);
+        const int nm = s_nm;  // written before the barrier; rewritten only after the batch's end barrier
+        if (abort_now) {
             drain_b[drain_n] = buf;
             drain_p[drain_n++] = par;
             if (nm > 0) {
