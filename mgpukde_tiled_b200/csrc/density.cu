@@ -29,7 +29,7 @@
 //    ambiguous are re-decided with the exact FP64 test of the oracle, so the
 //    summed pair set is exactly the reference's.
 //
-// Accumulation: FP32 partial sums over 16 points per cell (registers), added
+// Accumulation: FP32 partial sums over 32 points per cell (registers), added
 // into a Kahan-compensated FP32 accumulator (shared memory, 64 KB per CTA,
 // which with the 128 registers per thread leaves two CTAs per SM); the
 // epilogue forms (s - c) times the
@@ -616,8 +616,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     if (COUNT) cnt += __popc(inm & valid);
                 }
                 pc++;
-                if ((pc & 15u) == 0) {
-                    // 16-point partials into the Kahan accumulators in shared memory
+                if ((pc & 31u) == 0) {
+                    // 32-point partials into the Kahan accumulators in shared memory
 #pragma unroll
                     for (int q4 = 0; q4 < 8; q4++) {
                         float4 sv = ksum[q4 * kThreads + tid], cv = kcmp[q4 * kThreads + tid];
