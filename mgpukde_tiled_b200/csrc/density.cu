@@ -680,13 +680,25 @@ __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DPar
     density_item<VARH, COUNT>(P, P.items[blockIdx.x]);
 }
 
+// The job parameters live in mapped host memory: each CTA copies its job's
+// into shared memory once instead of reading them over the bus.
+__device__ __forceinline__ void load_job(const DParams* jobs, int j, DParams& dst) {
+    static_assert(sizeof(DParams) % 8 == 0, "DParams is copied in 8-byte words");
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(jobs + j);
+    unsigned long long* d = reinterpret_cast<unsigned long long*>(&dst);
+    for (int i = threadIdx.x; i < (int)(sizeof(DParams) / 8); i += blockDim.x) d[i] = src[i];
+    __syncthreads();
+}
+
 // Several tiles (of one or several indexes and rasters) in one launch: item
 // it belongs to job it.pad, whose parameters are jobs[it.pad].
 template <bool VARH, bool COUNT>
 __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density_jobs(const DParams* __restrict__ jobs,
                                                                                  const Item* __restrict__ items) {
+    __shared__ __align__(16) DParams sP;
     const Item it = items[blockIdx.x];
-    density_item<VARH, COUNT>(jobs[it.pad], it);
+    load_job(jobs, it.pad, sP);
+    density_item<VARH, COUNT>(sP, it);
 }
 
 
@@ -784,8 +796,10 @@ __global__ void k_store_flag(const unsigned long long* __restrict__ src, volatil
 
 // Merges of several jobs: entry b = {job, block, first slot, end slot}.
 __global__ void k_merge_jobs(const DParams* __restrict__ jobs, const int4* __restrict__ list) {
+    __shared__ __align__(16) DParams sP;
     const int4 m = list[blockIdx.x];
-    merge_block(jobs[m.x], m.y, m.z, m.w);
+    load_job(jobs, m.x, sP);
+    merge_block(sP, m.y, m.z, m.w);
 }
 
 template <bool VARH, bool COUNT>
@@ -1048,19 +1062,20 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     const int nblk_all = off[njobs];
     if (nblk_all == 0) return MGK_OK;
     int st;
-    int64_t* d_counts = nullptr;
-    if ((st = mgk_alloc(ctx, (void**)&d_counts, sizeof(int64_t) * nblk_all))) return st;
-    cudaError_t ce = cudaMemsetAsync(ctx->d_counter + 7, 0, sizeof(unsigned long long), s);
+    // Plan tables travel through the context's mapped page-locked staging
+    // (mgk_host_stage): no copy engine, so they never queue behind large
+    // copies that other streams have in flight.
+    char *h_st = nullptr, *d_st = nullptr;
+    if ((st = mgk_host_stage(ctx, sizeof(int64_t) * nblk_all, (void**)&h_st, (void**)&d_st))) return st;
+    cudaError_t ce = cudaSuccess;
     for (int j = 0; j < njobs && ce == cudaSuccess; j++) {
         const int nb = nbx[j] * nby[j];
-        if (nb) k_block_counts<<<(nb + 255) / 256, 256, 0, s>>>(P[j], nbx[j], nby[j], d_counts + off[j]);
+        if (nb)
+            k_block_counts<<<(nb + 255) / 256, 256, 0, s>>>(P[j], nbx[j], nby[j],
+                                                             reinterpret_cast<int64_t*>(d_st) + off[j]);
         ce = cudaGetLastError();
     }
-    std::vector<int64_t> counts(nblk_all);
-    if (ce == cudaSuccess)
-        ce = cudaMemcpyAsync(counts.data(), d_counts, sizeof(int64_t) * nblk_all, cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    mgk_free(ctx, d_counts, sizeof(int64_t) * nblk_all);
     if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density jobs plan");
     MGK_COUNT_LAUNCH(ctx, njobs);
     // plan each job; items of both bandwidth kinds, merges, slot offsets
@@ -1068,77 +1083,76 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     std::vector<int4> merges;
     int32_t nslots = 0;
     std::vector<int32_t> slot0(njobs, 0);
-    for (int j = 0; j < njobs; j++) {
-        if (!nbx[j]) continue;
-        TilePlan T;
-        plan_tile(counts.data() + off[j], nbx[j], nby[j], ctx->sm_count, ctx->split_waves, j, T);
-        slot0[j] = nslots;
-        for (size_t b = 0; b < T.split_blocks.size(); b++)
-            merges.push_back(make_int4(j, T.split_blocks[b], T.split_begin[b], T.split_begin[b + 1]));
-        nslots += T.nslots;
-        std::vector<Item>& dst = jobs[j].index->varh ? items_var : items_fix;
-        dst.insert(dst.end(), T.items.begin(), T.items.end());
+    {
+        const int64_t* counts = reinterpret_cast<const int64_t*>(h_st);
+        for (int j = 0; j < njobs; j++) {
+            if (!nbx[j]) continue;
+            TilePlan T;
+            plan_tile(counts + off[j], nbx[j], nby[j], ctx->sm_count, ctx->split_waves, j, T);
+            slot0[j] = nslots;
+            for (size_t b = 0; b < T.split_blocks.size(); b++)
+                merges.push_back(make_int4(j, T.split_blocks[b], T.split_begin[b], T.split_begin[b + 1]));
+            nslots += T.nslots;
+            std::vector<Item>& dst = jobs[j].index->varh ? items_var : items_fix;
+            dst.insert(dst.end(), T.items.begin(), T.items.end());
+        }
     }
     sort_items(items_fix);
     sort_items(items_var);
-    const size_t b_jobs = sizeof(DParams) * njobs;
-    const size_t b_items = sizeof(Item) * std::max<size_t>(items_fix.size() + items_var.size(), 1);
     const size_t b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
-    const size_t b_mg = sizeof(int4) * std::max<size_t>(merges.size(), 1);
-    DParams* d_jobs = nullptr;
-    Item* d_items = nullptr;
     double* d_scr = nullptr;
-    int4* d_mg = nullptr;
-    st = mgk_alloc(ctx, (void**)&d_jobs, b_jobs);
-    if (st == MGK_OK) st = mgk_alloc(ctx, (void**)&d_items, b_items);
-    if (st == MGK_OK && nslots) st = mgk_alloc(ctx, (void**)&d_scr, b_scr);
-    if (st == MGK_OK && !merges.empty()) st = mgk_alloc(ctx, (void**)&d_mg, b_mg);
-    unsigned long long err = 0;
-    if (st == MGK_OK) {
-        for (int j = 0; j < njobs; j++)
-            P[j].scratch = d_scr ? d_scr + (size_t)slot0[j] * kCells : nullptr;  // slots are job-local
-        std::vector<Item> all(items_fix);
-        all.insert(all.end(), items_var.begin(), items_var.end());
-        do {
-            if ((ce = cudaMemcpyAsync(d_jobs, P.data(), b_jobs, cudaMemcpyHostToDevice, s)) != cudaSuccess) break;
-            if ((ce = cudaMemcpyAsync(d_items, all.data(), sizeof(Item) * all.size(), cudaMemcpyHostToDevice, s)) !=
-                cudaSuccess)
-                break;
-            if (!merges.empty() && (ce = cudaMemcpyAsync(d_mg, merges.data(), sizeof(int4) * merges.size(),
-                                                         cudaMemcpyHostToDevice, s)) != cudaSuccess)
-                break;
-            cudaEventRecord(ctx->ev_a, s);
-            if (!items_fix.empty()) {
-                if (d_evals) launch_density_jobs<false, true>((unsigned)items_fix.size(), s, d_jobs, d_items);
-                else launch_density_jobs<false, false>((unsigned)items_fix.size(), s, d_jobs, d_items);
-                MGK_COUNT_LAUNCH(ctx, 1);
-            }
-            if (!items_var.empty()) {
-                const Item* iv = d_items + items_fix.size();
-                if (d_evals) launch_density_jobs<true, true>((unsigned)items_var.size(), s, d_jobs, iv);
-                else launch_density_jobs<true, false>((unsigned)items_var.size(), s, d_jobs, iv);
-                MGK_COUNT_LAUNCH(ctx, 1);
-            }
-            cudaEventRecord(ctx->ev_b, s);
-            if ((ce = cudaGetLastError()) != cudaSuccess) break;
-            if (!merges.empty()) {
-                k_merge_jobs<<<(unsigned)merges.size(), 256, 0, s>>>(d_jobs, d_mg);
-                if ((ce = cudaGetLastError()) != cudaSuccess) break;
-                MGK_COUNT_LAUNCH(ctx, 1);
-            }
-            if ((ce = cudaMemcpyAsync(&err, ctx->d_counter + 7, sizeof(err), cudaMemcpyDeviceToHost, s)) !=
-                cudaSuccess)
-                break;
-            ce = cudaStreamSynchronize(s);
-            if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
-        } while (0);
-        if (ce != cudaSuccess) st = mgk_cuda_fail(ctx, ce, "density jobs");
-        else if (err) st = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    if (nslots && (st = mgk_alloc(ctx, (void**)&d_scr, b_scr))) return st;
+    for (int j = 0; j < njobs; j++)
+        P[j].scratch = d_scr ? d_scr + (size_t)slot0[j] * kCells : nullptr;  // slots are job-local
+    // staging: [job parameters | items (fixed h, then per-point h) | merges | err]
+    auto up16 = [](size_t v) { return (v + 15) & ~(size_t)15; };
+    const size_t nitems = items_fix.size() + items_var.size();
+    const size_t o_items = up16(sizeof(DParams) * njobs);
+    const size_t o_mg = o_items + up16(sizeof(Item) * std::max<size_t>(nitems, 1));
+    const size_t o_err = o_mg + up16(sizeof(int4) * std::max<size_t>(merges.size(), 1));
+    if ((st = mgk_host_stage(ctx, o_err + sizeof(unsigned long long), (void**)&h_st, (void**)&d_st))) {
+        mgk_free(ctx, d_scr, b_scr);
+        return st;
     }
-    mgk_free(ctx, d_jobs, b_jobs);
-    mgk_free(ctx, d_items, b_items);
+    memcpy(h_st, P.data(), sizeof(DParams) * njobs);
+    memcpy(h_st + o_items, items_fix.data(), sizeof(Item) * items_fix.size());
+    memcpy(h_st + o_items + sizeof(Item) * items_fix.size(), items_var.data(), sizeof(Item) * items_var.size());
+    if (!merges.empty()) memcpy(h_st + o_mg, merges.data(), sizeof(int4) * merges.size());
+    volatile unsigned long long* h_err = reinterpret_cast<unsigned long long*>(h_st + o_err);
+    *h_err = 0;
+    const DParams* d_jobs = reinterpret_cast<const DParams*>(d_st);
+    const Item* d_items = reinterpret_cast<const Item*>(d_st + o_items);
+    const int4* d_mg = reinterpret_cast<const int4*>(d_st + o_mg);
+    do {
+        cudaEventRecord(ctx->ev_a, s);
+        if (!items_fix.empty()) {
+            if (d_evals) launch_density_jobs<false, true>((unsigned)items_fix.size(), s, d_jobs, d_items);
+            else launch_density_jobs<false, false>((unsigned)items_fix.size(), s, d_jobs, d_items);
+            MGK_COUNT_LAUNCH(ctx, 1);
+        }
+        if (!items_var.empty()) {
+            const Item* iv = d_items + items_fix.size();
+            if (d_evals) launch_density_jobs<true, true>((unsigned)items_var.size(), s, d_jobs, iv);
+            else launch_density_jobs<true, false>((unsigned)items_var.size(), s, d_jobs, iv);
+            MGK_COUNT_LAUNCH(ctx, 1);
+        }
+        cudaEventRecord(ctx->ev_b, s);
+        if ((ce = cudaGetLastError()) != cudaSuccess) break;
+        if (!merges.empty()) {
+            k_merge_jobs<<<(unsigned)merges.size(), 256, 0, s>>>(d_jobs, d_mg);
+            if ((ce = cudaGetLastError()) != cudaSuccess) break;
+            MGK_COUNT_LAUNCH(ctx, 1);
+        }
+        k_store_flag<<<1, 1, 0, s>>>(ctx->d_counter + 7, reinterpret_cast<unsigned long long*>(d_st + o_err));
+        if ((ce = cudaGetLastError()) != cudaSuccess) break;
+        MGK_COUNT_LAUNCH(ctx, 1);
+        // the staging and the scratch are released below: wait for the kernels
+        ce = cudaStreamSynchronize(s);
+        if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
+    } while (0);
+    if (ce != cudaSuccess) st = mgk_cuda_fail(ctx, ce, "density jobs");
+    else if (*h_err) st = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
     mgk_free(ctx, d_scr, b_scr);
-    mgk_free(ctx, d_mg, b_mg);
     return st;
 }
 

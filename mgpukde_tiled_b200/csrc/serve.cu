@@ -13,10 +13,13 @@
 //    and stay resident on the device while it is active;
 //  * ticks: each tick takes the next tile of every active request (row-major
 //    tiles of tile_side x tile_side cells) and runs all of them in one density
-//    launch (mgk_launch_density_jobs), then copies each tile to its request's
-//    host output.  Requests admitted between ticks join the next tick, so a
-//    short request that arrives while a large one is running finishes after a
-//    few ticks instead of waiting for the large one.
+//    launch (mgk_launch_density_jobs).  Each request has two device output
+//    tiles: a tick's results are copied to the requests' host outputs on a
+//    second stream while the next tick computes into the other tiles.
+//    Requests admitted between ticks join the next tick, so a short request
+//    that arrives while a large one is running finishes after a few ticks
+//    instead of waiting for the large one.  A request is complete when the
+//    copy of its last tile has landed.
 //
 // Each tile is planned on its own, so a request's raster is bitwise the same
 // whether it ran alone or in a mix.  Callers submit from any thread and wait
@@ -42,6 +45,10 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
 
+__global__ void k_copy_counts(int n, const unsigned long long* __restrict__ src, volatile unsigned long long* dst) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
+}
+
 struct Job {
     uint64_t id = 0;
     mgk_request req{};
@@ -53,7 +60,9 @@ struct Job {
     mgk_raster* em = nullptr;
     mgk_index* idx = nullptr;
     float* d_mask = nullptr;
-    float* d_out = nullptr;
+    float* d_out[2] = {nullptr, nullptr};  // tile k computes into d_out[k & 1]
+    cudaEvent_t out_free[2] = {nullptr, nullptr};  // the copy out of d_out[b] has finished
+    bool used[2] = {false, false};
     size_t tile_bytes = 0;
     int64_t tiles_x = 0, tiles_y = 0, next_tile = 0;
     int64_t evals = 0;
@@ -70,7 +79,12 @@ struct mgk_server {
     std::condition_variable cv_work, cv_done;
     std::deque<Job*> queue;
     std::map<uint64_t, Job*> jobs;  // every job until its result is collected
-    std::vector<Job*> active;
+    std::vector<Job*> active;    // tiles left to compute
+    std::vector<Job*> draining;  // every tile computed, the last copies in flight
+    cudaStream_t d2h = nullptr;  // copies of finished tiles to the host
+    unsigned long long* h_ev = nullptr;  // per-tick eval counts, mapped page-locked
+    unsigned long long* d_ev_map = nullptr;  // their device address
+    int ev_cap = 0;
     uint64_t reserved = 0;
     uint64_t next_id = 1;
     bool stop = false;
@@ -92,7 +106,7 @@ uint64_t estimate_bytes(const mgk_request& r, int64_t tile) {
     b += (uint64_t)(bins * 4.0);
     if (r.edge) b += (uint64_t)r.edge_grid.ncols * (uint64_t)r.edge_grid.nrows * 24;
     const uint64_t tr = (uint64_t)std::min<int64_t>(tile, r.grid.nrows), tc = (uint64_t)std::min<int64_t>(tile, r.grid.ncols);
-    b += 2 * tr * tc * 4;                                 // mask and output tile
+    b += 3 * tr * tc * 4;                                 // mask and two output tiles
     b += ((tr + 63) / 64) * ((tc + 63) / 64) * 64 * 1024;  // split-block scratch and work list
     return b + b / 4 + (16u << 20);
 }
@@ -103,11 +117,16 @@ void release(mgk_server* S, Job* J) {
     mgk_raster_destroy(J->em);
     mgk_points_destroy(J->p);
     mgk_free(c, J->d_mask, J->tile_bytes);
-    mgk_free(c, J->d_out, J->tile_bytes);
+    for (int b = 0; b < 2; b++) {
+        mgk_free(c, J->d_out[b], J->tile_bytes);
+        if (J->out_free[b]) cudaEventDestroy(J->out_free[b]);
+        J->d_out[b] = nullptr;
+        J->out_free[b] = nullptr;
+    }
     J->idx = nullptr;
     J->em = nullptr;
     J->p = nullptr;
-    J->d_mask = J->d_out = nullptr;
+    J->d_mask = nullptr;
 }
 
 // Uploads and indexes a newly admitted request (worker thread).
@@ -128,10 +147,15 @@ int prepare(mgk_server* S, Job* J) {
     if ((st = mgk_index_build(c, J->p, r.h, 0.0f, &J->idx))) return st;
     const int64_t tr = std::min<int64_t>(S->tile, r.grid.nrows), tc = std::min<int64_t>(S->tile, r.grid.ncols);
     J->tile_bytes = sizeof(float) * (size_t)tr * (size_t)tc;
-    if ((st = mgk_alloc(c, (void**)&J->d_out, J->tile_bytes))) return st;
-    if (r.mask && (st = mgk_alloc(c, (void**)&J->d_mask, J->tile_bytes))) return st;
     J->tiles_x = (r.grid.ncols + tc - 1) / tc;
     J->tiles_y = (r.grid.nrows + tr - 1) / tr;
+    const int nbuf = J->tiles_x * J->tiles_y > 1 ? 2 : 1;
+    for (int b = 0; b < nbuf; b++) {
+        if ((st = mgk_alloc(c, (void**)&J->d_out[b], J->tile_bytes))) return st;
+        const cudaError_t e = cudaEventCreateWithFlags(&J->out_free[b], cudaEventDisableTiming);
+        if (e != cudaSuccess) return mgk_cuda_fail(c, e, "serve: event");
+    }
+    if (r.mask && (st = mgk_alloc(c, (void**)&J->d_mask, J->tile_bytes))) return st;
     J->next_tile = 0;
     return MGK_OK;
 }
@@ -144,11 +168,35 @@ void finish(mgk_server* S, Job* J, int status) {
     J->t_done = Clock::now();
     S->reserved -= J->est;
     S->active.erase(std::remove(S->active.begin(), S->active.end(), J), S->active.end());
+    S->draining.erase(std::remove(S->draining.begin(), S->draining.end(), J), S->draining.end());
     S->completed++;
     S->cv_done.notify_all();
 }
 
-// One tick: the next tile of every active, prepared request in one launch.
+// The copy out of a job's last tile: its buffer's out_free event.
+cudaEvent_t last_copy(const Job* J) { return J->out_free[(J->next_tile - 1) & 1]; }
+
+// Completes the draining jobs whose last copy has landed (all of them when
+// wait is set).
+void reap(mgk_server* S, bool wait) {
+    std::vector<Job*> d;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        d = S->draining;
+    }
+    for (Job* J : d) {
+        cudaError_t e = wait ? cudaEventSynchronize(last_copy(J)) : cudaEventQuery(last_copy(J));
+        if (e == cudaErrorNotReady) {
+            (void)cudaGetLastError();
+            continue;
+        }
+        finish(S, J, e == cudaSuccess ? MGK_OK : mgk_cuda_fail(S->ctx, e, "serve: tile copy"));
+    }
+}
+
+// One tick: the next tile of every active, prepared request in one launch;
+// the tiles' copies to the host are queued on the copy stream and overlap the
+// next tick.
 void tick(mgk_server* S, std::vector<Job*>& act) {
     mgk_ctx* c = S->ctx;
     cudaStream_t s = c->stream;
@@ -162,6 +210,12 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
         const int64_t ty = J->next_tile / J->tiles_x, tx = J->next_tile % J->tiles_x;
         const int64_t r0 = ty * tr, c0 = tx * tc;
         const int64_t nr = std::min(tr, r.grid.nrows - r0), nc = std::min(tc, r.grid.ncols - c0);
+        const int b = (int)(J->next_tile & 1);
+        // the tile buffer's previous copy out must have finished before it is rewritten
+        if (J->used[b] && cudaStreamWaitEvent(s, J->out_free[b], 0) != cudaSuccess) {
+            st = MGK_ERR_CUDA;
+            break;
+        }
         if (r.mask) {
             const cudaError_t e = cudaMemcpy2DAsync(J->d_mask, sizeof(float) * nc, r.mask + r0 * r.grid.ncols + c0,
                                                     sizeof(float) * r.grid.ncols, sizeof(float) * nc, nr,
@@ -171,7 +225,7 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
                 break;
             }
         }
-        tj.push_back(mgk_tile_job{J->idx, r.grid, r0, c0, nr, nc, r.mask ? J->d_mask : nullptr, J->d_out});
+        tj.push_back(mgk_tile_job{J->idx, r.grid, r0, c0, nr, nc, r.mask ? J->d_mask : nullptr, J->d_out[b]});
         owner.push_back(J);
         r0s.push_back(r0);
         c0s.push_back(c0);
@@ -180,20 +234,31 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
     const size_t bev = sizeof(unsigned long long) * std::max<size_t>(tj.size(), 1);
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_ev, bev);
     if (st == MGK_OK && cudaMemsetAsync(d_ev, 0, bev, s) != cudaSuccess) st = MGK_ERR_CUDA;
-    if (st == MGK_OK) st = mgk_launch_density_jobs(c, (int)tj.size(), tj.data(), d_ev);
-    std::vector<unsigned long long> ev(tj.size(), 0);
-    for (size_t k = 0; k < tj.size() && st == MGK_OK; k++) {
-        const mgk_request& r = owner[k]->req;
-        const cudaError_t e = cudaMemcpy2DAsync(r.out + r0s[k] * r.grid.ncols + c0s[k], sizeof(float) * r.grid.ncols,
-                                                tj[k].d_out, sizeof(float) * tj[k].ncols, sizeof(float) * tj[k].ncols,
-                                                tj[k].nrows, cudaMemcpyDeviceToHost, s);
-        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "serve: tile result");
+    if (st == MGK_OK && (int)tj.size() > S->ev_cap) st = mgk_fail(c, MGK_ERR_INVALID, "serve: more tiles than slots");
+    if (st == MGK_OK) st = mgk_launch_density_jobs(c, (int)tj.size(), tj.data(), d_ev);  // returns after the kernels
+    if (st == MGK_OK) {
+        // eval counts into mapped host memory by a kernel: no copy engine, so
+        // they do not wait behind the previous tick's tile copies
+        k_copy_counts<<<1, 256, 0, s>>>((int)tj.size(), d_ev, S->d_ev_map);
+        MGK_COUNT_LAUNCH(c, 1);
+        if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) st = MGK_ERR_CUDA;
     }
-    if (st == MGK_OK && cudaMemcpyAsync(ev.data(), d_ev, sizeof(unsigned long long) * tj.size(),
-                                        cudaMemcpyDeviceToHost, s) != cudaSuccess)
-        st = MGK_ERR_CUDA;
-    if (st == MGK_OK && cudaStreamSynchronize(s) != cudaSuccess) st = MGK_ERR_CUDA;
     mgk_free(c, d_ev, bev);
+    std::vector<unsigned long long> ev(tj.size(), 0);
+    if (st == MGK_OK)
+        for (size_t k = 0; k < tj.size(); k++) ev[k] = S->h_ev[k];
+    // copies of this tick's tiles to the host outputs, on the copy stream
+    for (size_t k = 0; k < tj.size() && st == MGK_OK; k++) {
+        Job* J = owner[k];
+        const mgk_request& r = J->req;
+        const int b = (int)(J->next_tile & 1);
+        cudaError_t e = cudaMemcpy2DAsync(r.out + r0s[k] * r.grid.ncols + c0s[k], sizeof(float) * r.grid.ncols,
+                                          tj[k].d_out, sizeof(float) * tj[k].ncols, sizeof(float) * tj[k].ncols,
+                                          tj[k].nrows, cudaMemcpyDeviceToHost, S->d2h);
+        if (e == cudaSuccess) e = cudaEventRecord(J->out_free[b], S->d2h);
+        if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "serve: tile result");
+        J->used[b] = true;
+    }
     {
         std::lock_guard<std::mutex> lk(S->mu);
         S->ticks++;
@@ -203,11 +268,16 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
     for (size_t k = 0; k < owner.size(); k++) {
         Job* J = owner[k];
         if (st) {
+            cudaStreamSynchronize(S->d2h);  // nothing of the job stays in flight
             finish(S, J, st);
             continue;
         }
         J->evals += (int64_t)ev[k];
-        if (++J->next_tile == J->tiles_x * J->tiles_y) finish(S, J, MGK_OK);
+        if (++J->next_tile == J->tiles_x * J->tiles_y) {
+            std::lock_guard<std::mutex> lk(S->mu);
+            S->active.erase(std::remove(S->active.begin(), S->active.end(), J), S->active.end());
+            S->draining.push_back(J);
+        }
     }
 }
 
@@ -216,18 +286,24 @@ void worker_main(mgk_server* S) {
     std::vector<Job*> fresh;
     for (;;) {
         fresh.clear();
+        reap(S, false);
         {
             std::unique_lock<std::mutex> lk(S->mu);
             if (S->active.empty() && S->queue.empty()) {
+                if (!S->draining.empty()) {
+                    lk.unlock();
+                    reap(S, true);  // nothing to compute: wait for the last copies
+                    continue;
+                }
                 if (S->stop) return;
                 S->cv_work.wait_for(lk, std::chrono::milliseconds(50));
                 continue;
             }
             // admission: slots and the HBM budget; a request that fits nowhere
             // alone is still admitted when nothing else is active
-            while (!S->queue.empty() && (int)S->active.size() < S->max_active) {
+            while (!S->queue.empty() && (int)(S->active.size() + S->draining.size()) < S->max_active) {
                 Job* J = S->queue.front();
-                if (!S->active.empty() && S->reserved + J->est > S->budget) break;
+                if ((!S->active.empty() || !S->draining.empty()) && S->reserved + J->est > S->budget) break;
                 S->queue.pop_front();
                 J->state = 1;
                 J->t_start = Clock::now();
@@ -268,6 +344,17 @@ int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, i
     S->tile = tile_side;
     S->max_active = max_active;
     S->budget = c->budget;
+    S->ev_cap = max_active;
+    if (cudaStreamCreateWithFlags(&S->d2h, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaHostAlloc((void**)&S->h_ev, sizeof(unsigned long long) * (size_t)max_active, cudaHostAllocMapped) !=
+            cudaSuccess ||
+        cudaHostGetDevicePointer((void**)&S->d_ev_map, S->h_ev, 0) != cudaSuccess) {
+        if (S->h_ev) cudaFreeHost(S->h_ev);
+        if (S->d2h) cudaStreamDestroy(S->d2h);
+        mgk_ctx_destroy(c);
+        delete S;
+        return MGK_ERR_CUDA;
+    }
     S->worker = std::thread(worker_main, S);
     *out = S;
     return MGK_OK;
@@ -344,7 +431,7 @@ int mgk_serve_stats(mgk_server* S, mgk_serve_info* out) {
     out->max_batch = S->max_batch;
     out->completed = S->completed;
     out->queued = S->queue.size();
-    out->active = S->active.size();
+    out->active = S->active.size() + S->draining.size();
     out->reserved_bytes = S->reserved;
     out->device_bytes = S->ctx->in_use;
     return MGK_OK;
@@ -359,6 +446,8 @@ int mgk_serve_destroy(mgk_server* S) {
     }
     if (S->worker.joinable()) S->worker.join();  // finishes queued and active requests first
     for (auto& kv : S->jobs) delete kv.second;
+    cudaStreamDestroy(S->d2h);
+    cudaFreeHost(S->h_ev);
     mgk_ctx_destroy(S->ctx);
     delete S;
     return MGK_OK;
