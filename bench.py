@@ -162,6 +162,47 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows), "source": src}
 
 
+_ALL_CPUS = None
+
+
+def bind_local_numa(device):
+    """Runs this process on the host cores of the GPU's own NUMA node, so
+    that page-locked buffers are allocated in memory next to the GPU's PCIe
+    root (read-only sysfs queries; nothing about the GPU changes).  Returns
+    the node, or None when the topology is not visible."""
+    global _ALL_CPUS
+    try:
+        import torch
+        p = torch.cuda.get_device_properties(device)
+        bus = "%04x:%02x:%02x.0" % (p.pci_domain_id, p.pci_bus_id, p.pci_device_id)
+        with open(f"/sys/bus/pci/devices/{bus}/numa_node") as f:
+            node = int(f.read().strip())
+        if node < 0:
+            return None
+        with open(f"/sys/devices/system/node/node{node}/cpulist") as f:
+            cpus = set()
+            for part in f.read().strip().split(","):
+                a, _, b = part.partition("-")
+                cpus.update(range(int(a), int(b or a) + 1))
+        _ALL_CPUS = os.sched_getaffinity(0)
+        cpus &= _ALL_CPUS
+        if not cpus:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return node
+    except Exception:
+        return None
+
+
+def unbind_numa():
+    """All host cores again (the CPU baselines use every core)."""
+    if _ALL_CPUS:
+        try:
+            os.sched_setaffinity(0, _ALL_CPUS)
+        except Exception:
+            pass
+
+
 def build_workload(name, scale, seed):
     if name != "single_large":
         raise SystemExit(f"unknown workload {name}")
@@ -294,7 +335,8 @@ def config_of(args):
                         f"density 1e4^2 @ cell 1 polygon mask, edge mask 2500^2 @ cell 4, h=50"
                         + ("" if args.scale == 1.0 else f" (scaled x{args.scale})"),
             "scale": args.scale, "tile": "whole raster (one tile)", "parallelism": f"tiles x{args.gpus} (no exchange)",
-            "l2": "inputs larger than L2 (density mask and output 400 MB each)"}
+            "l2": "inputs larger than L2 (density mask and output 400 MB each)",
+            "host_numa_node": getattr(args, "numa_node", None)}
 
 
 # ------------------------------------------------------------------ GPU arm --
@@ -439,6 +481,7 @@ def run_mgk(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
+            unbind_numa()
             out["cpu_baseline"] = cpu_baseline(c)
         except Exception as e:  # reported, not fatal
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
@@ -637,6 +680,7 @@ def run_adaptive(args):
                    "h2d_bytes_per_step": int(3 * 4 * n + c["edge_mask"].nbytes), "d2h_bytes_per_step": int(4 * n)},
            "gpu_launches": launches, "clocks": clocks}
     if not args.no_cpu_baseline:
+        unbind_numa()
         out["cpu_baseline"] = adaptive_cpu_baseline(0.5 * args.scale)
     print(json.dumps(out))
     pts.close()
@@ -769,13 +813,13 @@ def run_serving(args):
         st = srv.stats()
     top = rows[-1]
     out = {"metric": "served evals/s at saturation (mixed-request p50/p99 ms alongside)", "value": top["evals_s"],
-           "unit": "evals/s", "n_gpus": 1, "steps": len(rates), "warmup": 1, "ms_per_step": None,
+           "unit": "evals/s", "n_gpus": 1, "steps": len(rates), "warmup": count, "ms_per_step": None,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
            "data": "synthetic (seeded PCG64)",
            "config": {"workload": f"serving: {count} requests per rate, N lognormal [1e3, 2e6], side U[256, 8192], "
                                   f"h U[5, 100], edge correction on half; Poisson arrivals; one untimed "
                                   f"pass of the request set first",
-                      "tile": 2048, "max_active": 8},
+                      "tile": 2048, "max_active": 8, "host_numa_node": getattr(args, "numa_node", None)},
            "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": rows,
            "server": {k: st[k] for k in ("ticks", "tiles", "max_batch", "completed")}}
     print(json.dumps(out))
@@ -795,6 +839,7 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)
+    args.numa_node = bind_local_numa(env_rank()[2])
     if args.workload == "bandwidth_select":
         return run_bandwidth_select(args)
     if args.workload == "serving":

@@ -49,6 +49,12 @@ __global__ void k_copy_counts(int n, const unsigned long long* __restrict__ src,
     for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = src[i];
 }
 
+// A kernel rather than a memset, so nothing on the context stream goes
+// through a copy engine during a tick.
+__global__ void k_zero_counts(int n, unsigned long long* __restrict__ a) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) a[i] = 0ull;
+}
+
 struct Job {
     uint64_t id = 0;
     mgk_request req{};
@@ -233,7 +239,11 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
     unsigned long long* d_ev = nullptr;
     const size_t bev = sizeof(unsigned long long) * std::max<size_t>(tj.size(), 1);
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&d_ev, bev);
-    if (st == MGK_OK && cudaMemsetAsync(d_ev, 0, bev, s) != cudaSuccess) st = MGK_ERR_CUDA;
+    if (st == MGK_OK) {
+        k_zero_counts<<<1, 256, 0, s>>>((int)std::max<size_t>(tj.size(), 1), d_ev);
+        MGK_COUNT_LAUNCH(c, 1);
+        if (cudaGetLastError() != cudaSuccess) st = MGK_ERR_CUDA;
+    }
     if (st == MGK_OK && (int)tj.size() > S->ev_cap) st = mgk_fail(c, MGK_ERR_INVALID, "serve: more tiles than slots");
     if (st == MGK_OK) st = mgk_launch_density_jobs(c, (int)tj.size(), tj.data(), d_ev);  // returns after the kernels
     if (st == MGK_OK) {
@@ -312,6 +322,10 @@ void worker_main(mgk_server* S) {
                 fresh.push_back(J);
             }
         }
+        // preparation reads small results back to the host; those copies
+        // would queue behind the tile copies still in flight on the copy
+        // engine, so let them land first
+        if (!fresh.empty()) cudaStreamSynchronize(S->d2h);
         for (Job* J : fresh) {
             const int st = prepare(S, J);
             if (st) finish(S, J, st);
