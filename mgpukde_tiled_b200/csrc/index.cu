@@ -209,7 +209,79 @@ __global__ void k_hmax(int64_t n, const float* __restrict__ h, unsigned* out) {
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// Z-order (Morton) key of the bin of each index record: bit-interleaved bin
+// column and row (16 bits each), value = the record's position.
+__device__ __forceinline__ unsigned spread16(unsigned v) {
+    v &= 0xffffu;
+    v = (v | (v << 8)) & 0x00ff00ffu;
+    v = (v | (v << 4)) & 0x0f0f0f0fu;
+    v = (v | (v << 2)) & 0x33333333u;
+    v = (v | (v << 1)) & 0x55555555u;
+    return v;
+}
+
+__global__ void k_morton_keys(int64_t n, const MgkPt* __restrict__ pts, double ox, double oy, double inv_side,
+                              int64_t nbx, int64_t nby, unsigned* __restrict__ keys, int32_t* __restrict__ vals) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const MgkPt p = pts[i];
+    int64_t bx = (int64_t)floor(((double)(p.xh + p.xl) - ox) * inv_side);
+    int64_t by = (int64_t)floor(((double)(p.yh + p.yl) - oy) * inv_side);
+    bx = bx < 0 ? 0 : (bx >= nbx ? nbx - 1 : bx);
+    by = by < 0 ? 0 : (by >= nby ? nby - 1 : by);
+    keys[i] = spread16((unsigned)bx) | (spread16((unsigned)by) << 1);
+    vals[i] = (int32_t)i;
+}
+
 }  // namespace
+
+// Positions of the index records in Z-order of their bins (stable: records
+// of one bin keep their order).  Consecutive runs of this order are compact
+// in both directions, unlike runs of the row-major record order.
+int mgk_index_zorder(mgk_ctx* ctx, const mgk_index* idx, int32_t* d_order) {
+    const int64_t n = idx->n;
+    if (n == 0) return MGK_OK;
+    if (idx->nbx > 65536 || idx->nby > 65536) return mgk_fail(ctx, MGK_ERR_INVALID, "index_zorder: bin grid too large");
+    cudaStream_t s = ctx->stream;
+    const int ntiles = (int)((n + kSortTile - 1) / kSortTile);
+    const size_t b_keys = sizeof(unsigned) * (size_t)n, b_vals = sizeof(int32_t) * (size_t)n;
+    const size_t b_cnt = sizeof(unsigned) * 256 * (size_t)ntiles;
+    unsigned *k0 = nullptr, *k1 = nullptr, *cnt = nullptr;
+    int32_t* v0 = nullptr;
+    int st;
+    if ((st = mgk_alloc(ctx, (void**)&k0, b_keys))) return st;
+    if ((st = mgk_alloc(ctx, (void**)&k1, b_keys))) { mgk_free(ctx, k0, b_keys); return st; }
+    if ((st = mgk_alloc(ctx, (void**)&v0, b_vals))) { mgk_free(ctx, k0, b_keys); mgk_free(ctx, k1, b_keys); return st; }
+    if ((st = mgk_alloc(ctx, (void**)&cnt, b_cnt))) {
+        mgk_free(ctx, k0, b_keys); mgk_free(ctx, k1, b_keys); mgk_free(ctx, v0, b_vals);
+        return st;
+    }
+    k_morton_keys<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, idx->pts, idx->ox, idx->oy, 1.0 / idx->side,
+                                                             idx->nbx, idx->nby, k0, v0);
+    const uint64_t maxb = (uint64_t)std::max(idx->nbx, idx->nby) - 1;
+    int bits = 0;
+    while (bits < 16 && (maxb >> bits) != 0) bits++;
+    const int passes = std::max(1, (2 * bits + 7) / 8);
+    unsigned *kin = k0, *kout = k1;
+    int32_t *vin = v0, *vout = d_order;
+    for (int p = 0; p < passes; p++) {
+        k_radix_hist<<<ntiles, kSortThreads, 0, s>>>(n, kin, 8 * p, ntiles, cnt);
+        k_scan_exclusive<<<1, 1024, 0, s>>>(cnt, (int64_t)256 * ntiles);
+        k_radix_scatter<<<ntiles, kSortThreads, 0, s>>>(n, kin, vin, kout, vout, 8 * p, ntiles, cnt);
+        std::swap(kin, kout);
+        std::swap(vin, vout);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && vin != d_order) e = cudaMemcpyAsync(d_order, vin, b_vals, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);  // the scratch is released below
+    MGK_COUNT_LAUNCH(ctx, 1 + 3 * passes);
+    mgk_free(ctx, k0, b_keys);
+    mgk_free(ctx, k1, b_keys);
+    mgk_free(ctx, v0, b_vals);
+    mgk_free(ctx, cnt, b_cnt);
+    if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "index_zorder");
+    return MGK_OK;
+}
 
 int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float bin_size, mgk_index* idx) {
     const int64_t n = pts->n;

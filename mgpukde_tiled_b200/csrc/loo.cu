@@ -45,6 +45,7 @@ struct LevelDesc {
     const MgkPt* pts;
     const int32_t* bin_start;
     const int32_t* perm;
+    const int32_t* qord;  // query order: record positions in Z-order of the bins
     double ox, oy, side, inv_side;
     int64_t nbx, nby;
 };
@@ -162,8 +163,11 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
         const float* ewk = P.ew ? P.ew + (int64_t)k * P.n : nullptr;
 
         // this item's query
-        const int64_t qpos = (int64_t)grp * kLooQ + tid;
-        const bool qv = qpos < P.n;
+        // the group's queries: 128 consecutive records of the Z-order, a
+        // compact patch of bins (row-major runs would be long thin strips)
+        const int64_t qk = (int64_t)grp * kLooQ + tid;
+        const bool qv = qk < P.n;
+        const int64_t qpos = qv ? (int64_t)L.qord[qk] : -1;
         MgkPt q{};
         if (qv) q = L.pts[qpos];
         const float qx = q.xh + q.xl, qy = q.yh + q.yl;
@@ -321,6 +325,7 @@ struct mgk_loo_batch {
     int nh = 0;
     int ngroups = 0;
     std::vector<mgk_index*> lev;
+    std::vector<int32_t*> qord;  // per level
     float* d_h = nullptr;
     float* d_ew = nullptr;
     LevelDesc* d_lev = nullptr;
@@ -371,6 +376,7 @@ void mgk_loo_batch_destroy(mgk_loo_batch* B) {
     if (B->graph) cudaGraphDestroy(B->graph);
     if (B->cap) cudaStreamDestroy(B->cap);
     mgk_free(c, B->d_lev, sizeof(LevelDesc) * kMaxLev);
+    for (int32_t* q : B->qord) mgk_free(c, q, sizeof(int32_t) * (size_t)std::max<int64_t>(B->n, 1));
     for (mgk_index* i : B->lev) mgk_index_destroy(i);
     const size_t nh = (size_t)B->nh;
     mgk_free(c, B->d_h, sizeof(float) * nh);
@@ -412,6 +418,13 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
         st = mgk_index_build(c, &view, h_lo, side, &idx);
         if (st == MGK_OK) {
             B->lev.push_back(idx);
+            int32_t* q = nullptr;
+            st = mgk_alloc(c, (void**)&q, sizeof(int32_t) * (size_t)std::max<int64_t>(p->n, 1));
+            if (st == MGK_OK) {
+                B->qord.push_back(q);
+                st = mgk_index_zorder(c, idx, q);
+            }
+            if (st) break;
             // levels whose side was raised to the bin-count limit repeat the previous one
             if (l > 0 && idx->side <= B->lev[l - 1]->side) break;
         }
@@ -444,7 +457,8 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
     LevelDesc hl[kMaxLev];
     for (int l = 0; l < P.nlev; l++) {
         const mgk_index* I = B->lev[l];
-        hl[l] = LevelDesc{I->pts, I->bin_start, I->perm, I->ox, I->oy, I->side, 1.0 / I->side, I->nbx, I->nby};
+        hl[l] = LevelDesc{I->pts, I->bin_start, I->perm, B->qord[l], I->ox, I->oy, I->side, 1.0 / I->side, I->nbx,
+                          I->nby};
         P.side[l] = I->side;
     }
     if (cudaMemcpy(B->d_lev, hl, sizeof(LevelDesc) * P.nlev, cudaMemcpyHostToDevice) != cudaSuccess) {

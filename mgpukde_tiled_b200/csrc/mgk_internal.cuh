@@ -218,6 +218,8 @@ __device__ __host__ __forceinline__ double mgk_h2(float h) {
 
 // ---- kernels launched across translation units ------------------------------
 int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float bin_size, mgk_index* idx);
+// d_order[k] = position of the k-th record of idx in Z-order of the bins (n entries, device).
+int mgk_index_zorder(mgk_ctx* ctx, const mgk_index* idx, int32_t* d_order);
 int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
                        int64_t col0, int64_t nr, int64_t nc, const float* d_mask, float* d_out,
                        unsigned long long* d_evals, bool fp64);
