@@ -107,7 +107,7 @@ uint64_t estimate_bytes(const mgk_request& r, int64_t tile) {
     uint64_t b = n * 24;         // x, y, w, dist2, ew
     b += n * 64;                 // index records, permutation and sort scratch
     const double ext = std::max(r.grid.ncols, r.grid.nrows) * (double)r.grid.cs + 6.0 * r.h;
-    const double side = std::max(0.75 * (double)r.h, ext / 4096.0);
+    const double side = std::max(0.5 * (double)r.h, ext / 4096.0);  // the default bin factor
     const double bins = std::min(4096.0 * 4096.0, std::pow(ext / side + 2.0, 2.0));
     b += (uint64_t)(bins * 4.0);
     if (r.edge) b += (uint64_t)r.edge_grid.ncols * (uint64_t)r.edge_grid.nrows * 24;
