@@ -336,6 +336,7 @@ void worker_main(mgk_server* S) {
             act = S->active;
         }
         if (!act.empty()) tick(S, act);
+        else reap(S, true);  // slots held by draining requests: wait for their copies instead of spinning
     }
 }
 
