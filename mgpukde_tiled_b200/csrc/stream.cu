@@ -97,16 +97,6 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
         if (st == MGK_OK && cudaEventCreateWithFlags(&ev_mask, cudaEventDisableTiming) != cudaSuccess)
             st = mgk_fail(c, MGK_ERR_CUDA, "event");
     }
-    for (int b = 0; b < 3 && st == MGK_OK; b++) {
-        if (cudaMallocHost((void**)&slots[b].host, tb) != cudaSuccess) st = mgk_fail(c, MGK_ERR_CUDA, "pinned");
-        else if (cudaEventCreateWithFlags(&slots[b].copied, cudaEventDisableTiming) != cudaSuccess)
-            st = mgk_fail(c, MGK_ERR_CUDA, "event");
-    }
-    if (st == MGK_OK && evals) {
-        st = mgk_alloc(c, (void**)&d_ev, sizeof(unsigned long long));
-        if (st == MGK_OK && cudaMemsetAsync(d_ev, 0, sizeof(unsigned long long), c->stream) != cudaSuccess)
-            st = MGK_ERR_CUDA;
-    }
     // The library's own copy sink into page-locked host memory: the result
     // tiles are copied straight into the target raster (2-D copies on the
     // copy stream), without the staging buffers and the writer thread.
@@ -117,6 +107,19 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
         if (t->base && cudaPointerGetAttributes(&pa, t->base) == cudaSuccess && pa.type == cudaMemoryTypeHost)
             direct = t;
         cudaGetLastError();
+    }
+    // three page-locked staging tiles for the writer thread (not needed by the
+    // direct copies; pinning them costs tens of ms for 4096^2 tiles)
+    for (int b = 0; b < 3 && st == MGK_OK; b++) {
+        if (!direct && cudaMallocHost((void**)&slots[b].host, tb) != cudaSuccess)
+            st = mgk_fail(c, MGK_ERR_CUDA, "pinned");
+        else if (cudaEventCreateWithFlags(&slots[b].copied, cudaEventDisableTiming) != cudaSuccess)
+            st = mgk_fail(c, MGK_ERR_CUDA, "event");
+    }
+    if (st == MGK_OK && evals) {
+        st = mgk_alloc(c, (void**)&d_ev, sizeof(unsigned long long));
+        if (st == MGK_OK && cudaMemsetAsync(d_ev, 0, sizeof(unsigned long long), c->stream) != cudaSuccess)
+            st = MGK_ERR_CUDA;
     }
     Writer W;
     W.sink = sink;
