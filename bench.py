@@ -401,7 +401,11 @@ def run_mgk(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     ms_max = float(t.item())
-    total_evals = evals * world
+    total_evals = evals
+    if world > 1:  # each rank ran its own study: the job's evals are the sum over ranks
+        ev_t = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
+        dist.all_reduce(ev_t, op=dist.ReduceOp.SUM)
+        total_evals = int(ev_t.item())
     value = total_evals / (ms_max / 1e3)
 
     # end to end: the C ABI from pinned host buffers (inputs H2D and the raster D2H every step)
