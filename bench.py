@@ -703,8 +703,12 @@ def run_out_of_core(args):
 
     import mgpukde_tiled_b200 as mk
 
+    import torch.distributed as dist
+
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
+    if world > 1:  # one job per rank (seed 3 + rank), no data exchange
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     c = synth.out_of_core(scale=args.scale, seed=3 + rank)
     dg, eg = mk.Grid.of(c["density_grid"]), mk.Grid.of(c["edge_grid"])
     h = float(c["h"])
@@ -747,7 +751,14 @@ def run_out_of_core(args):
     ms = e0.elapsed_time(e1) / args.steps
     launches = (ctx.kernel_launches - l0) / args.steps
     ntiles = ((dg.nrows + tile - 1) // tile) * ((dg.ncols + tile - 1) // tile)
-    out = {"metric": METRIC, "value": evals * world / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+    total_evals = evals
+    if world > 1:  # the slowest rank's time, every rank's evals
+        red = torch.tensor([ms, float(evals)], device="cuda", dtype=torch.float64)
+        t_max, ev_sum = red[:1].clone(), red[1:].clone()
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+        dist.all_reduce(ev_sum, op=dist.ReduceOp.SUM)
+        ms, total_evals = float(t_max.item()), int(ev_sum.item())
+    out = {"metric": METRIC, "value": total_evals / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
            "config": {"workload": f"out_of_core: {len(c['x'])} points (70% from 500 Gaussians, 30% uniform) in "
@@ -757,10 +768,13 @@ def run_out_of_core(args):
            "evals_per_step": evals, "density_evals": ev_d, "edge_evals": ev_e,
            "output_bytes": int(host.nbytes), "output_gb_s": host.nbytes / (ms / 1e3) / 1e9,
            "gpu_launches": launches, "clocks": clocks}
-    print(json.dumps(out))
+    if rank == 0:
+        print(json.dumps(out))
     pts.close()
     em.close()
     ctx.close()
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 
