@@ -22,7 +22,7 @@
 namespace {
 
 constexpr int kSortThreads = 256;
-constexpr int kSortItems = 8;  // per thread per tile
+constexpr int kSortItems = 32;  // per thread per tile
 constexpr int kSortTile = kSortThreads * kSortItems;
 
 __device__ __forceinline__ unsigned f2ord(float f) {
