@@ -258,8 +258,8 @@ def crop_evals(c, crop):
     b = o.mark_boundary(eg, c["edge_mask"])
     d2 = o.dist2_boundary(crop["x"], crop["y"], eg, b)
     ew, eev = o.edge_weights(crop["x"], crop["y"], c["h"], d2, eg, c["edge_mask"])
-    _, dev = o.density(crop["x"], crop["y"], crop["w"], ew, c["h"], o.grid(*crop["grid"].astuple()), crop["mask"])
-    return dev, eev, ew
+    den, dev = o.density(crop["x"], crop["y"], crop["w"], ew, c["h"], o.grid(*crop["grid"].astuple()), crop["mask"])
+    return dev, eev, ew, den
 
 
 def run_reference_binary(c, crop, threads):
@@ -284,11 +284,25 @@ def run_reference_binary(c, crop, threads):
         return (t_den + t_edge) / 1e3
 
 
-def cpu_baseline(c, side=1024):
-    """The reference's CPU path (or the FP64 oracle port) on a crop of the workload."""
+def cpu_baseline(c, side=1024, gpu_window=None):
+    """The reference's CPU path (or the FP64 oracle port) on a crop of the
+    workload.  gpu_window: the GPU raster over the same window, checked
+    against the FP64 oracle's density of the crop (its halo points are all
+    the points that reach it)."""
     threads = os.cpu_count() or 1
     crop = crop_inputs(c, side)
-    dev, eev, ew = crop_evals(c, crop)
+    dev, eev, ew, den_ref = crop_evals(c, crop)
+    acc = None
+    if gpu_window is not None:
+        valid = crop["mask"] != crop["grid"].nodata
+        ref = den_ref[valid].astype(np.float64)
+        got = gpu_window[valid].astype(np.float64)
+        rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
+        acc = {"max_rel_err": float(rel.max()) if rel.size else 0.0,
+               "nodata_cells_equal": bool(np.array_equal(gpu_window[~valid], crop["mask"][~valid])),
+               "cells": int(valid.sum()),
+               "sample": f"the cpu_baseline window ({side}x{side}) of the last timed step's raster against the "
+                         f"FP64 oracle"}
     if os.path.exists(REF_BIN):
         t = run_reference_binary(c, crop, threads)
         kind = "reference"
@@ -302,8 +316,11 @@ def cpu_baseline(c, side=1024):
     sample = (f"{side}x{side} density window (median-density of 25 candidate windows) with its {len(crop['x'])} halo points "
               f"(density + edge-correction evals {dev + eev}); reference brute-force CPU path, "
               f"{'mode 1, h_option -1' if kind == 'reference' else 'FP64 oracle'}")
-    return {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
-            "seconds": t}
+    out = {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+           "seconds": t}
+    if acc is not None:
+        out["accuracy"] = acc
+    return out
 
 
 def run_reference_arm(args):
@@ -401,6 +418,12 @@ def run_mgk(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     ms_max = float(t.item())
+    # the timed steps' raster over the CPU baseline's window, for the accuracy check
+    acc_window = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        side = min(1024, dg.nrows, dg.ncols)
+        wr0, wc0 = pick_window(c, side)
+        acc_window = dout[wr0:wr0 + side, wc0:wc0 + side].cpu().numpy()
     total_evals = evals
     if world > 1:  # each rank ran its own study: the job's evals are the sum over ranks
         ev_t = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
@@ -486,7 +509,8 @@ def run_mgk(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             unbind_numa()
-            out["cpu_baseline"] = cpu_baseline(c)
+            out["cpu_baseline"] = cpu_baseline(c, gpu_window=acc_window)
+            out["accuracy"] = out["cpu_baseline"].pop("accuracy", None)
         except Exception as e:  # reported, not fatal
             out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
     if rank == 0:
