@@ -524,6 +524,29 @@ def run_mgk(args):
 
 
 # ------------------------------------------------- bandwidth selection (C2) --
+def loo_cpu_check(c, hgrid, logl, pts, nsmall=16):
+    """The FP64 oracle's LogLikelihood (edge weights at h, leave-one-out sum)
+    for the nsmall smallest h of the grid, all host threads: the CPU baseline
+    (evals/s over those h) and the relative error of the GPU's logL there."""
+    import oracle_py as o
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    d2, _ = pts.download(dist2=True, ew=False)
+    eg = o.grid(*c["edge_grid"].astuple())
+    ks = list(np.argsort(hgrid)[:nsmall])
+    t0 = time.perf_counter()
+    refs = [o.loglik_at(c["x"], c["y"], c["w"], d2, eg, c["edge_mask"], float(hgrid[k])) for k in ks]
+    t = time.perf_counter() - t0
+    ev = sum(r[1] for r in refs)
+    rel = [abs(float(logl[k]) - r[0]) / abs(r[0]) for k, r in zip(ks, refs)]
+    cb = {"value": ev / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": "port", "seconds": t,
+          "sample": f"FP64 oracle LogLikelihood (edge weights + leave-one-out) at the {nsmall} smallest h of the grid "
+                    f"({', '.join('%.2f' % hgrid[k] for k in ks)}), all {len(c['x'])} points: {ev} evals"}
+    acc = {"logl_max_rel_err": float(max(rel)), "h_checked": [float(hgrid[k]) for k in ks],
+           "sample": "GPU logL of the timed batch against the FP64 oracle at those h"}
+    return cb, acc
+
+
 def run_bandwidth_select(args):
     """One step = one batched bandwidth selection: point-to-boundary distances,
     then edge weights and the leave-one-out log likelihood for 64 log-spaced
@@ -583,6 +606,9 @@ def run_bandwidth_select(args):
            "evals_per_step": evals, "edge_evals": ev_edge, "loo_evals": ev_loo,
            "batch_ms": float(np.mean(loo_ms)), "argmax": best, "h_best": float(hgrid[best]),
            "gpu_launches": launches, "clocks": clocks}
+    if not args.no_cpu_baseline:
+        unbind_numa()
+        out["cpu_baseline"], out["accuracy"] = loo_cpu_check(c, hgrid, logl, pts)
     print(json.dumps(out))
     pts.close()
     em.close()
@@ -591,7 +617,7 @@ def run_bandwidth_select(args):
 
 
 # ------------------------------------------------- adaptive bandwidths (h_option 2) --
-def adaptive_cpu_baseline(scale):
+def adaptive_cpu_baseline(scale, gpu_logl=None):
     """One adaptive likelihood evaluation of the FP64 oracle port, all host
     threads, on the workload's points and mask: edge weights at h, pilot
     density, bandwidths, edge weights at hs, leave-one-out density."""
@@ -609,14 +635,19 @@ def adaptive_cpu_baseline(scale):
     den0, p0 = o.point_density(x, y, w, ew1, h, self_term=True)
     hs = o.adaptive_bandwidths(den0, h, -0.5)
     ew2, e2 = o.edge_weights(x, y, 0.0, d2, eg, em, hs=hs)
-    _, p1 = o.point_density(x, y, w, ew2, 0.0, hs=hs, self_term=False)
+    den1, p1 = o.point_density(x, y, w, ew2, 0.0, hs=hs, self_term=False)
     t = time.perf_counter() - t0
     ev = e1 + e2 + p0 + p1
+    ref_ll = float(np.sum(np.log(np.maximum(den1, float(np.float32(1e-14))))))
     return {"value": ev / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"one adaptive likelihood evaluation (h = rule of thumb {h:.3f}, alpha = -0.5) of the FP64 "
                       f"oracle on the workload ({len(x)} points, edge mask "
                       f"{c['edge_grid'].ncols}^2): {e1 + e2} edge-mask cells, {p0 + p1} pairs",
-            "seconds": t}
+            "seconds": t,
+            "accuracy": None if gpu_logl is None else
+            {"logl_rel_err": abs(gpu_logl - ref_ll) / abs(ref_ll), "h": h, "alpha": -0.5,
+             "sample": "the GPU's adaptive LogLikelihood at the rule-of-thumb h and alpha -0.5 against the "
+                       "FP64 oracle's"}}
 
 
 def run_adaptive(args):
@@ -709,7 +740,10 @@ def run_adaptive(args):
            "gpu_launches": launches, "clocks": clocks}
     if not args.no_cpu_baseline:
         unbind_numa()
-        out["cpu_baseline"] = adaptive_cpu_baseline(0.5 * args.scale)
+        mk.calc_dist2_boundary(ctx, pts, em)
+        gpu_ll = mk.loglik_adaptive(ctx, pts, em, h0, -0.5)
+        out["cpu_baseline"] = adaptive_cpu_baseline(0.5 * args.scale, gpu_ll)
+        out["accuracy"] = out["cpu_baseline"].pop("accuracy", None)
     print(json.dumps(out))
     pts.close()
     em.close()
