@@ -78,29 +78,34 @@ int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes) {
     return MGK_OK;
 }
 
-int mgk_host_stage(mgk_ctx* c, size_t bytes, void** host, void** dev) {
-    if (bytes > c->h_stage_bytes) {
-        if (c->h_stage) cudaFreeHost(c->h_stage);
-        c->h_stage = nullptr;
-        c->d_stage = nullptr;
-        c->h_stage_bytes = 0;
+int mgk_host_stage_slot(mgk_ctx* c, int slot, size_t bytes, void** host, void** dev) {
+    if (slot < 0 || slot >= mgk_ctx::kStageSlots) return mgk_fail(c, MGK_ERR_INVALID, "staging slot out of range");
+    if (bytes > c->h_stage_bytes[slot]) {
+        if (c->h_stage[slot]) cudaFreeHost(c->h_stage[slot]);
+        c->h_stage[slot] = nullptr;
+        c->d_stage[slot] = nullptr;
+        c->h_stage_bytes[slot] = 0;
         const size_t want = std::max<size_t>(bytes + bytes / 4, 1 << 16);
-        cudaError_t e = cudaHostAlloc(&c->h_stage, want, cudaHostAllocMapped);
+        cudaError_t e = cudaHostAlloc(&c->h_stage[slot], want, cudaHostAllocMapped);
         if (e != cudaSuccess) {
-            c->h_stage = nullptr;
+            c->h_stage[slot] = nullptr;
             return mgk_cuda_fail(c, e, "mapped page-locked staging");
         }
-        e = cudaHostGetDevicePointer(&c->d_stage, c->h_stage, 0);
+        e = cudaHostGetDevicePointer(&c->d_stage[slot], c->h_stage[slot], 0);
         if (e != cudaSuccess) {
-            cudaFreeHost(c->h_stage);
-            c->h_stage = nullptr;
+            cudaFreeHost(c->h_stage[slot]);
+            c->h_stage[slot] = nullptr;
             return mgk_cuda_fail(c, e, "mapped page-locked staging address");
         }
-        c->h_stage_bytes = want;
+        c->h_stage_bytes[slot] = want;
     }
-    *host = c->h_stage;
-    *dev = c->d_stage;
+    *host = c->h_stage[slot];
+    *dev = c->d_stage[slot];
     return MGK_OK;
+}
+
+int mgk_host_stage(mgk_ctx* c, size_t bytes, void** host, void** dev) {
+    return mgk_host_stage_slot(c, 0, bytes, host, dev);
 }
 
 void mgk_free(mgk_ctx* ctx, void* p, size_t bytes) {
@@ -170,7 +175,8 @@ int mgk_ctx_destroy(mgk_ctx* c) {
     if (c->d_sum) cudaFree(c->d_sum);
     if (c->h_counter) cudaFreeHost(c->h_counter);
     if (c->h_sum) cudaFreeHost(c->h_sum);
-    if (c->h_stage) cudaFreeHost(c->h_stage);
+    for (int i = 0; i < mgk_ctx::kStageSlots; i++)
+        if (c->h_stage[i]) cudaFreeHost(c->h_stage[i]);
     if (c->ev_a) cudaEventDestroy(c->ev_a);
     if (c->ev_b) cudaEventDestroy(c->ev_b);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -690,6 +696,11 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         if (e == cudaSuccess) e = cudaEventRecord(pipe.mask_ready[b], pipe.h2d);
         return e;
     };
+    // the density kernels' eval counter and staging-wait flag (counters 4 and
+    // 7, shared by all tiles), zeroed before any copy is in flight
+    if (st == MGK_OK && (ce = cudaMemsetAsync(c->d_counter + 4, 0, 4 * sizeof(unsigned long long), c->stream)) !=
+                            cudaSuccess)
+        st = mgk_cuda_fail(c, ce, "kde_raster counters");
     if (st == MGK_OK) st = mgk_points_upload(c, n, x, y, w, h_pp, &p);
     if (st == MGK_OK && edge_correction) st = mgk_raster_upload(c, eg, emask, &em);
     // the first tile's mask travels while the points are prepared
@@ -707,11 +718,7 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         ce = cudaMemcpyAsync(out_ew, p->ew, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
         if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster ew");
     }
-    if (st == MGK_OK && evals) {
-        ce = cudaMemsetAsync(c->d_counter + 4, 0, sizeof(unsigned long long), c->stream);
-        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster counter");
-    }
-    // density of tile k - 1 out, after its kernels (event done) and into the host raster
+    // density of tile k out, after its kernels (event done) and into the host raster
     auto out_copy = [&](int64_t k) -> cudaError_t {
         if (k < 0) return cudaSuccess;
         int64_t r0, c0, nr, nc;
@@ -724,38 +731,87 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         if (e == cudaSuccess) e = cudaEventRecord(pipe.out_free[b], pipe.d2h);
         return e;
     };
-    // Per tile: plan it (this waits on the context stream and sends the small
-    // work list while no large copy is queued ahead of it), then queue the
-    // previous tile's density out and the next tile's mask in, then run the
-    // kernels, which the two large copies overlap.
-    for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
+    // Tile k's plan is made while tile k - 1 computes: the counting kernel of
+    // tile k is queued ahead of tile k - 1's density on the same stream, so
+    // the host can plan from its counts (staging slot 1 + k % 2) while that
+    // density runs, and the next density launch follows without a gap.  When
+    // the counting kernel of tile k has finished, the density of tile k - 2
+    // (queued before it) has too, so that plan and its staging slot are free.
+    mgk_dplan* plans[2] = {nullptr, nullptr};
+    cudaEvent_t counted = nullptr;
+    if (st == MGK_OK && (ce = cudaEventCreateWithFlags(&counted, cudaEventDisableTiming)) != cudaSuccess)
+        st = mgk_cuda_fail(c, ce, "kde_raster event");
+    unsigned long long* d_ev = evals ? c->d_counter + 4 : nullptr;
+    auto plan_of = [&](int64_t k) -> int {  // after tile k's counting kernel has finished
         int64_t r0, c0, nr, nc;
         tile_of(k, r0, c0, nr, nc);
         const int b = (int)(k & 1);
-        mgk_dplan* plan = nullptr;
-        if ((st = mgk_density_prepare(c, idx, dg, r0, c0, nr, nc, d_mask[b], d_out[b],
-                                      evals ? c->d_counter + 4 : nullptr, false, &plan)))
+        mgk_density_discard(c, plans[b]);  // tile k - 2's
+        plans[b] = nullptr;
+        return mgk_density_plan_counted(c, idx, dg, r0, c0, nr, nc, d_mask[b], d_out[b], d_ev, 1 + b, &plans[b]);
+    };
+    auto count_of = [&](int64_t k) -> int {
+        int64_t r0, c0, nr, nc;
+        tile_of(k, r0, c0, nr, nc);
+        return mgk_density_counts_launch(c, idx, dg, r0, c0, nr, nc, 1 + (int)(k & 1), c->stream);
+    };
+    // both slots sized up front for a full tile's counts and work list, so a
+    // counting launch never has to regrow a slot whose previous plan may still
+    // be running
+    for (int i = 1; i <= 2 && st == MGK_OK; i++) {
+        void *hs = nullptr, *ds = nullptr;
+        const size_t nblk = (size_t)((tr + 63) / 64) * (size_t)((tc + 127) / 128);
+        st = mgk_host_stage_slot(c, i, 64 * nblk + 4096, &hs, &ds);
+    }
+    if (st == MGK_OK && ntiles > 0 && (st = count_of(0)) == MGK_OK) {
+        if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster plan");
+        else st = plan_of(0);
+    }
+    for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
+        const int b = (int)(k & 1);
+        ce = mask_in(k + 1);  // after tile k - 1's density has read that buffer
+        if (ce != cudaSuccess) {
+            st = mgk_cuda_fail(c, ce, "kde_raster mask");
             break;
-        ce = out_copy(k - 1);
-        if (ce == cudaSuccess) ce = mask_in(k + 1);
-        if (ce == cudaSuccess && dmask) ce = cudaStreamWaitEvent(c->stream, pipe.mask_ready[b], 0);
+        }
+        if (k + 1 < ntiles) {
+            if ((st = count_of(k + 1))) break;
+            if ((ce = cudaEventRecord(counted, c->stream)) != cudaSuccess) {
+                st = mgk_cuda_fail(c, ce, "kde_raster");
+                break;
+            }
+        }
+        if (dmask) ce = cudaStreamWaitEvent(c->stream, pipe.mask_ready[b], 0);
         if (ce == cudaSuccess && k >= 2) ce = cudaStreamWaitEvent(c->stream, pipe.out_free[b], 0);
         if (ce != cudaSuccess) {
-            mgk_density_discard(c, plan);
             st = mgk_cuda_fail(c, ce, "kde_raster tile");
             break;
         }
-        if ((st = mgk_density_execute(c, plan))) break;
-        if ((ce = cudaEventRecord(pipe.done[b], c->stream)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster");
+        if ((st = mgk_density_launch_plan(c, plans[b], c->stream))) break;
+        ce = cudaEventRecord(pipe.done[b], c->stream);
+        if (ce == cudaSuccess) ce = out_copy(k);
+        if (ce != cudaSuccess) {
+            st = mgk_cuda_fail(c, ce, "kde_raster tile");
+            break;
+        }
+        if (k + 1 < ntiles) {
+            if ((ce = cudaEventSynchronize(counted)) != cudaSuccess) {
+                st = mgk_cuda_fail(c, ce, "kde_raster plan");
+                break;
+            }
+            st = plan_of(k + 1);
+        }
     }
-    if (st == MGK_OK && (ce = out_copy(ntiles - 1)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster tile");
     // every copy and kernel of this call ends before its buffers are released
     if ((ce = cudaStreamSynchronize(pipe.h2d)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
     if ((ce = cudaStreamSynchronize(pipe.d2h)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
     if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
-    if (st == MGK_OK && evals) {
-        ce = cudaMemcpy(c->h_counter + 4, c->d_counter + 4, sizeof(unsigned long long), cudaMemcpyDeviceToHost);
-        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster counter");
+    for (int i = 0; i < 2; i++) mgk_density_discard(c, plans[i]);  // every kernel has ended
+    if (counted) cudaEventDestroy(counted);
+    if (st == MGK_OK) {  // counters 4 (density evals) and 7 (staging-wait flag)
+        ce = cudaMemcpy(c->h_counter + 4, c->d_counter + 4, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+        if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster counters");
+        else if (c->h_counter[7]) st = mgk_fail(c, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
         else ev_den = (int64_t)c->h_counter[4];
     }
     for (int i = 0; i < 2; i++) {

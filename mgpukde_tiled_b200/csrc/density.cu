@@ -922,12 +922,33 @@ static void dplan_release(mgk_ctx* ctx, mgk_dplan* D) {
 
 void mgk_density_discard(mgk_ctx* ctx, mgk_dplan* D) { dplan_release(ctx, D); }
 
-int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+// The counting kernel of a tile into staging slot `slot` (counts at offset 0).
+static int counts_launch(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                         int64_t nr, int64_t nc, int slot, cudaStream_t s, bool zero_err) {
+    if (nr <= 0 || nc <= 0) return MGK_OK;
+    DParams P;
+    fill_params(P, idx, g, row0, col0, nr, nc, nullptr, nullptr);
+    P.err = zero_err ? ctx->d_counter + 7 : nullptr;  // other tiles' kernels may share the flag
+    const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
+    const int nblk = nbx_t * nby_t;
+    char *h_st = nullptr, *d_st = nullptr;
+    const int st = mgk_host_stage_slot(ctx, slot, sizeof(int64_t) * nblk, (void**)&h_st, (void**)&d_st);
+    if (st) return st;
+    k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, reinterpret_cast<int64_t*>(d_st));
+    const cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    return MGK_OK;
+}
+
+// The plan of a tile from the counts in staging slot `slot` (its counting
+// kernel has finished); the work list, split tables and error flag go into
+// the same slot.
+static int plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
                         int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
-                        bool fp64, mgk_dplan** out) {
+                        bool fp64, int slot, mgk_dplan** out) {
     *out = nullptr;
     if (nr <= 0 || nc <= 0) return MGK_OK;
-    cudaStream_t s = ctx->stream;
     mgk_dplan* D = new (std::nothrow) mgk_dplan();
     if (!D) return mgk_fail(ctx, MGK_ERR_INVALID, "density plan: out of host memory");
     D->idx = idx;
@@ -937,26 +958,17 @@ int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
     fill_params(P, idx, g, row0, col0, nr, nc, d_mask, d_out);
     P.evals = d_evals;
     P.err = ctx->d_counter + 7;
-
     const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
-    const int nblk = nbx_t * nby_t;
     int st;
-    // ---- plan: candidates per block (written straight into host memory) ->
-    // work items (heavy blocks split) ----
-    char *h_st = nullptr, *d_st = nullptr;
-    if ((st = mgk_host_stage(ctx, sizeof(int64_t) * nblk, (void**)&h_st, (void**)&d_st))) {
-        delete D;
-        return st;
-    }
-    k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, reinterpret_cast<int64_t*>(d_st));
-    cudaError_t ce = cudaGetLastError();
-    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
-    if (ce != cudaSuccess) {
-        delete D;
-        return mgk_cuda_fail(ctx, ce, "density plan");
-    }
     TilePlan& T = D->T;
-    plan_tile(reinterpret_cast<const int64_t*>(h_st), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
+    {
+        char *h_st = nullptr, *d_st = nullptr;
+        if ((st = mgk_host_stage_slot(ctx, slot, sizeof(int64_t) * nbx_t * nby_t, (void**)&h_st, (void**)&d_st))) {
+            delete D;
+            return st;
+        }
+        plan_tile(reinterpret_cast<const int64_t*>(h_st), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
+    }
     sort_items(T.items);
     const int32_t nslots = T.nslots;
     D->b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
@@ -970,7 +982,8 @@ int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
     const size_t b_items = sizeof(Item) * T.items.size();
     const size_t b_sb = sizeof(int32_t) * T.split_blocks.size(), b_sbeg = sizeof(int32_t) * T.split_begin.size();
     const size_t o_sb = up16(b_items), o_sbeg = o_sb + up16(b_sb), o_err = o_sbeg + up16(b_sbeg);
-    if ((st = mgk_host_stage(ctx, o_err + sizeof(unsigned long long), (void**)&h_st, (void**)&d_st))) {
+    char *h_st = nullptr, *d_st = nullptr;
+    if ((st = mgk_host_stage_slot(ctx, slot, o_err + sizeof(unsigned long long), (void**)&h_st, (void**)&d_st))) {
         dplan_release(ctx, D);
         return st;
     }
@@ -986,6 +999,51 @@ int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
     D->d_err = reinterpret_cast<unsigned long long*>(d_st + o_err);
     *D->h_err = 0;
     *out = D;
+    return MGK_OK;
+}
+
+int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                        int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
+                        bool fp64, mgk_dplan** out) {
+    *out = nullptr;
+    if (nr <= 0 || nc <= 0) return MGK_OK;
+    int st = counts_launch(ctx, idx, g, row0, col0, nr, nc, 0, ctx->stream, true);
+    if (st) return st;
+    const cudaError_t ce = cudaStreamSynchronize(ctx->stream);
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density plan");
+    return plan_counted(ctx, idx, g, row0, col0, nr, nc, d_mask, d_out, d_evals, fp64, 0, out);
+}
+
+int mgk_density_counts_launch(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                              int64_t nr, int64_t nc, int slot, cudaStream_t s) {
+    return counts_launch(ctx, idx, g, row0, col0, nr, nc, slot, s, false);
+}
+
+int mgk_density_plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                             int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
+                             int slot, mgk_dplan** out) {
+    return plan_counted(ctx, idx, g, row0, col0, nr, nc, d_mask, d_out, d_evals, false, slot, out);
+}
+
+int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
+    if (!D) return MGK_OK;
+    const DParams& P = D->P;
+    const bool varh = D->idx->varh;
+    const unsigned grid = (unsigned)D->T.items.size();
+    if (D->count) {
+        if (varh) launch_density<true, true>(grid, s, P);
+        else launch_density<false, true>(grid, s, P);
+    } else {
+        if (varh) launch_density<true, false>(grid, s, P);
+        else launch_density<false, false>(grid, s, P);
+    }
+    MGK_COUNT_LAUNCH(ctx, 1);
+    if (D->T.nslots) {
+        k_merge<<<(unsigned)D->T.split_blocks.size(), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
+        MGK_COUNT_LAUNCH(ctx, 1);
+    }
+    const cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density");
     return MGK_OK;
 }
 
@@ -1011,7 +1069,7 @@ int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* D) {
         }
         cudaEventRecord(ctx->ev_b, s);
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
-        MGK_COUNT_LAUNCH(ctx, 2);  // plan + density
+        MGK_COUNT_LAUNCH(ctx, 1);  // density (the counting kernel counts itself)
         if (D->T.nslots) {
             k_merge<<<(unsigned)D->T.split_blocks.size(), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
             if ((ce = cudaGetLastError()) != cudaSuccess) break;

@@ -34,9 +34,12 @@ struct mgk_ctx {
     unsigned long long* h_counter = nullptr;  // pinned mirror
     double* d_sum = nullptr;                  // 256 doubles
     double* h_sum = nullptr;                  // pinned mirror
-    void* h_stage = nullptr;                  // mapped page-locked staging of plans and counts (mgk_host_stage)
-    void* d_stage = nullptr;                  // its device address
-    size_t h_stage_bytes = 0;
+    // mapped page-locked staging of plans and counts (mgk_host_stage), in
+    // kStageSlots independent slots; h_stage[i] and d_stage[i] address the same bytes
+    static constexpr int kStageSlots = 3;
+    void* h_stage[kStageSlots] = {};
+    void* d_stage[kStageSlots] = {};
+    size_t h_stage_bytes[kStageSlots] = {};
     std::multimap<size_t, void*> pool;        // cached device blocks by size class
     uint64_t launches = 0;                    // kernels launched by this context
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
@@ -129,6 +132,9 @@ int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes);
 // behind large copies that other streams have in flight.  One user at a time:
 // kernels using it must have finished before the next call.
 int mgk_host_stage(mgk_ctx* ctx, size_t bytes, void** host, void** dev);
+// The same for staging slot `slot` (0 is the one mgk_host_stage uses); plans
+// that are alive at the same time use different slots.
+int mgk_host_stage_slot(mgk_ctx* ctx, int slot, size_t bytes, void** host, void** dev);
 void mgk_free(mgk_ctx* ctx, void* p, size_t bytes);
 
 #define MGK_CHECK_CUDA(ctx, expr)                                   \
@@ -237,6 +243,19 @@ int mgk_density_prepare(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
                         bool fp64, mgk_dplan** out);
 int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* plan);
 void mgk_density_discard(mgk_ctx* ctx, mgk_dplan* plan);
+// A tile pipeline that plans tile k + 1 while tile k computes, all on one
+// stream: counts_launch queues the counting kernel of a tile into staging
+// slot `slot` (it leaves the shared staging-wait flag alone: the caller
+// zeroes it once and reads it at the end); once that kernel has finished,
+// plan_counted builds the plan from the counts into the same slot; launch
+// queues the plan's kernels on stream s without waiting; discard releases the
+// plan after its kernels have finished.
+int mgk_density_counts_launch(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                              int64_t nr, int64_t nc, int slot, cudaStream_t s);
+int mgk_density_plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                             int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
+                             int slot, mgk_dplan** out);
+int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
 int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r);
