@@ -127,9 +127,51 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
     W.device = c->device;
     std::thread wt;
     if (st == MGK_OK) wt = std::thread([&W] { W.run(); });
-    int64_t k_out = 0;  // tiles computed in this call (selects the device buffer)
-    for (int64_t t = 0; st == MGK_OK && t < ntx * nty; t++) {
-        if (done && done[t]) continue;
+    // The tiles this call computes (a resume skips those marked done).
+    std::vector<int64_t> todo;
+    for (int64_t t = 0; t < ntx * nty; t++)
+        if (!done || !done[t]) todo.push_back(t);
+    auto geom = [&](int64_t t, int64_t& r0, int64_t& c0, int64_t& nr, int64_t& nc) {
+        r0 = (t / ntx) * tr;
+        c0 = (t % ntx) * tc;
+        nr = std::min(tr, g->nrows - r0);
+        nc = std::min(tc, g->ncols - c0);
+    };
+    // Tile k + 1 is planned while tile k computes: its counting kernel is
+    // queued on the context stream ahead of tile k's density, the host plans
+    // from the counts (staging slot 1 + (k + 1) % 2) while that density runs,
+    // and the next launch follows without a gap.  The staging-wait flag
+    // (counter 7) is shared by all tiles: zeroed here, read at the end.
+    mgk_dplan* plans[2] = {nullptr, nullptr};
+    cudaEvent_t counted = nullptr;
+    if (st == MGK_OK && cudaEventCreateWithFlags(&counted, cudaEventDisableTiming) != cudaSuccess)
+        st = mgk_fail(c, MGK_ERR_CUDA, "event");
+    if (st == MGK_OK && cudaMemsetAsync(c->d_counter + 7, 0, sizeof(unsigned long long), c->stream) != cudaSuccess)
+        st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: flag");
+    for (int i = 1; i <= 2 && st == MGK_OK; i++) {  // slots sized for a full tile up front
+        void *hs = nullptr, *ds = nullptr;
+        st = mgk_host_stage_slot(c, i, 64 * (size_t)((tr + 63) / 64) * (size_t)((tc + 127) / 128) + 4096, &hs, &ds);
+    }
+    auto count_of = [&](size_t k) -> int {
+        int64_t r0, c0, nr, nc;
+        geom(todo[k], r0, c0, nr, nc);
+        return mgk_density_counts_launch(c, idx, g, r0, c0, nr, nc, 1 + (int)(k & 1), c->stream);
+    };
+    auto plan_of = [&](size_t k) -> int {  // after tile k's counting kernel has finished
+        int64_t r0, c0, nr, nc;
+        geom(todo[k], r0, c0, nr, nc);
+        const int b = (int)(k & 1);
+        mgk_density_discard(c, plans[b]);  // tile k - 2's, whose kernels have ended
+        plans[b] = nullptr;
+        return mgk_density_plan_counted(c, idx, g, r0, c0, nr, nc, mask_src ? d_mask : nullptr, d_out[b], d_ev,
+                                        1 + b, &plans[b]);
+    };
+    if (st == MGK_OK && !todo.empty() && (st = count_of(0)) == MGK_OK) {
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess) st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: plan");
+        else st = plan_of(0);
+    }
+    for (size_t k_out = 0; st == MGK_OK && k_out < todo.size(); k_out++) {
+        const int64_t t = todo[k_out];
         {
             std::lock_guard<std::mutex> lk(W.mu);
             if (W.status) {
@@ -137,8 +179,8 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
                 break;
             }
         }
-        const int64_t r0 = (t / ntx) * tr, c0 = (t % ntx) * tc;
-        const int64_t nr = std::min(tr, g->nrows - r0), nc = std::min(tc, g->ncols - c0);
+        int64_t r0, c0, nr, nc;
+        geom(t, r0, c0, nr, nc);
         const int b = (int)(k_out & 1);
         // the mask tile: read on this thread, copied on the copy stream
         if (mask_src) {
@@ -150,19 +192,23 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
             // the previous density must be done with d_mask before it is overwritten
             if (cudaStreamWaitEvent(cs, ev_den[b ^ 1], 0) != cudaSuccess ||
                 cudaMemcpyAsync(d_mask, h_mask, sizeof(float) * nr * nc, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
-                cudaEventRecord(ev_mask, cs) != cudaSuccess ||
-                cudaStreamWaitEvent(c->stream, ev_mask, 0) != cudaSuccess) {
+                cudaEventRecord(ev_mask, cs) != cudaSuccess) {
                 st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: mask copy");
                 break;
             }
         }
+        // the next tile's counting kernel goes ahead of this tile's density
+        if (k_out + 1 < todo.size()) {
+            if ((st = count_of(k_out + 1))) break;
+            if (cudaEventRecord(counted, c->stream) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
+        }
+        if (mask_src && cudaStreamWaitEvent(c->stream, ev_mask, 0) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
         // d_out[b] was last copied out two tiles ago: the copy stream's order covers it
         if (k_out >= 2 && cudaStreamWaitEvent(c->stream, slots[(k_out - 2) % 3].copied, 0) != cudaSuccess) {
             st = MGK_ERR_CUDA;
             break;
         }
-        if ((st = mgk_launch_density(c, idx, g, r0, c0, nr, nc, mask_src ? d_mask : nullptr, d_out[b], d_ev, false)))
-            break;
+        if ((st = mgk_density_launch_plan(c, plans[b], c->stream))) break;
         if (cudaEventRecord(ev_den[b], c->stream) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
         if (direct) {
             if (cudaStreamWaitEvent(cs, ev_den[b], 0) != cudaSuccess ||
@@ -172,34 +218,36 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
                 st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: result copy");
                 break;
             }
-            k_out++;
-            continue;
+        } else {
+            // a free host slot (the writer may still hold the one used three tiles ago)
+            Slot* sl = &slots[k_out % 3];
+            {
+                std::unique_lock<std::mutex> lk(W.mu);
+                W.cv.wait(lk, [&] { return !sl->busy || W.status != MGK_OK; });
+                if (W.status) { st = W.status; break; }
+            }
+            sl->tile = t;
+            sl->r0 = r0;
+            sl->c0 = c0;
+            sl->nr = nr;
+            sl->nc = nc;
+            if (cudaStreamWaitEvent(cs, ev_den[b], 0) != cudaSuccess ||
+                cudaMemcpyAsync(sl->host, d_out[b], sizeof(float) * nr * nc, cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
+                cudaEventRecord(sl->copied, cs) != cudaSuccess) {
+                st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: result copy");
+                break;
+            }
+            {
+                std::lock_guard<std::mutex> lk(W.mu);
+                sl->busy = true;
+                W.q.push_back(sl);
+            }
+            W.cv.notify_all();
         }
-        // a free host slot (the writer may still hold the one used three tiles ago)
-        Slot* s = &slots[k_out % 3];
-        {
-            std::unique_lock<std::mutex> lk(W.mu);
-            W.cv.wait(lk, [&] { return !s->busy || W.status != MGK_OK; });
-            if (W.status) { st = W.status; break; }
+        if (k_out + 1 < todo.size()) {
+            if (cudaEventSynchronize(counted) != cudaSuccess) { st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: plan"); break; }
+            st = plan_of(k_out + 1);
         }
-        s->tile = t;
-        s->r0 = r0;
-        s->c0 = c0;
-        s->nr = nr;
-        s->nc = nc;
-        if (cudaStreamWaitEvent(cs, ev_den[b], 0) != cudaSuccess ||
-            cudaMemcpyAsync(s->host, d_out[b], sizeof(float) * nr * nc, cudaMemcpyDeviceToHost, cs) != cudaSuccess ||
-            cudaEventRecord(s->copied, cs) != cudaSuccess) {
-            st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: result copy");
-            break;
-        }
-        {
-            std::lock_guard<std::mutex> lk(W.mu);
-            s->busy = true;
-            W.q.push_back(s);
-        }
-        W.cv.notify_all();
-        k_out++;
     }
     if (wt.joinable()) {
         {
@@ -213,6 +261,13 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
     }
     cudaStreamSynchronize(c->stream);
     cudaStreamSynchronize(cs);
+    for (int i = 0; i < 2; i++) mgk_density_discard(c, plans[i]);  // every kernel has ended
+    if (counted) cudaEventDestroy(counted);
+    if (st == MGK_OK) {
+        unsigned long long flag = 0;
+        if (cudaMemcpy(&flag, c->d_counter + 7, sizeof(flag), cudaMemcpyDeviceToHost) != cudaSuccess) st = MGK_ERR_CUDA;
+        else if (flag) st = mgk_fail(c, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    }
     if (st == MGK_OK && evals) {
         unsigned long long v = 0;
         if (cudaMemcpy(&v, d_ev, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) st = MGK_ERR_CUDA;
