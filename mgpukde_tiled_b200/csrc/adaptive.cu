@@ -29,6 +29,7 @@
 #include <cfloat>
 #include <climits>
 #include <cmath>
+#include <cstring>
 
 #include "mgk_internal.cuh"
 
@@ -302,31 +303,82 @@ int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den, do
     return MGK_OK;
 }
 
-// Steps 1-3: e(h), the pilot density with self, and hs into p->h.
-int pilot_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* d_den,
-                     double* d_scal) {
+// Pilot densities by bandwidth.  The search evaluates the likelihood at
+// (h, alpha) pairs that share h (the centre and its two alpha neighbours),
+// and the pilot density with its log sum (steps 1-3 up to the geometric
+// mean) depends on h alone, so it is kept for the last few h.
+struct PilotCache {
+    static constexpr int kEntries = 6;
+    mgk_ctx* c = nullptr;
+    int64_t n = 0;
+    uint32_t hbits[kEntries] = {};
+    double* buf[kEntries] = {};  // den0[max(n, 1)], then the log sum
+    uint64_t last[kEntries] = {};
+    uint64_t tick = 0;
+    size_t bytes() const { return sizeof(double) * (size_t)(std::max<int64_t>(n, 1) + 1); }
+    ~PilotCache() {
+        for (int i = 0; i < kEntries; i++)
+            if (buf[i]) mgk_free(c, buf[i], bytes());
+    }
+};
+
+// Steps 1-3 up to the geometric mean for bandwidth h: den0 (input order) and
+// its log sum, computed or taken from the cache.
+int pilot_density(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, PilotCache& pc, double** den0) {
+    uint32_t hb;
+    memcpy(&hb, &h, sizeof(hb));
+    int slot = -1;
+    for (int i = 0; i < PilotCache::kEntries; i++)
+        if (pc.buf[i] && pc.hbits[i] == hb) slot = i;
+    if (slot >= 0) {
+        pc.last[slot] = ++pc.tick;
+        *den0 = pc.buf[slot];
+        return MGK_OK;
+    }
+    for (int i = 0; i < PilotCache::kEntries; i++)  // a free entry, else the least recently used
+        if (slot < 0 || !pc.buf[i] || (pc.buf[slot] && pc.last[i] < pc.last[slot])) slot = i;
     int st;
+    if (!pc.buf[slot] && (st = mgk_alloc(c, (void**)&pc.buf[slot], pc.bytes()))) return st;
+    pc.hbits[slot] = hb;
+    pc.last[slot] = ++pc.tick;
+    double* den = pc.buf[slot];
     if (r) st = mgk_launch_edge_weights(c, p->n, p->x, p->y, nullptr, h, p->dist2, r, p->ew, edge_count(c));
     else st = mgk_edge_weights_unit(c, p);
-    if (st) return st;
-    p->has_ew = true;
-    mgk_index* idx = nullptr;
-    if ((st = mgk_index_build(c, p, h, 0.0f, &idx))) return st;  // h > 0: fixed-h index
-    st = point_density(c, idx, true, d_den, 0.0, d_scal);
+    if (st == MGK_OK) {
+        p->has_ew = true;
+        mgk_index* idx = nullptr;
+        if ((st = mgk_index_build(c, p, h, 0.0f, &idx)) == MGK_OK) {  // h > 0: fixed-h index
+            st = point_density(c, idx, true, den, 0.0, den + std::max<int64_t>(p->n, 1));
+            mgk_index_destroy(idx);
+        }
+    }
+    if (st) {
+        pc.hbits[slot] = 0;  // not a valid entry
+        mgk_free(c, pc.buf[slot], pc.bytes());
+        pc.buf[slot] = nullptr;
+        return st;
+    }
+    *den0 = den;
+    return MGK_OK;
+}
+
+// Steps 1-3: the pilot density at h and hs = h (den0 / gml)^alpha into p->h.
+int pilot_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, PilotCache& pc) {
+    double* den0 = nullptr;
+    int st = pilot_density(c, p, r, h, pc, &den0);
     if (st == MGK_OK && p->n > 0) {
-        k_adaptive_h<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->n, d_den, d_scal, h, alpha, p->h);
+        k_adaptive_h<<<(unsigned)((p->n + 255) / 256), 256, 0, c->stream>>>(p->n, den0, den0 + p->n, h, alpha, p->h);
         MGK_COUNT_LAUNCH(c, 1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) st = mgk_cuda_fail(c, e, "adaptive bandwidths");
     }
-    mgk_index_destroy(idx);
     return st;
 }
 
 // LogLikelihood(h, alpha): steps 1-6.
 int loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* d_den,
-                    double* d_scal, double* logl) {
-    int st = pilot_bandwidths(c, p, r, h, alpha, d_den, d_scal);
+                    double* d_scal, double* logl, PilotCache& pc) {
+    int st = pilot_bandwidths(c, p, r, h, alpha, pc);
     if (st) return st;
     if (r && (st = mgk_launch_edge_weights(c, p->n, p->x, p->y, p->h, 0.0f, p->dist2, r, p->ew, edge_count(c))))
         return st;
@@ -371,9 +423,14 @@ int mgk_loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h,
         mgk_free(c, d_den, bd);
         return st;
     }
-    st = count_begin(c);
-    if (st == MGK_OK) st = loglik_adaptive(c, p, r, h, alpha, d_den, d_scal, logl);
-    if (st == MGK_OK) st = count_end(c);
+    {
+        PilotCache pc;
+        pc.c = c;
+        pc.n = p->n;
+        st = count_begin(c);
+        if (st == MGK_OK) st = loglik_adaptive(c, p, r, h, alpha, d_den, d_scal, logl, pc);
+        if (st == MGK_OK) st = count_end(c);
+    }
     mgk_free(c, d_den, bd);
     mgk_free(c, d_scal, 2 * sizeof(double));
     return st;
@@ -399,9 +456,12 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
     // the likelihoods are kept as floats, the type of the reference's Ls array,
     // so that ties and near-ties compare as they do there
     float L[5] = {0, 0, 0, 0, 0};
+    PilotCache pc;
+    pc.c = c;
+    pc.n = p->n;
     auto ll = [&](float h, float a, float* out) {
         double v = 0.0;
-        const int s1 = loglik_adaptive(c, p, r, h, a, d_den, d_scal, &v);
+        const int s1 = loglik_adaptive(c, p, r, h, a, d_den, d_scal, &v, pc);
         *out = (float)v;
         return s1;
     };
@@ -458,7 +518,7 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
         it++;
     }
     // final bandwidths at the optimum (main :566-572)
-    if (st == MGK_OK) st = pilot_bandwidths(c, p, r, h0, alpha0, d_den, d_scal);
+    if (st == MGK_OK) st = pilot_bandwidths(c, p, r, h0, alpha0, pc);
     if (st == MGK_OK && hs_out && p->n > 0) {
         const cudaError_t e = cudaMemcpyAsync(hs_out, p->h, sizeof(float) * (size_t)p->n, cudaMemcpyDeviceToHost,
                                               c->stream);
