@@ -10,7 +10,10 @@
 //    requests is below the slot count and its estimated device footprint fits
 //    beside the active ones inside the budget;
 //  * preparation: its points, index (and edge-correction weights) are built
-//    and stay resident on the device while it is active;
+//    and stay resident on the device while it is active.  A second thread
+//    with a context of its own does this (admission, preparation, and the
+//    release of finished requests' memory), so new requests are prepared on
+//    the GPU while the worker's ticks run;
 //  * ticks: each tick takes the next tile of every active request (row-major
 //    tiles of tile_side x tile_side cells) and runs all of them in one density
 //    launch (mgk_launch_density_jobs).  Each request has two device output
@@ -76,17 +79,35 @@ struct Job {
 
 }  // namespace
 
+namespace {
+// The device resources of a request, handed to the preparation thread (whose
+// context allocated them) for release once the request has finished.
+struct Res {
+    mgk_points* p = nullptr;
+    mgk_raster* em = nullptr;
+    mgk_index* idx = nullptr;
+    float* d_mask = nullptr;
+    float* d_out[2] = {nullptr, nullptr};
+    cudaEvent_t out_free[2] = {nullptr, nullptr};
+    size_t tile_bytes = 0;
+};
+}  // namespace
+
 struct mgk_server {
-    mgk_ctx* ctx = nullptr;
+    mgk_ctx* ctx = nullptr;   // the worker's: ticks and copies
+    mgk_ctx* pctx = nullptr;  // the preparation thread's: requests' points, indexes and tiles
     int64_t tile = 2048;
     int max_active = 8;
     uint64_t budget = 0;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_prep;
     std::deque<Job*> queue;
     std::map<uint64_t, Job*> jobs;  // every job until its result is collected
+    int preparing = 0;           // admitted, being prepared
     std::vector<Job*> active;    // tiles left to compute
     std::vector<Job*> draining;  // every tile computed, the last copies in flight
+    std::vector<Res> to_release;
+    std::thread prep;
     cudaStream_t d2h = nullptr;  // copies of finished tiles to the host
     unsigned long long* h_ev = nullptr;  // per-tick eval counts, mapped page-locked
     unsigned long long* d_ev_map = nullptr;  // their device address
@@ -117,27 +138,43 @@ uint64_t estimate_bytes(const mgk_request& r, int64_t tile) {
     return b + b / 4 + (16u << 20);
 }
 
-void release(mgk_server* S, Job* J) {
-    mgk_ctx* c = S->ctx;
-    mgk_index_destroy(J->idx);
-    mgk_raster_destroy(J->em);
-    mgk_points_destroy(J->p);
-    mgk_free(c, J->d_mask, J->tile_bytes);
+void release(mgk_ctx* pc, Res& R) {
+    mgk_index_destroy(R.idx);
+    mgk_raster_destroy(R.em);
+    mgk_points_destroy(R.p);
+    mgk_free(pc, R.d_mask, R.tile_bytes);
     for (int b = 0; b < 2; b++) {
-        mgk_free(c, J->d_out[b], J->tile_bytes);
-        if (J->out_free[b]) cudaEventDestroy(J->out_free[b]);
+        mgk_free(pc, R.d_out[b], R.tile_bytes);
+        if (R.out_free[b]) cudaEventDestroy(R.out_free[b]);
+    }
+    R = Res{};
+}
+
+// Moves a request's device resources out of the job.
+Res take(Job* J) {
+    Res R;
+    R.p = J->p;
+    R.em = J->em;
+    R.idx = J->idx;
+    R.d_mask = J->d_mask;
+    R.tile_bytes = J->tile_bytes;
+    for (int b = 0; b < 2; b++) {
+        R.d_out[b] = J->d_out[b];
+        R.out_free[b] = J->out_free[b];
         J->d_out[b] = nullptr;
         J->out_free[b] = nullptr;
     }
-    J->idx = nullptr;
-    J->em = nullptr;
     J->p = nullptr;
+    J->em = nullptr;
+    J->idx = nullptr;
     J->d_mask = nullptr;
+    return R;
 }
 
-// Uploads and indexes a newly admitted request (worker thread).
+// Uploads and indexes a newly admitted request (preparation thread, its own
+// context and stream); returns once the device holds all of it.
 int prepare(mgk_server* S, Job* J) {
-    mgk_ctx* c = S->ctx;
+    mgk_ctx* c = S->pctx;
     const mgk_request& r = J->req;
     int st = mgk_points_upload(c, r.n, r.x, r.y, r.w, nullptr, &J->p);
     if (st) return st;
@@ -163,12 +200,18 @@ int prepare(mgk_server* S, Job* J) {
     }
     if (r.mask && (st = mgk_alloc(c, (void**)&J->d_mask, J->tile_bytes))) return st;
     J->next_tile = 0;
+    const cudaError_t e = cudaStreamSynchronize(c->stream);  // the worker's stream reads all of it
+    if (e != cudaSuccess) return mgk_cuda_fail(c, e, "serve: preparation");
     return MGK_OK;
 }
 
+// A request is done: its device memory goes to the preparation thread for
+// release, and its waiters are told.
 void finish(mgk_server* S, Job* J, int status) {
-    release(S, J);
+    Res R = take(J);
     std::lock_guard<std::mutex> lk(S->mu);
+    S->to_release.push_back(R);
+    S->cv_prep.notify_one();
     J->status = status;
     J->state = 2;
     J->t_done = Clock::now();
@@ -291,52 +334,80 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
     }
 }
 
+// The worker: ticks over the prepared requests and completes those whose
+// last copy has landed.
 void worker_main(mgk_server* S) {
     cudaSetDevice(S->ctx->device);
-    std::vector<Job*> fresh;
     for (;;) {
-        fresh.clear();
         reap(S, false);
+        std::vector<Job*> act;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            if (S->active.empty() && S->queue.empty()) {
+            if (S->active.empty()) {
                 if (!S->draining.empty()) {
                     lk.unlock();
                     reap(S, true);  // nothing to compute: wait for the last copies
                     continue;
                 }
-                if (S->stop) return;
+                if (S->stop && S->queue.empty() && S->preparing == 0) return;
                 S->cv_work.wait_for(lk, std::chrono::milliseconds(50));
                 continue;
             }
-            // admission: slots and the HBM budget; a request that fits nowhere
-            // alone is still admitted when nothing else is active
-            while (!S->queue.empty() && (int)(S->active.size() + S->draining.size()) < S->max_active) {
+            act = S->active;
+        }
+        tick(S, act);
+    }
+}
+
+// The preparation thread: releases finished requests' memory, admits queued
+// requests by free slots and the HBM budget (a request that fits nowhere
+// alone is admitted when nothing else is in the server), prepares them, and
+// hands them to the worker.
+void prep_main(mgk_server* S) {
+    cudaSetDevice(S->pctx->device);
+    for (;;) {
+        std::vector<Res> rel;
+        std::vector<Job*> fresh;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            auto admissible = [&] {
+                if (S->queue.empty()) return false;
+                const int held = (int)(S->active.size() + S->draining.size()) + S->preparing;
+                if (held >= S->max_active) return false;
+                return held == 0 || S->reserved + S->queue.front()->est <= S->budget;
+            };
+            auto idle = [&] {
+                return S->stop && S->queue.empty() && S->preparing == 0 && S->active.empty() &&
+                       S->draining.empty() && S->to_release.empty();
+            };
+            if (S->to_release.empty() && !admissible()) {
+                if (idle()) return;
+                S->cv_prep.wait_for(lk, std::chrono::milliseconds(50));
+            }
+            rel.swap(S->to_release);
+            while (admissible()) {
                 Job* J = S->queue.front();
-                if ((!S->active.empty() || !S->draining.empty()) && S->reserved + J->est > S->budget) break;
                 S->queue.pop_front();
                 J->state = 1;
                 J->t_start = Clock::now();
                 S->reserved += J->est;
-                S->active.push_back(J);
+                S->preparing++;
                 fresh.push_back(J);
             }
         }
-        // preparation reads small results back to the host; those copies
-        // would queue behind the tile copies still in flight on the copy
-        // engine, so let them land first
-        if (!fresh.empty()) cudaStreamSynchronize(S->d2h);
+        for (Res& R : rel) release(S->pctx, R);
         for (Job* J : fresh) {
             const int st = prepare(S, J);
+            {
+                std::lock_guard<std::mutex> lk(S->mu);
+                S->preparing--;
+                if (st == MGK_OK) {
+                    S->active.push_back(J);
+                    S->cv_work.notify_one();
+                }
+            }
             if (st) finish(S, J, st);
         }
-        std::vector<Job*> act;
-        {
-            std::lock_guard<std::mutex> lk(S->mu);
-            act = S->active;
-        }
-        if (!act.empty()) tick(S, act);
-        else reap(S, true);  // slots held by draining requests: wait for their copies instead of spinning
     }
 }
 
@@ -347,15 +418,21 @@ extern "C" {
 int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, int max_active, mgk_server** out) {
     if (!out || max_active <= 0 || tile_side < 64) return MGK_ERR_INVALID;
     *out = nullptr;
-    mgk_ctx* c = nullptr;
+    mgk_ctx *c = nullptr, *pc = nullptr;
     int st = mgk_ctx_create(device, hbm_budget_bytes, &c);
     if (st) return st;
+    if ((st = mgk_ctx_create(device, hbm_budget_bytes, &pc))) {
+        mgk_ctx_destroy(c);
+        return st;
+    }
     mgk_server* S = new (std::nothrow) mgk_server();
     if (!S) {
+        mgk_ctx_destroy(pc);
         mgk_ctx_destroy(c);
         return MGK_ERR_INVALID;
     }
     S->ctx = c;
+    S->pctx = pc;
     S->tile = tile_side;
     S->max_active = max_active;
     S->budget = c->budget;
@@ -366,11 +443,13 @@ int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, i
         cudaHostGetDevicePointer((void**)&S->d_ev_map, S->h_ev, 0) != cudaSuccess) {
         if (S->h_ev) cudaFreeHost(S->h_ev);
         if (S->d2h) cudaStreamDestroy(S->d2h);
+        mgk_ctx_destroy(pc);
         mgk_ctx_destroy(c);
         delete S;
         return MGK_ERR_CUDA;
     }
     S->worker = std::thread(worker_main, S);
+    S->prep = std::thread(prep_main, S);
     *out = S;
     return MGK_OK;
 }
@@ -394,7 +473,7 @@ int mgk_serve_submit(mgk_server* S, const mgk_request* r, uint64_t* ticket) {
     S->jobs[J->id] = J;
     S->queue.push_back(J);
     *ticket = J->id;
-    S->cv_work.notify_one();
+    S->cv_prep.notify_one();
     return MGK_OK;
 }
 
@@ -446,9 +525,9 @@ int mgk_serve_stats(mgk_server* S, mgk_serve_info* out) {
     out->max_batch = S->max_batch;
     out->completed = S->completed;
     out->queued = S->queue.size();
-    out->active = S->active.size() + S->draining.size();
+    out->active = S->active.size() + S->draining.size() + (uint64_t)S->preparing;
     out->reserved_bytes = S->reserved;
-    out->device_bytes = S->ctx->in_use;
+    out->device_bytes = S->ctx->in_use + S->pctx->in_use;
     return MGK_OK;
 }
 
@@ -458,11 +537,15 @@ int mgk_serve_destroy(mgk_server* S) {
         std::lock_guard<std::mutex> lk(S->mu);
         S->stop = true;
         S->cv_work.notify_all();
+        S->cv_prep.notify_all();
     }
-    if (S->worker.joinable()) S->worker.join();  // finishes queued and active requests first
+    // both threads finish the queued and active requests first
+    if (S->worker.joinable()) S->worker.join();
+    if (S->prep.joinable()) S->prep.join();
     for (auto& kv : S->jobs) delete kv.second;
     cudaStreamDestroy(S->d2h);
     cudaFreeHost(S->h_ev);
+    mgk_ctx_destroy(S->pctx);
     mgk_ctx_destroy(S->ctx);
     delete S;
     return MGK_OK;
