@@ -363,9 +363,9 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     __shared__ unsigned char procmask[kMB];  // warp w processes the point
     __shared__ unsigned char fullmask[kMB];  // every cell of warp w's sub-block is inside the cutoff
     __shared__ float s_cxh[kBC], s_cxl[kBC], s_cxg[kBC], s_cyh[kBR], s_cyl[kBR], s_cyg[kBR];
-    __shared__ int s_abort;
-    __shared__ BatchCur s_cur[kNCur];  // the item's candidate cursors (thread 0)
+    __shared__ BatchCur s_cur[kNCur];  // the item's candidate cursors
     __shared__ int s_nm;               // size of the batch being staged
+    __shared__ int s_load[2][8];       // per batch buffer: points warp w sums (phase B)
 
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -391,8 +391,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         mbar_init(&mbar[0], 1);
         mbar_init(&mbar[1], 1);
         fence_mbar_init();
-        s_abort = 0;
     }
+    if (tid < 16) s_load[tid >> 3][tid & 7] = 0;
 #pragma unroll
     for (int q4 = 0; q4 < 8; q4++) {
         ksum[q4 * kThreads + tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -435,27 +435,16 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     int m = s_nm;
     unsigned phase0 = 0, phase1 = 0;
     int buf = 0;
-    // outstanding copies at an abort: (buffer, parity) pairs to drain
-    int drain_n = 0, drain_b[2] = {0, 0};
-    unsigned drain_p[2] = {0, 0};
+    // Two block barriers per batch: after the factor tables (which also
+    // shares a staging wait that ran out) and after the sums.  The next
+    // batch is staged during the sums, by the warp with the fewest points to
+    // sum, so the serial fill is off the critical path.
+    bool aborted = false;
+    unsigned abort_par = 0;
     while (m > 0) {
-        if (tid == 0) s_nm = fill_batch(P, G, s_cur, &stage[(buf ^ 1) * kMB], &mbar[buf ^ 1]);
         const unsigned par = buf ? phase1 : phase0;
-        if (!mbar_wait(&mbar[buf], par)) {
-            atomicExch(P.err, 1ull);
-            s_abort = 1;
-        }
-        const bool abort_now = __syncthreads_or(s_abort);
-        const int nm = s_nm;  // written before the barrier; rewritten only after the batch's end barrier
-        if (abort_now) {
-            drain_b[drain_n] = buf;
-            drain_p[drain_n++] = par;
-            if (nm > 0) {
-                drain_b[drain_n] = buf ^ 1;
-                drain_p[drain_n++] = buf ? phase0 : phase1;
-            }
-            break;
-        }
+        const bool ok = mbar_wait(&mbar[buf], par);  // every thread; bounded
+        if (!ok) atomicExch(P.err, 1ull);
         if (buf) phase1 ^= 1u;
         else phase0 ^= 1u;
         const MgkPt* st = stage + buf * kMB;
@@ -464,7 +453,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         {
             bool proc = false, full = false;
             unsigned lo32 = 0, hi32 = 0, lo32h = 0, hi32h = 0;
-            if (qa < m) {
+            if (ok && qa < m) {
                 const MgkPt r = st[qa];
                 float k2h, k2l, cutf, epsd2;
                 if (VARH) {
@@ -534,6 +523,11 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             }
             const unsigned bal = __ballot_sync(0xffffffffu, proc);
             const unsigned balf = __ballot_sync(0xffffffffu, full);
+            if (lane < 8) {
+                // this warp's points (4) that sub-block warp `lane` sums
+                const int nl = __popc(bal & (0x01010101u << lane));
+                if (nl) atomicAdd(&s_load[buf][lane], nl);
+            }
             if (ka == 0) {
                 rowflag[qa][0] = ((unsigned long long)hi32 << 32) | lo32;
                 rowflag[qa][1] = ((unsigned long long)hi32h << 32) | lo32h;
@@ -541,10 +535,31 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 fullmask[qa] = (unsigned char)((balf >> (8 * (qa & 3))) & 0xffu);
             }
         }
-        __syncthreads();
+        if (__syncthreads_or(!ok)) {
+            // a staging wait ran out: the batch's copy is the only one in flight
+            aborted = true;
+            abort_par = par;
+            break;
+        }
 
         // ---------------- phase B ----------------
         {
+            // stage the next batch: the warp with the fewest points to sum
+            // (lowest index on ties) fills; the buffer's last readers were
+            // the previous batch's sums, before that batch's end barrier
+            int filler = 0, least = s_load[buf][0];
+#pragma unroll
+            for (int w = 1; w < 8; w++)
+                if (s_load[buf][w] < least) {
+                    least = s_load[buf][w];
+                    filler = w;
+                }
+            if (warp == filler && lane == 0) s_nm = fill_batch(P, G, s_cur, &stage[(buf ^ 1) * kMB], &mbar[buf ^ 1]);
+            if (tid == 32 * ((filler + 1) & 7)) {
+                // the other buffer's counts were last read before the previous end barrier
+#pragma unroll
+                for (int w = 0; w < 8; w++) s_load[buf ^ 1][w] = 0;
+            }
             // this warp's processed, fully-inside and flagged points of the batch as bit masks
             const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
             const bool lv = lane < m;
@@ -632,15 +647,14 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 }
             }
         }
-        __syncthreads();  // factor tables and stage[buf] are reused next
-        m = nm;
+        __syncthreads();  // factor tables, s_nm and stage[buf] are reused next
+        m = s_nm;
         buf ^= 1;
     }
-    if (drain_n) {
-        // a staging wait ran out: give the outstanding copies a second bounded
-        // wait before the CTA (and its shared memory) goes away
-        if (tid == 0)
-            for (int d = 0; d < drain_n; d++) mbar_wait(&mbar[drain_b[d]], drain_p[d]);
+    if (aborted) {
+        // give the outstanding copy a second bounded wait before the CTA (and
+        // its shared memory) goes away
+        if (tid == 0) mbar_wait(&mbar[buf], abort_par);
         __syncthreads();
         return;
     }
