@@ -266,7 +266,10 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
 // bin rows spread over the candidate window.  Points from one bin row all
 // touch the same warp rows of the block; mixing rows keeps the eight warps'
 // phase-B work per batch even and shortens the waits at the batch barriers.
-constexpr int kNCur = 2;
+#ifndef MGK_DENSITY_NCUR
+#define MGK_DENSITY_NCUR 4
+#endif
+constexpr int kNCur = MGK_DENSITY_NCUR;
 struct BatchCur {
     long long by, seq, pos, end;  // bin row, its offset in the block's sequence, next and end candidate
     long long sb, len;            // the current row's range of the index
