@@ -50,7 +50,7 @@ constexpr int kThreads = 256;
 constexpr int kBR = 64;         // cell rows of a CTA block
 constexpr int kBC = 128;        // cell columns of a CTA block
 constexpr int kCells = kBR * kBC;
-constexpr int kMB = 32;         // points per mini-batch
+constexpr int kMB = 64;         // points per mini-batch (a multiple of 32)
 constexpr int kStage64 = 512;   // points staged per batch by the FP64 form
 constexpr float kAmbEps = 4e-6f;
 constexpr long long kSpinLimit = 1ll << 24;
@@ -197,6 +197,48 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* b, unsigned parity) {
     return false;
 }
 
+// ---- tensor memory (sm_100a tcgen05) ---------------------------------------
+// The per-cell Kahan accumulators of a block live in tensor memory.  A warp
+// may address only its quarter of the 128 TMEM lanes (warp w: lanes
+// 32 (w % 4) ..); with the 32x32b shape thread t of the warp reads and writes
+// lane 32 (w % 4) + t, one 32-bit column per register.  TMEM addresses carry
+// the lane in bits 31:16 and the column in bits 15:0.
+constexpr unsigned kTmemCols = 128;  // warps w and w + 4 share lanes: columns 64 (w / 4) .. + 64
+
+__device__ __forceinline__ void tmem_alloc(unsigned* dst) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(dst)),
+                 "r"(kTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(unsigned taddr) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(kTmemCols) : "memory");
+}
+__device__ __forceinline__ void tmem_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Columns taddr .. taddr + 7 of the thread's lane into v (valid on return:
+// the wait names the registers, so no use of them moves above it).
+__device__ __forceinline__ void tmem_ld8(unsigned taddr, float (&v)[8]) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]), "=f"(v[4]), "=f"(v[5]), "=f"(v[6]), "=f"(v[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_ld(float (&a)[8], float (&b)[8]) {
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+f"(a[0]), "+f"(a[1]), "+f"(a[2]), "+f"(a[3]), "+f"(a[4]), "+f"(a[5]), "+f"(a[6]), "+f"(a[7]),
+                   "+f"(b[0]), "+f"(b[1]), "+f"(b[2]), "+f"(b[3]), "+f"(b[4]), "+f"(b[5]), "+f"(b[6]), "+f"(b[7])
+                 :
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_st8(unsigned taddr, const float (&v)[8]) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8};" ::"r"(taddr),
+                 "f"(v[0]), "f"(v[1]), "f"(v[2]), "f"(v[3]), "f"(v[4]), "f"(v[5]), "f"(v[6]), "f"(v[7])
+                 : "memory");
+}
+
 // Exponent a = (t + lo)^2 (k2h + k2l) as a float pair ah + al.  t is exact
 // (difference of two multiples of the quantum), |lo| <= quantum.  dx = t + lo
 // is formed as an exact pair (dh, de) first, so p = dh^2 is the rounded
@@ -267,7 +309,7 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
 // touch the same warp rows of the block; mixing rows keeps the eight warps'
 // phase-B work per batch even and shortens the waits at the batch barriers.
 #ifndef MGK_DENSITY_NCUR
-#define MGK_DENSITY_NCUR 4
+#define MGK_DENSITY_NCUR 2
 #endif
 constexpr int kNCur = MGK_DENSITY_NCUR;
 struct BatchCur {
@@ -328,17 +370,16 @@ __device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, 
     return m;
 }
 
-// Dynamic shared memory of k_density (bytes): the staged points, the factor
-// tables (row strides of 136 and 72 floats, both 8 mod 32, so that the
-// phase-A stores of 4 points hit distinct banks) and the per-cell Kahan
-// accumulators (sum and compensation, 8192 floats each).
+// Dynamic shared memory of k_density (bytes): the staged points and the
+// factor tables (row strides of 136 and 72 floats, both 8 mod 32, so that the
+// phase-A stores of 4 points hit distinct banks).  The per-cell Kahan
+// accumulators are in tensor memory.
 constexpr int kFStrideC = 136;  // column table, floats per point
 constexpr int kFStride = 72;    // row tables, floats per point
 constexpr size_t kSmemStage = 2 * kMB * sizeof(MgkPt);
 constexpr size_t kSmemColTab = (size_t)kMB * kFStrideC * sizeof(float);
 constexpr size_t kSmemRowTab = (size_t)kMB * kFStride * sizeof(float);
-constexpr size_t kSmemKahan = (size_t)kCells * sizeof(float);
-constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab + 2 * kSmemKahan;
+constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab;
 
 #ifndef MGK_DENSITY_MIN_CTAS
 #define MGK_DENSITY_MIN_CTAS 2  // resident CTAs per SM (shared memory allows two)
@@ -358,10 +399,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     float* colE = reinterpret_cast<float*>(dsm + kSmemStage);                   // [kMB][kFStrideC] E_j
     float* rowF = reinterpret_cast<float*>(dsm + kSmemStage + kSmemColTab);     // [kMB][kFStride] F_i
     float* rowG = reinterpret_cast<float*>(dsm + kSmemStage + kSmemColTab + kSmemRowTab);  // [kMB][kFStride] G_i
-    // Kahan sum / compensation of the thread's 32 cells: float4 [8][256] each
-    float4* ksum = reinterpret_cast<float4*>(dsm + kSmemStage + kSmemColTab + 2 * kSmemRowTab);
-    float4* kcmp = ksum + kCells / 4;
     __shared__ __align__(8) uint64_t mbar[2];
+    __shared__ unsigned s_tmem;  // TMEM base of the block's Kahan accumulators
     __shared__ __align__(16) unsigned long long rowflag[kMB][2];  // per column half: 64 row bits
     __shared__ unsigned char procmask[kMB];  // warp w processes the point
     __shared__ unsigned char fullmask[kMB];  // every cell of warp w's sub-block is inside the cutoff
@@ -396,12 +435,23 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         fence_mbar_init();
     }
     if (tid < 16) s_load[tid >> 3][tid & 7] = 0;
-#pragma unroll
-    for (int q4 = 0; q4 < 8; q4++) {
-        ksum[q4 * kThreads + tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        kcmp[q4 * kThreads + tid] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    }
+    __syncwarp();
+    if (warp == 0) tmem_alloc(&s_tmem);
+    tmem_fence_before();
     regular = __syncthreads_and(regular);
+    tmem_fence_after();
+    // Kahan sum and compensation of the thread's 32 cells (cell k = i * 8 + j
+    // at column k of tS and of tC)
+    const unsigned tS = s_tmem + ((32u * (unsigned)(warp & 3)) << 16) + 64u * (unsigned)(warp >> 2);
+    const unsigned tC = tS + 32u;
+    {
+        const float z[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+            tmem_st8(tS + 8u * c, z);
+            tmem_st8(tC + 8u * c, z);
+        }
+    }
     const float inv_cs = 1.0f / (float)P.cs;
 
     // validity of the lane's 32 cells (inside the tile and not NoData); bit i*8+j
@@ -453,36 +503,72 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         const MgkPt* st = stage + buf * kMB;
 
         // ---------------- phase A ----------------
-        {
+        // thread (qa, ka) builds part ka of the tables of points qa, qa + 32
+#pragma unroll 1
+        for (int hq = 0; hq < kMB / 32; hq++) {
+            const int pq = qa + 32 * hq;
+            const bool act = ok && pq < m;
             bool proc = false, full = false;
             unsigned lo32 = 0, hi32 = 0, lo32h = 0, hi32h = 0;
-            if (ok && qa < m) {
-                const MgkPt r = st[qa];
-                float k2h, k2l, cutf, epsd2;
-                if (VARH) {
-                    k2h = r.k2h;
-                    k2l = r.k2l;
-                    cutf = 9.0f * r.hh;
-                    epsd2 = r.hh * (4.0f * kAmbEps / (float)MGK_LOG2E);
-                } else {
-                    k2h = P.k2h;
-                    k2l = P.k2l;
-                    cutf = P.cutf;
-                    epsd2 = P.epsd2;
-                }
-                float* cE = colE + qa * kFStrideC;
-                float* rF = rowF + qa * kFStride;
-                float* rG = rowG + qa * kFStride;
+            const MgkPt r = st[act ? pq : 0];
+            float k2h, k2l, cutf, epsd2;
+            if (VARH) {
+                k2h = r.k2h;
+                k2l = r.k2l;
+                cutf = 9.0f * r.hh;
+                epsd2 = r.hh * (4.0f * kAmbEps / (float)MGK_LOG2E);
+            } else {
+                k2h = P.k2h;
+                k2l = P.k2l;
+                cutf = P.cutf;
+                epsd2 = P.epsd2;
+            }
+            if (act && sk_on) {
+                // distance from the point to the sub-block rectangle of cell centres
+                const float dxl = __fadd_rn(__fsub_rn(s_cxh[sk_c0], r.xh), __fsub_rn(s_cxl[sk_c0], r.xl));
+                const float dxr = __fadd_rn(__fsub_rn(r.xh, s_cxh[sk_c1]), __fsub_rn(r.xl, s_cxl[sk_c1]));
+                const float dyt = __fadd_rn(__fsub_rn(r.yh, s_cyh[sk_r0]), __fsub_rn(r.yl, s_cyl[sk_r0]));
+                const float dyb = __fadd_rn(__fsub_rn(s_cyh[sk_r1], r.yh), __fsub_rn(s_cyl[sk_r1], r.yl));
+                const float ddx = fmaxf(0.0f, fmaxf(dxl, dxr));
+                const float ddy = fmaxf(0.0f, fmaxf(dyt, dyb));
+                proc = ddx * ddx + ddy * ddy < cutf * 1.0001f;
+                // farthest corner well inside the cutoff: no cell of the sub-block needs the test
+                const float fx = fmaxf(fabsf(dxl), fabsf(dxr)), fy = fmaxf(fabsf(dyt), fabsf(dyb));
+                full = fx * fx + fy * fy < cutf * 0.9999f;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, proc);
+            const unsigned balf = __ballot_sync(0xffffffffu, full);
+            // the sub-blocks that sum point pq: bit k is sub-block (k >> 1, k & 1).
+            // Only their column halves and rows of the tables are built; the
+            // other entries are never read (the warps that would read them skip
+            // the point)
+            const unsigned pb = (bal >> (8 * (qa & 3))) & 0xffu;
+            if (pb) {
+                float* cE = colE + pq * kFStrideC;
+                float* rF = rowF + pq * kFStride;
+                float* rG = rowG + pq * kFStride;
+                if (pb & 0x55u) {  // columns 0-63, read by the warps of column half 0
 #pragma unroll
-                for (int c = 0; c < 16; c++) {
-                    const int j = ka + 8 * c;
-                    float ah, al, d2;
-                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                    cE[j] = exp2_pair(ah, al);
+                    for (int c = 0; c < 8; c++) {
+                        const int j = ka + 8 * c;
+                        float ah, al, d2;
+                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
+                        cE[j] = exp2_pair(ah, al);
+                    }
+                }
+                if (pb & 0xaau) {  // columns 64-127
+#pragma unroll
+                    for (int c = 8; c < 16; c++) {
+                        const int j = ka + 8 * c;
+                        float ah, al, d2;
+                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
+                        cE[j] = exp2_pair(ah, al);
+                    }
                 }
                 const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
+                    if (!((pb >> (2 * (c >> 1))) & 3u)) continue;  // row ka + 8c lies in warp row c / 2
                     const int i = ka + 8 * c;
                     float bh, bl, d2;
                     exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
@@ -502,21 +588,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                         hi32h |= (a >> 1) << sh;
                     }
                 }
-                if (sk_on) {
-                    // distance from the point to the sub-block rectangle of cell centres
-                    const float dxl = __fadd_rn(__fsub_rn(s_cxh[sk_c0], r.xh), __fsub_rn(s_cxl[sk_c0], r.xl));
-                    const float dxr = __fadd_rn(__fsub_rn(r.xh, s_cxh[sk_c1]), __fsub_rn(r.xl, s_cxl[sk_c1]));
-                    const float dyt = __fadd_rn(__fsub_rn(r.yh, s_cyh[sk_r0]), __fsub_rn(r.yl, s_cyl[sk_r0]));
-                    const float dyb = __fadd_rn(__fsub_rn(s_cyh[sk_r1], r.yh), __fsub_rn(s_cyl[sk_r1], r.yl));
-                    const float ddx = fmaxf(0.0f, fmaxf(dxl, dxr));
-                    const float ddy = fmaxf(0.0f, fmaxf(dyt, dyb));
-                    proc = ddx * ddx + ddy * ddy < cutf * 1.0001f;
-                    // farthest corner well inside the cutoff: no cell of the sub-block needs the test
-                    const float fx = fmaxf(fabsf(dxl), fabsf(dxr)), fy = fmaxf(fabsf(dyt), fabsf(dyb));
-                    full = fx * fx + fy * fy < cutf * 0.9999f;
-                }
             }
-            // the row flags of point qa come from its 8 threads (same warp)
+            // the row flags of point pq come from its 8 threads (same warp)
 #pragma unroll
             for (int o = 1; o < 8; o <<= 1) {
                 lo32 |= __shfl_xor_sync(0xffffffffu, lo32, o);
@@ -524,18 +597,16 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 lo32h |= __shfl_xor_sync(0xffffffffu, lo32h, o);
                 hi32h |= __shfl_xor_sync(0xffffffffu, hi32h, o);
             }
-            const unsigned bal = __ballot_sync(0xffffffffu, proc);
-            const unsigned balf = __ballot_sync(0xffffffffu, full);
             if (lane < 8) {
                 // this warp's points (4) that sub-block warp `lane` sums
                 const int nl = __popc(bal & (0x01010101u << lane));
                 if (nl) atomicAdd(&s_load[buf][lane], nl);
             }
             if (ka == 0) {
-                rowflag[qa][0] = ((unsigned long long)hi32 << 32) | lo32;
-                rowflag[qa][1] = ((unsigned long long)hi32h << 32) | lo32h;
-                procmask[qa] = (unsigned char)((bal >> (8 * (qa & 3))) & 0xffu);
-                fullmask[qa] = (unsigned char)((balf >> (8 * (qa & 3))) & 0xffu);
+                rowflag[pq][0] = ((unsigned long long)hi32 << 32) | lo32;
+                rowflag[pq][1] = ((unsigned long long)hi32h << 32) | lo32h;
+                procmask[pq] = (unsigned char)((bal >> (8 * (qa & 3))) & 0xffu);
+                fullmask[pq] = (unsigned char)((balf >> (8 * (qa & 3))) & 0xffu);
             }
         }
         if (__syncthreads_or(!ok)) {
@@ -563,89 +634,99 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
                 for (int w = 0; w < 8; w++) s_load[buf ^ 1][w] = 0;
             }
-            // this warp's processed, fully-inside and flagged points of the batch as bit masks
-            const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
-            const bool lv = lane < m;
-            const bool pm = lv && ((procmask[lane] >> warp) & 1u);
-            const bool fm = lv && ((fullmask[lane] >> warp) & 1u);
-            const unsigned myflag = lv ? (unsigned)rf16[lane * 8 + wc * 4 + wr] : 0u;  // 16 rows, point `lane`
-            unsigned todo = __ballot_sync(0xffffffffu, pm);
-            const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
-            const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
-            while (todo) {
-                const int q = __ffs(todo) - 1;
-                todo &= todo - 1u;
-                const float* pE = colE + q * kFStrideC + wc * 64 + tc * 4;
-                const float* pF = rowF + q * kFStride + wr * 16 + tr * 4;
-                const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
-                const float4 f4 = *reinterpret_cast<const float4*>(pF);
-                const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
-                const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
-                if (!COUNT && ((fullb >> q) & 1u)) {
-                    // the whole sub-block is inside the cutoff: one FFMA per cell
-#pragma unroll
-                    for (int i = 0; i < 4; i++)
-#pragma unroll
-                        for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
-                } else {
-                    const float4 g4 = *reinterpret_cast<const float4*>(rowG + q * kFStride + wr * 16 + tr * 4);
-                    const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
-                    unsigned inm = 0;
-                    if (COUNT) {
+            // the batch in halves of 32 points, one lane per point
+#pragma unroll 1
+            for (int hq = 0; hq < kMB / 32; hq++) {
+                // this warp's processed, fully-inside and flagged points of the batch as bit masks
+                const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
+                const int pl = lane + 32 * hq;  // this lane's point of the half
+                const bool lv = pl < m;
+                const bool pm = lv && ((procmask[pl] >> warp) & 1u);
+                const bool fm = lv && ((fullmask[pl] >> warp) & 1u);
+                const unsigned myflag = lv ? (unsigned)rf16[pl * 8 + wc * 4 + wr] : 0u;  // 16 rows, point pl
+                unsigned todo = __ballot_sync(0xffffffffu, pm);
+                const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
+                const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
+                while (todo) {
+                    const int q = __ffs(todo) - 1, qq = q + 32 * hq;
+                    todo &= todo - 1u;
+                    const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
+                    const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
+                    const float4 e4a = *reinterpret_cast<const float4*>(pE);
+                    const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
+                    const float4 f4 = *reinterpret_cast<const float4*>(pF);
+                    const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
+                    const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
+                    if (!COUNT && ((fullb >> q) & 1u)) {
+                        // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
-                            for (int j = 0; j < 8; j++) {
-                                const bool in = rg[i] < ce[j];
-                                if (in) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
-                                inm |= (unsigned)in << (i * 8 + j);
-                            }
+                            for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
                     } else {
+                        const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * 16 + tr * 4);
+                        const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
+                        unsigned inm = 0;
+                        if (COUNT) {
 #pragma unroll
-                        for (int i = 0; i < 4; i++)
-#pragma unroll
-                            for (int j = 0; j < 8; j++) fma_if_less(part[i * 8 + j], rg[i], ce[j], ce[j], rv[i]);
-                    }
-                    if ((ambb >> q) & 1u) {
-                        // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
-                        const unsigned fl = (__shfl_sync(0xffffffffu, myflag, q) >> (tr * 4)) & 0xfu;
-                        if (fl) {
-                            const MgkPt r = st[q];
-                            const float px = r.xh + r.xl, py = r.yh + r.yl;
-                            const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
-#pragma unroll
-                            for (int i = 0; i < 4; i++) {
-                                if (!((fl >> i) & 1u)) continue;
+                            for (int i = 0; i < 4; i++)
 #pragma unroll
                                 for (int j = 0; j < 8; j++) {
-                                    const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
-                                                                 s_cyg[wr * 16 + tr * 4 + i]) < cut;
-                                    const bool fi = rg[i] < ce[j];
-                                    if (ex != fi) {
-                                        const float t = __fmul_rn(ce[j], rv[i]);
-                                        part[i * 8 + j] = __fadd_rn(part[i * 8 + j], ex ? t : -t);
-                                        if (COUNT) inm ^= 1u << (i * 8 + j);
+                                    const bool in = rg[i] < ce[j];
+                                    if (in) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
+                                    inm |= (unsigned)in << (i * 8 + j);
+                                }
+                        } else {
+#pragma unroll
+                            for (int i = 0; i < 4; i++)
+#pragma unroll
+                                for (int j = 0; j < 8; j++) fma_if_less(part[i * 8 + j], rg[i], ce[j], ce[j], rv[i]);
+                        }
+                        if ((ambb >> q) & 1u) {
+                            // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
+                            const unsigned fl = (__shfl_sync(0xffffffffu, myflag, q) >> (tr * 4)) & 0xfu;
+                            if (fl) {
+                                const MgkPt r = st[qq];
+                                const float px = r.xh + r.xl, py = r.yh + r.yl;
+                                const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
+#pragma unroll
+                                for (int i = 0; i < 4; i++) {
+                                    if (!((fl >> i) & 1u)) continue;
+#pragma unroll
+                                    for (int j = 0; j < 8; j++) {
+                                        const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
+                                                                     s_cyg[wr * 16 + tr * 4 + i]) < cut;
+                                        const bool fi = rg[i] < ce[j];
+                                        if (ex != fi) {
+                                            const float t = __fmul_rn(ce[j], rv[i]);
+                                            part[i * 8 + j] = __fadd_rn(part[i * 8 + j], ex ? t : -t);
+                                            if (COUNT) inm ^= 1u << (i * 8 + j);
+                                        }
                                     }
                                 }
                             }
                         }
+                        if (COUNT) cnt += __popc(inm & valid);
                     }
-                    if (COUNT) cnt += __popc(inm & valid);
-                }
-                pc++;
-                if ((pc & 31u) == 0) {
-                    // 32-point partials into the Kahan accumulators in shared memory
+                    pc++;
+                    if ((pc & 31u) == 0) {
+                        // 32-point partials into the Kahan accumulators in tensor memory
+                        __syncwarp();
+                        tmem_wait_st();  // the previous flush's stores have landed
 #pragma unroll
-                    for (int q4 = 0; q4 < 8; q4++) {
-                        float4 sv = ksum[q4 * kThreads + tid], cv = kcmp[q4 * kThreads + tid];
-                        kahan_add(sv.x, cv.x, part[q4 * 4 + 0]);
-                        kahan_add(sv.y, cv.y, part[q4 * 4 + 1]);
-                        kahan_add(sv.z, cv.z, part[q4 * 4 + 2]);
-                        kahan_add(sv.w, cv.w, part[q4 * 4 + 3]);
-                        ksum[q4 * kThreads + tid] = sv;
-                        kcmp[q4 * kThreads + tid] = cv;
-                        part[q4 * 4 + 0] = part[q4 * 4 + 1] = part[q4 * 4 + 2] = part[q4 * 4 + 3] = 0.0f;
+                        for (int c = 0; c < 4; c++) {
+                            float sv[8], cv[8];
+                            tmem_ld8(tS + 8u * c, sv);
+                            tmem_ld8(tC + 8u * c, cv);
+                            tmem_wait_ld(sv, cv);
+#pragma unroll
+                            for (int u = 0; u < 8; u++) {
+                                kahan_add(sv[u], cv[u], part[c * 8 + u]);
+                                part[c * 8 + u] = 0.0f;
+                            }
+                            tmem_st8(tS + 8u * c, sv);
+                            tmem_st8(tC + 8u * c, cv);
+                        }
                     }
                 }
             }
@@ -654,27 +735,35 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         m = s_nm;
         buf ^= 1;
     }
+    __syncwarp();
+    tmem_wait_st();
     if (aborted) {
         // give the outstanding copy a second bounded wait before the CTA (and
-        // its shared memory) goes away
+        // its shared memory) goes away; release the tensor memory
         if (tid == 0) mbar_wait(&mbar[buf], abort_par);
+        tmem_fence_before();
         __syncthreads();
+        if (warp == 0) {
+            tmem_fence_after();
+            tmem_dealloc(s_tmem);
+        }
         return;
     }
 
     // epilogue: FP64 result = (s - c) * normalisation
     const double norm = VARH ? 1.0 : P.k0;
 #pragma unroll
-    for (int q4 = 0; q4 < 8; q4++) {
-        float4 sv = ksum[q4 * kThreads + tid], cv = kcmp[q4 * kThreads + tid];
-        kahan_add(sv.x, cv.x, part[q4 * 4 + 0]);
-        kahan_add(sv.y, cv.y, part[q4 * 4 + 1]);
-        kahan_add(sv.z, cv.z, part[q4 * 4 + 2]);
-        kahan_add(sv.w, cv.w, part[q4 * 4 + 3]);
-        const float ss[4] = {sv.x, sv.y, sv.z, sv.w}, cc[4] = {cv.x, cv.y, cv.z, cv.w};
+    for (int q8 = 0; q8 < 4; q8++) {
+        float ss[8], cc[8];
+        __syncwarp();
+        tmem_ld8(tS + 8u * q8, ss);
+        tmem_ld8(tC + 8u * q8, cc);
+        tmem_wait_ld(ss, cc);
 #pragma unroll
-        for (int u = 0; u < 4; u++) {
-            const int k = q4 * 4 + u, i = k >> 3, j = k & 7;
+        for (int u = 0; u < 8; u++) kahan_add(ss[u], cc[u], part[q8 * 8 + u]);
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const int k = q8 * 8 + u, i = k >> 3, j = k & 7;
             const int r = wr * 16 + tr * 4 + i, c = lane_col(wc, tc, j);
             if (r >= G.nrow || c >= G.ncol) continue;
             const double v = ((double)ss[u] - (double)cc[u]) * norm;
@@ -685,6 +774,12 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 P.out[o] = ((valid >> k) & 1u) ? (float)v : P.nodata;
             }
         }
+    }
+    tmem_fence_before();
+    __syncthreads();
+    if (warp == 0) {
+        tmem_fence_after();
+        tmem_dealloc(s_tmem);
     }
     if (COUNT) {
         for (int o = 16; o; o >>= 1) cnt += __shfl_xor_sync(0xffffffffu, cnt, o);
