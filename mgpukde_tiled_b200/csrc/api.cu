@@ -616,8 +616,14 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
 // of each kind and events between the stages.  Without an explicit tile
 // side the raster is cut into full-width bands of about an eighth of its
 // rows (at least 256, a multiple of the 64-row density block), so that the
-// copies in and out hide under the density of the neighbouring bands.
+// copies in and out hide under the density of the neighbouring bands.  The
+// last 256 rows form a band of their own: its copy out follows the last
+// density launch with nothing left to hide it, so it is kept short.
+#ifndef MGK_RASTER_BANDS
+#define MGK_RASTER_BANDS 8
+#endif
 namespace {
+constexpr int64_t kRasterBands = MGK_RASTER_BANDS;  // full-width bands without an explicit tile side
 struct RasterPipe {
     cudaStream_t h2d = nullptr, d2h = nullptr;
     cudaEvent_t mask_ready[2] = {}, done[2] = {}, out_free[2] = {};
@@ -652,15 +658,21 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
     // tile grid (kde_cuda_kdtr_tiled.cu:1373-1517 walks tiles row-major)
     int64_t tr, tc;
     const int64_t T = tile_side > 0 ? tile_side : c->tile_side;
+    std::vector<int64_t> band_r0;  // full-width bands: first row of band k, then nrows
     if (T > 0) {
         tr = std::min<int64_t>(T, dg->nrows);
         tc = std::min<int64_t>(T, dg->ncols);
     } else {
-        tr = std::max<int64_t>(256, ((dg->nrows + 7) / 8 + 63) / 64 * 64);
+        tr = std::max<int64_t>(256, ((dg->nrows + kRasterBands - 1) / kRasterBands + 63) / 64 * 64);
         tr = std::min<int64_t>(tr, dg->nrows);
         tc = dg->ncols;
+        const int64_t tail = dg->nrows > 2 * 256 ? 256 : 0;
+        for (int64_t r0 = 0; r0 < dg->nrows - tail; r0 += tr) band_r0.push_back(r0);
+        if (tail) band_r0.push_back(dg->nrows - tail);
+        band_r0.push_back(dg->nrows);
     }
-    const int64_t ntr = (dg->nrows + tr - 1) / tr, ntc = (dg->ncols + tc - 1) / tc, ntiles = ntr * ntc;
+    const int64_t ntc = (dg->ncols + tc - 1) / tc;
+    const int64_t ntiles = band_r0.empty() ? (dg->nrows + tr - 1) / tr * ntc : (int64_t)band_r0.size() - 1;
     const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
     RasterPipe pipe;
     cudaError_t ce = pipe.init();
@@ -678,6 +690,13 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask[i], tb);
     }
     auto tile_of = [&](int64_t k, int64_t& r0, int64_t& c0, int64_t& nr, int64_t& nc) {
+        if (!band_r0.empty()) {
+            r0 = band_r0[k];
+            nr = std::min<int64_t>(band_r0[k + 1], r0 + tr) - r0;
+            c0 = 0;
+            nc = dg->ncols;
+            return;
+        }
         r0 = (k / ntc) * tr;
         c0 = (k % ntc) * tc;
         nr = std::min<int64_t>(tr, dg->nrows - r0);
