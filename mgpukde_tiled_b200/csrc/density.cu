@@ -465,6 +465,10 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             if (v && P.mask) v = P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata;
             valid |= (unsigned)v << (i * 8 + j);
         }
+    // A block whose cells are all NoData gathers no candidates: its output
+    // is NoData throughout (the reference skips NoData cells before any sum,
+    // kde_kernel_kdtr.cu:426-428).
+    const bool any_valid = __syncthreads_or(valid != 0u);
 
     float part[32];
 #pragma unroll
@@ -482,7 +486,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 
     if (tid == 0) {
         for (int c = 0; c < kNCur; c++) cur_init(P, G, it, c, s_cur[c]);
-        s_nm = fill_batch(P, G, s_cur, &stage[0], &mbar[0]);
+        s_nm = any_valid ? fill_batch(P, G, s_cur, &stage[0], &mbar[0]) : 0;
     }
     __syncthreads();
     int m = s_nm;
@@ -831,7 +835,14 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
     double acc[32];
 #pragma unroll
     for (int k = 0; k < 32; k++) acc[k] = 0.0;
-    if (G.any) {
+    // all-NoData blocks are skipped, as in the FP32 kernel
+    bool mine = false;
+    for (int k = 0; k < 32 && !mine; k++) {
+        const int r = wr * 16 + tr * 4 + (k >> 3), c = wc * 64 + tc * 8 + (k & 7);
+        mine = r < G.nrow && c < G.ncol &&
+               (!P.mask || P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata);
+    }
+    if (__syncthreads_or(mine) && G.any) {
         int64_t seq = 0;
         for (int64_t by = G.by0; by <= G.by1 && seq < it.k1; by++) {
             int64_t sb, len;
