@@ -286,12 +286,35 @@ __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restr
 }
 
 
-__global__ void k_dist2_cands(int64_t n, const float* __restrict__ x, const float* __restrict__ y,
-                              const float2* __restrict__ cells, const int* __restrict__ start,
-                              const int* __restrict__ near, const float2* __restrict__ cand,
-                              const int* __restrict__ cstart, BinGrid B, double* __restrict__ out) {
+// Points are searched in the order of their bins (a counting sort by bin),
+// so the threads of a warp mostly walk one bin's candidate list: the list's
+// loads are shared and the loop lengths agree.  Each result is stored by
+// point index, so the order changes no value.
+__global__ void k_point_bins(int64_t n, const float* __restrict__ x, const float* __restrict__ y, BinGrid B,
+                             int* __restrict__ key, int* __restrict__ cnt) {
     const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
     if (i >= n) return;
+    int bx, by;
+    bin_of(B, x[i], y[i], bx, by);
+    key[i] = by * B.nbx + bx;
+    atomicAdd(&cnt[key[i]], 1);
+}
+
+__global__ void k_point_order(int64_t n, const int* __restrict__ key, int* __restrict__ cursor,
+                              int32_t* __restrict__ order) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    order[atomicAdd(&cursor[key[i]], 1)] = (int32_t)i;
+}
+
+__global__ void k_dist2_cands(int64_t n, const int32_t* __restrict__ order, const float* __restrict__ x,
+                              const float* __restrict__ y, const float2* __restrict__ cells,
+                              const int* __restrict__ start, const int* __restrict__ near,
+                              const float2* __restrict__ cand, const int* __restrict__ cstart, BinGrid B,
+                              double* __restrict__ out) {
+    const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = order ? order[t] : t;
     const double px = x[i], py = y[i];
     double best = DBL_MAX;
     const double fx = floor((px - B.x0) / B.side), fy = floor((py - B.y0) / B.side);
@@ -519,9 +542,38 @@ int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {
     if (r->nb == 0) {
         k_dist2_binned<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(
             p->n, p->x, p->y, r->bcells, r->bstart, r->bnear, B, p->dist2);
-    } else {
+    } else if (p->n >= (int64_t)INT32_MAX) {
         k_dist2_cands<<<(unsigned)((p->n + 255) / 256), 256, 0, ctx->stream>>>(
-            p->n, p->x, p->y, r->bcells, r->bstart, r->bnear, r->cand, r->cstart, B, p->dist2);
+            p->n, nullptr, p->x, p->y, r->bcells, r->bstart, r->bnear, r->cand, r->cstart, B, p->dist2);
+    } else {
+        // counting sort of the points by bin, then the search in that order
+        const size_t b_key = sizeof(int) * (size_t)p->n, b_cnt = sizeof(int) * (size_t)(r->nbins + 1);
+        int *key = nullptr, *cnt = nullptr;
+        int32_t* order = nullptr;
+        int st;
+        if ((st = mgk_alloc(ctx, (void**)&key, b_key))) return st;
+        if ((st = mgk_alloc(ctx, (void**)&order, b_key)) || (st = mgk_alloc(ctx, (void**)&cnt, b_cnt))) {
+            mgk_free(ctx, key, b_key);
+            mgk_free(ctx, order, b_key);
+            return st;
+        }
+        const unsigned gp = (unsigned)((p->n + 255) / 256);
+        cudaError_t e = cudaMemsetAsync(cnt, 0, b_cnt, ctx->stream);
+        if (e == cudaSuccess) {
+            k_point_bins<<<gp, 256, 0, ctx->stream>>>(p->n, p->x, p->y, B, key, cnt);
+            k_scan_small<<<1, 1024, 0, ctx->stream>>>(cnt, (int)r->nbins);
+            k_point_order<<<gp, 256, 0, ctx->stream>>>(p->n, key, cnt, order);
+            k_dist2_cands<<<gp, 256, 0, ctx->stream>>>(p->n, order, p->x, p->y, r->bcells, r->bstart, r->bnear,
+                                                       r->cand, r->cstart, B, p->dist2);
+            e = cudaGetLastError();
+        }
+        // the buffers go back to the context's pool; later users are ordered
+        // after these kernels on the same stream
+        mgk_free(ctx, key, b_key);
+        mgk_free(ctx, order, b_key);
+        mgk_free(ctx, cnt, b_cnt);
+        if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "k_dist2");
+        MGK_COUNT_LAUNCH(ctx, 3);
     }
     MGK_CHECK_LAUNCH(ctx, "k_dist2");
     MGK_COUNT_LAUNCH(ctx, 1);
