@@ -50,7 +50,31 @@ struct EdgeParams {
     float* ew;  // [nh][ew_stride]
     int64_t ew_stride;
     unsigned long long* evals;
+    const int* list;        // with nh = 1: the points within 3h of the boundary, else null (all points)
+    const int* list_count;  // its length (device)
 };
+
+// One bandwidth with boundary distances: the weight of a point 3h or more
+// from the boundary is 1 (a coalesced pass); the others are listed (warp-
+// aggregated appends, in no fixed order: each weight depends on its point
+// alone) for the integral kernel.
+template <bool VARH>
+__global__ void k_edge_near(EdgeParams E, int* __restrict__ list, int* __restrict__ count) {
+    const int64_t p = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    bool near = false;
+    if (p < E.n) {
+        const float hp = VARH ? E.hpp[p] : (E.hgrid ? E.hgrid[0] : E.hfix);
+        if (E.dist2[p] >= MGK_CUT * mgk_h2(hp)) E.ew[p] = 1.0f;
+        else near = true;
+    }
+    const unsigned b = __ballot_sync(0xffffffffu, near);
+    if (!b) return;  // warp-uniform
+    int base = 0;
+    if (lane == 0) base = atomicAdd(count, __popc(b));
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (near) list[base + __popc(b & ((1u << lane) - 1u))] = (int)p;
+}
 
 __device__ __forceinline__ int64_t trunc_index(double v) {
     v = fmin(fmax(v, -1.0e15), 1.0e15);
@@ -105,7 +129,9 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
     const double cell_area = (double)(g.cs * g.cs);  // float product, kde_cuda_kdtr_tiled.cu:2698
     const int nh = VARH ? 1 : E.nh;
     unsigned long long cnt_total = 0;
-    for (int64_t p = warp0; p < E.n; p += nwarps) {
+    const int64_t ntask = E.list ? (int64_t)*E.list_count : E.n;
+    for (int64_t t = warp0; t < ntask; t += nwarps) {
+        const int64_t p = E.list ? (int64_t)E.list[t] : t;
         const double px = E.x[p], py = E.y[p];
         const double d2b = E.dist2 ? E.dist2[p] : 0.0;
         for (int k = 0; k < nh; k++) {
@@ -242,11 +268,45 @@ int mgk_launch_edge_weights_multi(mgk_ctx* ctx, int64_t n, const float* x, const
     E.ew_stride = ew_stride;
     E.evals = d_evals;
     const int threads = kEdgeWarps * 32;
-    const int64_t blocks = std::min<int64_t>((int64_t)ctx->sm_count * 8, (n + kEdgeWarps - 1) / kEdgeWarps);
-    if (hpp) k_edge_rows<true><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
-    else k_edge_rows<false><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
-    MGK_CHECK_LAUNCH(ctx, "k_edge_rows");
-    MGK_COUNT_LAUNCH(ctx, 1);
+    // a grid-stride kernel: one resident wave, so that no CTA starts its
+    // share only after the others have finished theirs
+    int occ = 1;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &occ, hpp ? (const void*)k_edge_rows<true> : (const void*)k_edge_rows<false>, threads, 0);
+    if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "edge weights occupancy");
+    occ = std::max(occ, 1);
+    const int64_t blocks = std::min<int64_t>((int64_t)ctx->sm_count * occ, (n + kEdgeWarps - 1) / kEdgeWarps);
+    int *list = nullptr, *count = nullptr;
+    const size_t b_list = sizeof(int) * (size_t)n;
+    const bool listed = E.nh == 1 && dist2 && n < (int64_t)INT32_MAX;
+    if (listed) {
+        if ((st = mgk_alloc(ctx, (void**)&list, b_list))) return st;
+        if ((st = mgk_alloc(ctx, (void**)&count, sizeof(int)))) {
+            mgk_free(ctx, list, b_list);
+            return st;
+        }
+        e = cudaMemsetAsync(count, 0, sizeof(int), ctx->stream);
+        if (e == cudaSuccess) {
+            const unsigned gn = (unsigned)((n + 255) / 256);
+            if (hpp) k_edge_near<true><<<gn, 256, 0, ctx->stream>>>(E, list, count);
+            else k_edge_near<false><<<gn, 256, 0, ctx->stream>>>(E, list, count);
+            e = cudaGetLastError();
+        }
+        E.list = list;
+        E.list_count = count;
+    }
+    if (e == cudaSuccess) {
+        if (hpp) k_edge_rows<true><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
+        else k_edge_rows<false><<<(unsigned)blocks, threads, 0, ctx->stream>>>(E);
+        e = cudaGetLastError();
+    }
+    // back to the context's pool; later users are ordered after these kernels on the same stream
+    if (listed) {
+        mgk_free(ctx, list, b_list);
+        mgk_free(ctx, count, sizeof(int));
+    }
+    if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "k_edge_rows");
+    MGK_COUNT_LAUNCH(ctx, listed ? 2 : 1);
     return MGK_OK;
 }
 
