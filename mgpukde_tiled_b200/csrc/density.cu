@@ -50,6 +50,7 @@ constexpr int kThreads = 256;
 constexpr int kBR = 64;         // cell rows of a CTA block
 constexpr int kBC = 128;        // cell columns of a CTA block
 constexpr int kCells = kBR * kBC;
+constexpr int kMergeParts = 8;  // CTAs per split block in the merge kernels (kCells / 8 cells each)
 constexpr int kMB = 64;         // points per mini-batch (a multiple of 32)
 constexpr int kStage64 = 512;   // points staged per batch by the FP64 form
 constexpr float kAmbEps = 4e-6f;
@@ -891,13 +892,17 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
 }
 
 // Merge of split blocks: cell value = sum over the block's slots in order.
+// Cells [part * kCells / gridDim.y, ...) of the block: a block's cells are
+// spread over gridDim.y CTAs, so each thread sums a few cells and the
+// launch is not bound by one CTA's sequential loads.
 __device__ __forceinline__ void merge_block(const DParams& P, int32_t blk, int s0, int s1) {
+    const int per = kCells / (int)gridDim.y, e0 = (int)blockIdx.y * per;
     const int nbx_t = (int)((P.nc + kBC - 1) / kBC);
     const int bxi = blk % nbx_t, byi = blk / nbx_t;
     const int64_t r0 = P.row0 + (int64_t)byi * kBR, c0 = P.col0 + (int64_t)bxi * kBC;
     const int nrow = (int)mgk_min64(kBR, P.row0 + P.nr - r0);
     const int ncol = (int)mgk_min64(kBC, P.col0 + P.nc - c0);
-    for (int e = threadIdx.x; e < kCells; e += blockDim.x) {
+    for (int e = e0 + (int)threadIdx.x; e < e0 + per; e += blockDim.x) {
         const int r = e / kBC, c = e % kBC;
         if (r >= nrow || c >= ncol) continue;
         double v = 0.0;
@@ -1162,7 +1167,7 @@ int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
     }
     MGK_COUNT_LAUNCH(ctx, 1);
     if (D->T.nslots) {
-        k_merge<<<(unsigned)D->T.split_blocks.size(), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
+        k_merge<<<dim3((unsigned)D->T.split_blocks.size(), kMergeParts), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
         MGK_COUNT_LAUNCH(ctx, 1);
     }
     const cudaError_t ce = cudaGetLastError();
@@ -1194,7 +1199,7 @@ int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* D) {
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
         MGK_COUNT_LAUNCH(ctx, 1);  // density (the counting kernel counts itself)
         if (D->T.nslots) {
-            k_merge<<<(unsigned)D->T.split_blocks.size(), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
+            k_merge<<<dim3((unsigned)D->T.split_blocks.size(), kMergeParts), 256, 0, s>>>(P, D->d_sb, D->d_sbeg);
             if ((ce = cudaGetLastError()) != cudaSuccess) break;
             MGK_COUNT_LAUNCH(ctx, 1);
         }
@@ -1320,7 +1325,7 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
         cudaEventRecord(ctx->ev_b, s);
         if ((ce = cudaGetLastError()) != cudaSuccess) break;
         if (!merges.empty()) {
-            k_merge_jobs<<<(unsigned)merges.size(), 256, 0, s>>>(d_jobs, d_mg);
+            k_merge_jobs<<<dim3((unsigned)merges.size(), kMergeParts), 256, 0, s>>>(d_jobs, d_mg);
             if ((ce = cudaGetLastError()) != cudaSuccess) break;
             MGK_COUNT_LAUNCH(ctx, 1);
         }
@@ -1473,7 +1478,7 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc");
     MGK_COUNT_LAUNCH(ctx, 2);
     if (nsplit) {
-        k_merge<<<(unsigned)nsplit, 256, 0, s>>>(P, d_sb, d_sbeg);
+        k_merge<<<dim3((unsigned)nsplit, kMergeParts), 256, 0, s>>>(P, d_sb, d_sbeg);
         if ((ce = cudaGetLastError()) != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density_tile_noalloc merge");
         MGK_COUNT_LAUNCH(ctx, 1);
     }
