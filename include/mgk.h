@@ -303,13 +303,16 @@ int mgk_autotune(mgk_ctx* ctx, const mgk_points* pts, float h, const mgk_grid* g
                  mgk_tuning* out);
 
 /* ---- serving loop ------------------------------------------------------ */
-/* A worker thread with its own context on `device` (HBM budget as for
- * mgk_ctx_create) serves whole fixed-h KDE requests: admission by free slots
- * (max_active) and the estimated device footprint within the budget, points
- * and index resident while a request is active, and each tick one density
- * launch over the next tile (tile_side^2 cells) of every active request, so
- * requests that arrive while others run join the next tick (continuous
- * batching).  A request's raster is bitwise the same alone or in a mix.  No
+/* Two threads, each with its own context on `device` (HBM budget as for
+ * mgk_ctx_create), serve whole fixed-h KDE requests.  The preparation thread
+ * admits requests by free slots (max_active) and their estimated device
+ * footprint within the budget, uploads and indexes them (their points,
+ * index and tiles are its context's memory, resident while a request is
+ * active) and frees them when they finish.  The worker thread runs each
+ * tick as one density launch over the next tile (tile_side^2 cells) of
+ * every active request, so requests that arrive while others run join the
+ * next tick (continuous batching); its context holds only per-tick plan
+ * scratch.  A request's raster is bitwise the same alone or in a mix.  No
  * reference counterpart (the reference runs one study per process). */
 typedef struct mgk_server mgk_server;
 typedef struct mgk_request {
@@ -341,7 +344,7 @@ int mgk_serve_poll(mgk_server* srv, uint64_t ticket, int* done, mgk_result* res)
  * passes (MGK_ERR_TIMEOUT, the ticket stays valid). */
 int mgk_serve_wait(mgk_server* srv, uint64_t ticket, double timeout_s, mgk_result* res);
 int mgk_serve_stats(mgk_server* srv, mgk_serve_info* out);
-/* Finishes the queued and active requests, then stops the worker. */
+/* Finishes the queued and active requests, then stops both threads. */
 int mgk_serve_destroy(mgk_server* srv);
 
 /* ---- whole path from host buffers ------------------------------------- */

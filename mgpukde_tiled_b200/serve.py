@@ -1,6 +1,8 @@
 """Python side of the serving loop (mgk_serve_* in the C ABI).
 
-A Server owns a worker thread and a device context; submit() queues a whole
+A Server owns a preparation thread and a worker thread, each with a device
+context (requests are uploaded and indexed on the first while the second
+runs the ticks); submit() queues a whole
 fixed-h KDE request and returns a Ticket; wait() blocks until the request's
 raster is in its host output array.  The arrays handed to submit() are kept
 alive by the ticket until the request completes.
