@@ -63,7 +63,7 @@ int mgk_alloc(mgk_ctx* ctx, void** p, size_t bytes) {
     if (ctx->in_use + cls > ctx->budget)
         return mgk_fail(ctx, MGK_ERR_BUDGET,
                         "HBM budget exceeded: need " + std::to_string(cls) + " B, in use " +
-                            std::to_string(ctx->in_use) + " of " + std::to_string(ctx->budget));
+                            std::to_string(ctx->in_use.load()) + " of " + std::to_string(ctx->budget));
     cudaError_t e = cudaMalloc(p, cls);
     if (e == cudaErrorMemoryAllocation && !ctx->pool.empty()) {
         (void)cudaGetLastError();
@@ -198,7 +198,7 @@ int mgk_ctx_synchronize(mgk_ctx* c) {
 
 const char* mgk_ctx_last_error(const mgk_ctx* c) { return c ? c->last_error.c_str() : "no context"; }
 
-uint64_t mgk_ctx_bytes_in_use(const mgk_ctx* c) { return c ? c->in_use : 0; }
+uint64_t mgk_ctx_bytes_in_use(const mgk_ctx* c) { return c ? c->in_use.load() : 0; }
 
 uint64_t mgk_ctx_kernel_launches(const mgk_ctx* c) { return c ? c->launches : 0; }
 

@@ -3,6 +3,7 @@
 
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -27,7 +28,7 @@ struct mgk_ctx {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     uint64_t budget = 0;
-    uint64_t in_use = 0;
+    std::atomic<uint64_t> in_use{0};  // read by other threads (serving statistics)
     std::string last_error;
     // small pinned/device scratch for scalar results
     unsigned long long* d_counter = nullptr;  // 8 counters
