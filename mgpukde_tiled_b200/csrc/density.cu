@@ -8,34 +8,39 @@
 //   den(c) = sum_p [d^2 < 9 h_p^2] exp(-d^2 / 2 h_p^2) / (h_p^2 TWO_PI) w_p e_p
 //
 // Layout: a CTA (256 threads) owns a 64 x 128 block of cells; warp w owns a
-// 16 x 64 sub-block, lane l a 4 x 8 micro-tile.  Candidates (points of the
-// bins within 3h of the block, one contiguous range per bin row) arrive in
-// mini-batches of 32, taken across bin rows, through a double-buffered TMA
-// bulk copy (cp.async.bulk + mbarrier) into shared memory.  Per mini-batch:
+// 16 x 64 sub-block, lane l a 4 x 8 micro-tile.  A block whose cells are all
+// NoData stages no candidates and writes NoData (the reference skips NoData
+// cells, kde_kernel_kdtr.cu:426-428).  Candidates (points of the bins within
+// 3h of the block, one contiguous range per bin row) arrive in mini-batches
+// of 64, taken by two cursors across bin rows, through a double-buffered TMA
+// bulk copy (cp.async.bulk + mbarrier) into shared memory; the next batch is
+// staged during the current batch's phase B by the warp with the fewest
+// points to sum.  Per mini-batch:
 //
-//  phase A (all 256 threads, 8 per point): the Gaussian factorises over the
-//    grid, exp2(-(a_j + b_i)) = E_j F_i with a_j = dx_j^2 k2, b_i = dy_i^2 k2,
-//    k2 = log2(e) / (2 h^2).  The 128 column factors and 64 row factors of
-//    the block are computed once per point.  Coordinates are hi/lo float pairs on
-//    a common quantum, so dx = (xh - cxh) + (xl - cxl) is exact as a pair and
-//    a = dx^2 k2 is formed with error-free float products (no FP64, no
-//    conversions); E = ex2(-a_hi) (1 - a_lo ln2).  Row entries also carry the
-//    cutoff threshold G_i = 2^-cut / 2^-b_i (a_j < cut - b_i <=> E_j > G_i),
-//    a flag marking rows where some column lies within a 4e-6 (log2 units)
-//    band of the cutoff, and each warp's sub-block gets an exact-enough
-//    rectangle-vs-disc test.
-//  phase B (each warp, its processed points): per cell one compare
-//    E_j > G_i and a predicated FFMA part += E_j F_i.  Rows flagged as
-//    ambiguous are re-decided with the exact FP64 test of the oracle, so the
-//    summed pair set is exactly the reference's.
+//  phase A (all 256 threads, 8 per point): each warp's sub-block first gets
+//    an exact-enough rectangle-vs-disc test (skip, fully inside, partial).
+//    The Gaussian factorises over the grid, exp2(-(a_j + b_i)) = E_j F_i with
+//    a_j = dx_j^2 k2, b_i = dy_i^2 k2, k2 = log2(e) / (2 h^2); the column
+//    factors and row factors are built only for the column halves and warp
+//    rows of the sub-blocks that sum the point.  Coordinates are hi/lo float
+//    pairs on a common quantum, so dx = (xh - cxh) + (xl - cxl) is exact as a
+//    pair and a = dx^2 k2 is formed with error-free float products (no FP64,
+//    no conversions); E = ex2(-a_hi) (1 - a_lo ln2).  Row entries also carry
+//    the cutoff threshold G_i = 2^-cut / 2^-b_i (a_j < cut - b_i <=>
+//    E_j > G_i) and a flag marking rows where some column lies within a 4e-6
+//    (log2 units) band of the cutoff.
+//  phase B (each warp, its processed points): per cell one FFMA (fully
+//    inside) or one compare E_j > G_i and a predicated FFMA part += E_j F_i.
+//    Rows flagged as ambiguous are re-decided with the exact FP64 test of the
+//    oracle, so the summed pair set is exactly the reference's.
 //
 // Accumulation: FP32 partial sums over 32 points per cell (registers), added
-// into a Kahan-compensated FP32 accumulator (shared memory, 64 KB per CTA,
-// which with the 128 registers per thread leaves two CTAs per SM); the
-// epilogue forms (s - c) times the
-// kernel normalisation in FP64.  Heavy blocks are split into work items whose
-// FP64 partials are merged in a fixed order, so results are bitwise
-// reproducible.
+// into a Kahan-compensated FP32 accumulator in tensor memory (tcgen05: 128
+// columns per CTA, sum and compensation of each thread's 32 cells in 64
+// columns of its warp's lane quarter); the epilogue forms (s - c) times the
+// kernel normalisation in FP64.  With 126-128 registers per thread two CTAs
+// run per SM.  Heavy blocks are split into work items whose FP64 partials
+// are merged in a fixed order, so results are bitwise reproducible.
 #include <algorithm>
 #include <cstring>
 #include <cmath>
