@@ -323,6 +323,29 @@ def cpu_baseline(c, side=1024, gpu_window=None):
     return out
 
 
+def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_bytes, hbm_gbs):
+    """The roofline object of the density kernel's bench line.  The kernel is
+    bound by FP32 issue: `achieved` is its algorithmic FLOP rate (8 flop-
+    equivalents per in-cutoff pair) against the nominal FP32 peak (the
+    measured peaks hold no FP32 figure).  `hbm` gives the same launch against
+    the measured copy bandwidth: its algorithmic bytes (mask read plus
+    output write) and its measured DRAM traffic per launch, as GB/s."""
+    fp32_peak = nsm * 128 * 2 * sm_max_mhz * 1e6 / 1e12
+    achieved = evals * FLOP_PER_EVAL / kernel_s / 1e12
+    out = {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+           "frac": achieved / fp32_peak, "traffic": traffic, "kernel": "k_density",
+           "kernel_ms": kernel_s * 1e3, "flop_per_eval": FLOP_PER_EVAL,
+           "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max_mhz:.0f} MHz "
+                        f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"}
+    if hbm_gbs:
+        hbm_achieved = alg_bytes / kernel_s / 1e9
+        out["hbm"] = {"achieved": hbm_achieved, "peak": hbm_gbs, "unit": "GB/s", "frac": hbm_achieved / hbm_gbs,
+                      "algorithmic_bytes": alg_bytes,
+                      "traffic_gbs": None if traffic is None else traffic / kernel_s / 1e9,
+                      "peak_note": f"measured copy bandwidth ({peak_kind})"}
+    return out
+
+
 def run_reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -480,9 +503,7 @@ def run_mgk(args):
     peaks, peak_kind = load_peaks()
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))
     nsm = torch.cuda.get_device_properties(local).multi_processor_count
-    fp32_peak_tflops = nsm * 128 * 2 * sm_max * 1e6 / 1e12
     dens_s = float(np.mean(dens_ms)) / 1e3
-    achieved = ev_d * FLOP_PER_EVAL / dens_s / 1e12
     traffic = None
     tp = os.path.join(REPO, "profiles", "k_density_traffic.txt")
     if os.path.exists(tp) and args.scale == 1.0:
@@ -498,11 +519,8 @@ def run_mgk(args):
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(e2e_ms.item())},
         "gpu_launches": launches,
-        "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak_tflops, "unit": "TFLOP/s",
-                     "frac": achieved / fp32_peak_tflops, "traffic": traffic, "kernel": "k_density",
-                     "kernel_ms": dens_s * 1e3, "flop_per_eval": FLOP_PER_EVAL,
-                     "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
-                                  f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"},
+        "roofline": density_roofline(ev_d, dens_s, nsm, sm_max, peak_kind, traffic,
+                                     4 * dg.nrows * dg.ncols * 2, peaks.get("hbm_gbs")),
         "clocks": clocks,
         "fp64_form": fp64_form,
     }

@@ -1,7 +1,7 @@
-"""bench.py's reference arm on the CPU: its JSON line keeps the bench
-contract (the reference program's own CPU path, timed on the host cores,
-on the single-large workload), and under torchrun only rank 0 works and
-prints."""
+"""bench.py's contract on the CPU: the reference arm's JSON line (the
+reference program's own CPU path, timed on the host cores, on the
+single-large workload), rank 0 alone working and printing under torchrun,
+and the roofline object of the GPU line computed from known numbers."""
 import json
 import os
 import subprocess
@@ -44,3 +44,24 @@ def test_reference_arm_other_ranks_exit_quietly():
     p = run(env)
     assert p.returncode == 0, p.stderr[-2000:]
     assert not p.stdout.strip()
+
+
+def test_density_roofline_fields():
+    """The GPU line's roofline object, from known numbers: 4e10 evals in 10 ms
+    on 148 SMs at 1965 MHz, 850.6 MB of traffic, 800 MB algorithmic."""
+    sys.path.insert(0, REPO)
+    import bench
+
+    r = bench.density_roofline(4.0e10, 0.010, 148, 1965.0, "measured", 850_600_000, 800_000_000, 6454.6)
+    assert r["bound"] == "fp32" and r["unit"] == "TFLOP/s" and r["kernel"] == "k_density"
+    assert abs(r["peak"] - 148 * 128 * 2 * 1965e6 / 1e12) < 1e-9
+    assert abs(r["achieved"] - 4.0e10 * 8 / 0.010 / 1e12) < 1e-9
+    assert abs(r["frac"] - r["achieved"] / r["peak"]) < 1e-12
+    assert r["traffic"] == 850_600_000 and abs(r["kernel_ms"] - 10.0) < 1e-9
+    h = r["hbm"]
+    assert h["unit"] == "GB/s" and h["peak"] == 6454.6
+    assert abs(h["achieved"] - 80.0) < 1e-9 and abs(h["traffic_gbs"] - 85.06) < 1e-9
+    assert abs(h["frac"] - 80.0 / 6454.6) < 1e-12
+    # no measured HBM figure, no traffic capture: the FP32 view alone / no traffic rate
+    assert "hbm" not in bench.density_roofline(1e9, 0.01, 148, 1965.0, "fallback", None, 1, None)
+    assert bench.density_roofline(1e9, 0.01, 148, 1965.0, "measured", None, 8, 6000.0)["hbm"]["traffic_gbs"] is None
