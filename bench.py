@@ -248,8 +248,9 @@ def crop_inputs(c, side):
     x, y = c["x"], c["y"]
     keep = (x > x0 - reach) & (x < x1 + reach) & (y > y0 - reach) & (y < y1 + reach)
     g = synth.Grid(side, side, np.float32(x0), np.float32(y0), dg.cs, dg.nodata)
-    return dict(x=x[keep], y=y[keep], w=c["w"][keep], grid=g, mask=c["density_mask"][r0:r0 + side, c0:c0 + side],
-                window=(r0, c0, side, side))
+    mask = (np.ones((side, side), np.float32) if c["density_mask"] is None
+            else c["density_mask"][r0:r0 + side, c0:c0 + side])
+    return dict(x=x[keep], y=y[keep], w=c["w"][keep], grid=g, mask=mask, window=(r0, c0, side, side))
 
 
 def crop_evals(c, crop):
@@ -284,25 +285,12 @@ def run_reference_binary(c, crop, threads):
         return (t_den + t_edge) / 1e3
 
 
-def cpu_baseline(c, side=1024, gpu_window=None):
+def cpu_baseline(c, side=1024):
     """The reference's CPU path (or the FP64 oracle port) on a crop of the
-    workload.  gpu_window: the GPU raster over the same window, checked
-    against the FP64 oracle's density of the crop (its halo points are all
-    the points that reach it)."""
+    workload: a side x side density window with its halo points."""
     threads = os.cpu_count() or 1
     crop = crop_inputs(c, side)
     dev, eev, ew, den_ref = crop_evals(c, crop)
-    acc = None
-    if gpu_window is not None:
-        valid = crop["mask"] != crop["grid"].nodata
-        ref = den_ref[valid].astype(np.float64)
-        got = gpu_window[valid].astype(np.float64)
-        rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
-        acc = {"max_rel_err": float(rel.max()) if rel.size else 0.0,
-               "nodata_cells_equal": bool(np.array_equal(gpu_window[~valid], crop["mask"][~valid])),
-               "cells": int(valid.sum()),
-               "sample": f"the cpu_baseline window ({side}x{side}) of the last timed step's raster against the "
-                         f"FP64 oracle"}
     if os.path.exists(REF_BIN):
         t = run_reference_binary(c, crop, threads)
         kind = "reference"
@@ -316,10 +304,59 @@ def cpu_baseline(c, side=1024, gpu_window=None):
     sample = (f"{side}x{side} density window (median-density of 25 candidate windows) with its {len(crop['x'])} halo points "
               f"(density + edge-correction evals {dev + eev}); reference brute-force CPU path, "
               f"{'mode 1, h_option -1' if kind == 'reference' else 'FP64 oracle'}")
-    out = {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
-           "seconds": t}
-    if acc is not None:
-        out["accuracy"] = acc
+    return {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "cores": threads, "kind": kind, "sample": sample,
+            "seconds": t}
+
+
+# ------------------------------------------------------------ accuracy legs --
+def max_rel_err(got, ref, valid, rows=256):
+    """Largest |got - ref| / |ref| over the valid cells, a band of rows at a
+    time (bounded temporaries on rasters of 1e8-1e9 cells)."""
+    m = 0.0
+    for r in range(0, got.shape[0], rows):
+        v = valid[r:r + rows]
+        if not v.any():
+            continue
+        g = got[r:r + rows][v].astype(np.float64)
+        f = np.asarray(ref[r:r + rows][v], np.float64)
+        m = max(m, float(np.max(np.abs(g - f) / np.maximum(np.abs(f), 1e-300))))
+    return m
+
+
+def single_large_accuracy(c, rasters, ev_d, ev_e):
+    """The whole study recomputed by the FP64 oracle on all host threads
+    (boundary, distances and edge weights of every point, density of every
+    cell of the raster), against each GPU raster in `rasters` (name ->
+    host array): max relative error over the valid cells, NoData cells equal,
+    and the in-cutoff pair counts equal."""
+    import oracle_py as o
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    dg, mask = c["density_grid"], c["density_mask"]
+    t0 = time.perf_counter()
+    eg = o.grid(*c["edge_grid"].astuple())
+    d2 = o.dist2_boundary(c["x"], c["y"], eg, o.mark_boundary(eg, c["edge_mask"]))
+    ew, eev = o.edge_weights(c["x"], c["y"], c["h"], d2, eg, c["edge_mask"])
+    den, dev = o.density(c["x"], c["y"], c["w"], ew, c["h"], o.grid(*dg.astuple()), mask)
+    t = time.perf_counter() - t0
+    valid = mask != dg.nodata
+    out = {"scope": f"every cell of the {dg.nrows}x{dg.ncols} raster", "cells": int(valid.sum()),
+           "nodata_cells": int(valid.size - valid.sum())}
+    errs, nds = [], []
+    for name, r in rasters.items():
+        e = max_rel_err(r, den, valid)
+        nd = bool(np.array_equal(r[~valid], mask[~valid]))
+        out[f"max_rel_err_{name}"] = e
+        out[f"nodata_cells_equal_{name}"] = nd
+        errs.append(e)
+        nds.append(nd)
+    out.update({"max_rel_err": max(errs), "nodata_cells_equal": all(nds), "tolerance": 1e-6,
+                "density_evals_equal": bool(dev == ev_d), "edge_evals_equal": bool(eev == ev_e),
+                "oracle_density_evals": int(dev), "oracle_edge_evals": int(eev),
+                "oracle_seconds": t, "oracle_threads": threads,
+                "sample": "the FP64 oracle of the whole study against " + " and ".join(
+                    {"step": "the last timed step's raster", "e2e": "the last end-to-end call's raster"}.get(k, k)
+                    for k in rasters)})
     return out
 
 
@@ -441,12 +478,8 @@ def run_mgk(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
     ms_max = float(t.item())
-    # the timed steps' raster over the CPU baseline's window, for the accuracy check
-    acc_window = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        side = min(1024, dg.nrows, dg.ncols)
-        wr0, wc0 = pick_window(c, side)
-        acc_window = dout[wr0:wr0 + side, wc0:wc0 + side].cpu().numpy()
+    # the last timed step's raster, for the whole-raster accuracy check
+    step_raster = dout.cpu().numpy() if (rank == 0 and world == 1 and not args.no_accuracy) else None
     total_evals = evals
     if world > 1:  # each rank ran its own study: the job's evals are the sum over ranks
         ev_t = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
@@ -524,13 +557,15 @@ def run_mgk(args):
         "clocks": clocks,
         "fp64_form": fp64_form,
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        try:
-            unbind_numa()
-            out["cpu_baseline"] = cpu_baseline(c, gpu_window=acc_window)
-            out["accuracy"] = out["cpu_baseline"].pop("accuracy", None)
-        except Exception as e:  # reported, not fatal
-            out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+    if rank == 0 and world == 1:
+        unbind_numa()
+        if not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_baseline(c)
+            except Exception as e:  # reported, not fatal
+                out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if step_raster is not None:
+            out["accuracy"] = single_large_accuracy(c, {"step": step_raster, "e2e": hout.numpy()}, ev_d, ev_e)
     if rank == 0:
         print(json.dumps(out))
     pts.close()
@@ -563,6 +598,44 @@ def loo_cpu_check(c, hgrid, logl, pts, nsmall=16):
     acc = {"logl_max_rel_err": float(max(rel)), "h_checked": [float(hgrid[k]) for k in ks],
            "sample": "GPU logL of the timed batch against the FP64 oracle at those h"}
     return cb, acc
+
+
+def loo_argmax_check(c, hgrid, logl, best, radius=2):
+    """The FP64 oracle's LogLikelihood (its own boundary distances and edge
+    weights at each h, then the leave-one-out sum) at the GPU's argmax index
+    and its `radius` neighbours on each side: the argmax over that
+    neighbourhood must be the same index, and the margin to the runner-up is
+    reported next to the largest relative logL error there."""
+    import oracle_py as o
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    eg, em = o.grid(*c["edge_grid"].astuple()), c["edge_mask"]
+    x, y, w = c["x"], c["y"], c["w"]
+    t0 = time.perf_counter()
+    d2 = o.dist2_boundary(x, y, eg, o.mark_boundary(eg, em))
+    ks = [k for k in range(best - radius, best + radius + 1) if 0 <= k < len(hgrid)]
+    refs = [o.loglik_at(x, y, w, d2, eg, em, float(hgrid[k])) for k in ks]
+    t = time.perf_counter() - t0
+    ref_ll = np.array([r[0] for r in refs])
+    gl = np.asarray(logl, np.float64)
+    k_or = ks[int(np.argmax(ref_ll))]
+    masked = gl.copy()
+    masked[best] = -np.inf
+    runner = int(np.argmax(masked))
+    ib = ks.index(best)
+    or_others = np.delete(ref_ll, ib)
+    rel = np.abs(gl[ks] - ref_ll) / np.abs(ref_ll)
+    return {"argmax_gpu": int(best), "argmax_oracle": int(k_or), "argmax_equal": bool(k_or == best),
+            "h_best": float(hgrid[best]), "indices_checked": ks,
+            "h_checked": [float(hgrid[k]) for k in ks],
+            "logl_oracle": [float(v) for v in ref_ll], "logl_gpu": [float(gl[k]) for k in ks],
+            "logl_max_rel_err": float(rel.max()),
+            "runner_up_gpu": runner, "margin_gpu": float(gl[best] - gl[runner]),
+            "margin_oracle": float(ref_ll[ib] - or_others.max()) if or_others.size else None,
+            "margin_rel": float((gl[best] - gl[runner]) / abs(gl[best])),
+            "oracle_seconds": t, "oracle_threads": threads,
+            "sample": f"FP64 oracle LogLikelihood at the GPU's argmax index and {radius} neighbours on each side, "
+                      f"all {len(x)} points"}
 
 
 def run_bandwidth_select(args):
@@ -624,9 +697,11 @@ def run_bandwidth_select(args):
            "evals_per_step": evals, "edge_evals": ev_edge, "loo_evals": ev_loo,
            "batch_ms": float(np.mean(loo_ms)), "argmax": best, "h_best": float(hgrid[best]),
            "gpu_launches": launches, "clocks": clocks}
+    unbind_numa()
     if not args.no_cpu_baseline:
-        unbind_numa()
         out["cpu_baseline"], out["accuracy"] = loo_cpu_check(c, hgrid, logl, pts)
+    if not args.no_accuracy:
+        out.setdefault("accuracy", {})["argmax"] = loo_argmax_check(c, hgrid, logl, best)
     print(json.dumps(out))
     pts.close()
     em.close()
@@ -844,6 +919,15 @@ def run_out_of_core(args):
            "evals_per_step": evals, "density_evals": ev_d, "edge_evals": ev_e,
            "output_bytes": int(host.nbytes), "output_gb_s": host.nbytes / (ms / 1e3) / 1e9,
            "gpu_launches": launches, "clocks": clocks}
+    if rank == 0 and world == 1:
+        unbind_numa()
+        if not args.no_cpu_baseline:
+            try:
+                out["cpu_baseline"] = cpu_baseline(c, side=512)
+            except Exception as e:  # reported, not fatal
+                out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if not args.no_accuracy:
+            out["accuracy"] = out_of_core_accuracy(c, host, tile)
     if rank == 0:
         print(json.dumps(out))
     pts.close()
@@ -852,6 +936,47 @@ def run_out_of_core(args):
     if world > 1:
         dist.destroy_process_group()
     return 0
+
+
+def out_of_core_accuracy(c, host, tile):
+    """Whole output tiles of the streamed raster recomputed by the FP64 oracle
+    on all host threads: two corner tiles (the top-left one and the ragged
+    bottom-right one), two edge tiles and an interior one.  Each tile's
+    oracle sees every point within 3h of it, with its own boundary distances
+    and edge weights.  The raster has no density mask (every cell valid)."""
+    import oracle_py as o
+    threads = os.cpu_count() or 1
+    o.set_threads(threads)
+    dg = c["density_grid"]
+    nt_r, nt_c = (dg.nrows + tile - 1) // tile, (dg.ncols + tile - 1) // tile
+    picks = [(0, 0), (0, nt_c // 2), (nt_r // 2, 0), (nt_r // 2, nt_c // 2), (nt_r - 1, nt_c - 1)]
+    reach = 3.0 * c["h"]
+    t0 = time.perf_counter()
+    eg = o.grid(*c["edge_grid"].astuple())
+    bnd = o.mark_boundary(eg, c["edge_mask"])
+    x, y, w = c["x"], c["y"], c["w"]
+    tiles = []
+    for tr, tc in picks:
+        r0, c0 = tr * tile, tc * tile
+        nr, nc = min(tile, dg.nrows - r0), min(tile, dg.ncols - c0)
+        x0 = float(dg.xll) + c0 * float(dg.cs)
+        x1 = x0 + nc * float(dg.cs)
+        y1 = float(dg.yll) + (dg.nrows - r0) * float(dg.cs)
+        y0 = y1 - nr * float(dg.cs)
+        keep = (x > x0 - reach - 1) & (x < x1 + reach + 1) & (y > y0 - reach - 1) & (y < y1 + reach + 1)
+        xs, ys, ws = x[keep], y[keep], w[keep]
+        d2 = o.dist2_boundary(xs, ys, eg, bnd)
+        ew, _ = o.edge_weights(xs, ys, c["h"], d2, eg, c["edge_mask"])
+        den, dev = o.density(xs, ys, ws, ew, c["h"], o.grid(*dg.astuple()), None, window=(r0, c0, nr, nc))
+        got = host[r0:r0 + nr, c0:c0 + nc]
+        tiles.append({"tile": [int(tr), int(tc)], "cells": int(nr * nc), "points": int(keep.sum()),
+                      "evals": int(dev), "max_rel_err": max_rel_err(got, den, np.ones((nr, nc), bool))})
+    t = time.perf_counter() - t0
+    return {"scope": f"{len(tiles)} whole output tiles of {tile}^2 (ragged at the raster's edge)",
+            "tiles": tiles, "max_rel_err": max(tt["max_rel_err"] for tt in tiles), "tolerance": 1e-6,
+            "cells": sum(tt["cells"] for tt in tiles), "nodata_cells": 0,
+            "oracle_seconds": t, "oracle_threads": threads,
+            "sample": "the last timed job's streamed raster against the FP64 oracle, tile by tile"}
 
 
 # ------------------------------------------------------------ serving (C4) --
@@ -930,6 +1055,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-form", action="store_true")
+    ap.add_argument("--no-accuracy", action="store_true",
+                    help="skip the FP64 oracle check of the whole output (minutes of host CPU at full scale)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference_arm(args)

@@ -185,9 +185,13 @@ int mgk_density_tile_fp64(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g,
  * lives in one fixed file-scope device array of about 12.3 MiB that every GPU
  * loading the library holds until the process exits.  Limit: tiles of at most
  * 4096 x 4096 cells (MGK_ERR_INVALID beyond).  The first call on a device looks
- * up that array's device address (once per device); make that first call
- * before any stream capture.  All calls share the one array: calls that
- * overlap on the GPU (other streams, other threads) race and must be
+ * up that array's device address (once per device).  Every call makes
+ * ctx's device current for its duration (the caller's device is restored on
+ * return) and waits on ctx's stream twice (the plan reads the block counts
+ * back, and the call finishes before returning, because the next call reuses
+ * the array), so it cannot be called while that stream is being captured.
+ * All calls share the one array and keep the last call's contents: calls
+ * that overlap on the GPU (other streams, other threads) race and must be
  * serialised by the caller.  No counterpart in the reference. */
 int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
                              int64_t col0, int64_t nr, int64_t nc, const float* d_mask_tile,

@@ -1387,6 +1387,20 @@ Item g_na_items[kNaMaxItems];
 int32_t g_na_split[kNaMaxSlots];
 int32_t g_na_split_begin[kNaMaxSlots + 1];
 
+// Makes `device` current for a scope and restores the caller's device after.
+struct NaDeviceScope {
+    int prev = -1;
+    cudaError_t err = cudaSuccess;
+    explicit NaDeviceScope(int device) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != device) err = cudaSetDevice(device);
+    }
+    ~NaDeviceScope() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
 }  // namespace
 
 extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
@@ -1405,15 +1419,15 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     std::lock_guard<std::mutex> lock(g_na_mu);
     if (ctx->device < 0 || ctx->device >= kNaMaxDevices)
         return mgk_fail(ctx, MGK_ERR_INVALID, "density_tile_noalloc: device index out of range");
+    // the context's device stays current for the whole call (the address
+    // look-up, the kernels and the copies); the caller's is restored on return
+    NaDeviceScope scope(ctx->device);
+    if (scope.err != cudaSuccess) return mgk_cuda_fail(ctx, scope.err, "density_tile_noalloc: cudaSetDevice");
     // set-up, once per device, with that device current: the host-side name of
     // a __device__ array is not its device address, so look the address up
     if (!g_na_addr[ctx->device]) {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (cur != ctx->device) cudaSetDevice(ctx->device);
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_density_scratch);
-        if (cur != ctx->device && cur >= 0) cudaSetDevice(cur);
         if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "cudaGetSymbolAddress(g_density_scratch)");
         g_na_addr[ctx->device] = static_cast<unsigned char*>(p);
     }
@@ -1431,8 +1445,9 @@ extern "C" int mgk_density_tile_noalloc(mgk_ctx* ctx, const mgk_index* idx, cons
     P.scratch = reinterpret_cast<double*>(base + kNaOffSlots);
 
     // plan: candidates per block (device) -> work items (host, static arrays)
+    // (k_block_counts also clears the staging-wait flag P.err of this launch)
     k_block_counts<<<(nblk + 255) / 256, 256, 0, s>>>(P, nbx_t, nby_t, d_counts);
-    cudaError_t ce = cudaMemsetAsync(P.err, 0, sizeof(unsigned long long), s);
+    cudaError_t ce = cudaGetLastError();
     if (ce == cudaSuccess)
         ce = cudaMemcpyAsync(g_na_counts, d_counts, sizeof(int64_t) * nblk, cudaMemcpyDeviceToHost, s);
     if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);

@@ -277,15 +277,80 @@ static void bins_free(bins_t* b) {
     free(b->idx);
 }
 
-/* Bin index range covering [lo, hi] along one axis, clamped. */
-static inline void bin_span(double lo, double hi, double o, double side, int64_t nbins,
-                            int64_t* a, int64_t* z) {
-    int64_t l = (int64_t)floor((lo - o) / side) - 1;
-    int64_t u = (int64_t)floor((hi - o) / side) + 1;
+/* Sources sorted by bin with their data stored contiguously, so that a
+ * query streams through memory instead of gathering by index.  Bins of side
+ * about h_max; a query at (qx, qy) with reach R visits, per bin row within R,
+ * only the bins that the disc of radius R reaches in that row.  Points are
+ * binned with floor((v - o) / side) in double, which is monotone in v, so the
+ * visited bins hold every source within R of the query (the candidate set is
+ * a superset of the in-cutoff pairs; the cutoff test itself is unchanged). */
+typedef struct {
+    bins_t b;
+    float* x;      /* bin-major copies of the sources */
+    float* y;
+    double* w;     /* (double) weight, or 1 */
+    double* e;     /* edge weight, or 1 */
+    double* h2;    /* orc_h2 of the source's bandwidth */
+    int64_t* id;   /* original index */
+} sbins_t;
+
+static void sbins_build(sbins_t* s, int64_t n, const float* x, const float* y, const float* w,
+                        const double* ew, const float* hs, float h, double side) {
+    bins_build(&s->b, n, x, y, side);
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    s->x = (float*)malloc(sizeof(float) * nn);
+    s->y = (float*)malloc(sizeof(float) * nn);
+    s->w = (double*)malloc(sizeof(double) * nn);
+    s->e = (double*)malloc(sizeof(double) * nn);
+    s->h2 = (double*)malloc(sizeof(double) * nn);
+    s->id = s->b.idx;
+    for (int64_t t = 0; t < n; t++) {
+        const int64_t i = s->b.idx[t];
+        s->x[t] = x[i];
+        s->y[t] = y[i];
+        s->w[t] = (double)(w ? w[i] : 1.0f);
+        s->e[t] = ew ? ew[i] : 1.0;
+        s->h2[t] = orc_h2(hs ? hs[i] : h);
+    }
+}
+
+static void sbins_free(sbins_t* s) {
+    free(s->x);
+    free(s->y);
+    free(s->w);
+    free(s->e);
+    free(s->h2);
+    bins_free(&s->b);
+}
+
+/* Bin rows [*by0, *by1] within reach R of qy. */
+static inline void sbins_rows(const sbins_t* s, double qy, double R, int64_t* by0, int64_t* by1) {
+    const bins_t* b = &s->b;
+    int64_t l = (int64_t)floor((qy - R - b->y0) / b->side);
+    int64_t u = (int64_t)floor((qy + R - b->y0) / b->side);
+    *by0 = l < 0 ? 0 : l;
+    *by1 = u > b->nby - 1 ? b->nby - 1 : u;
+}
+
+/* Candidate range [*t0, *t1) of bin row by for a query at (qx, qy), reach R:
+ * the row's bins that intersect the disc's chord at the row's nearest y. */
+static inline void sbins_row_range(const sbins_t* s, int64_t by, double qx, double qy, double R,
+                                   int64_t* t0, int64_t* t1) {
+    const bins_t* b = &s->b;
+    const double rlo = b->y0 + (double)by * b->side, rhi = rlo + b->side;
+    double dy = qy < rlo ? rlo - qy : (qy > rhi ? qy - rhi : 0.0);
+    dy *= 1.0 - 1e-9;
+    const double rr = R * R - dy * dy;
+    *t0 = *t1 = 0;
+    if (rr < 0.0) return;
+    const double hw = sqrt(rr) * (1.0 + 1e-9);
+    int64_t l = (int64_t)floor((qx - hw - b->x0) / b->side);
+    int64_t u = (int64_t)floor((qx + hw - b->x0) / b->side);
     if (l < 0) l = 0;
-    if (u > nbins - 1) u = nbins - 1;
-    *a = l;
-    *z = u;
+    if (u > b->nbx - 1) u = b->nbx - 1;
+    if (l > u) return;
+    *t0 = b->start[by * b->nbx + l];
+    *t1 = b->start[by * b->nbx + u + 1];
 }
 
 void orc_density(int64_t n, const float* x, const float* y, const float* w,
@@ -299,9 +364,10 @@ void orc_density(int64_t n, const float* x, const float* y, const float* w,
         for (int64_t i = 0; i < n; i++)
             if (hs[i] > hmax) hmax = hs[i];
     }
-    bins_t b;
-    memset(&b, 0, sizeof(b));
-    if (!brute) bins_build(&b, n, x, y, 3.0 * (double)hmax);
+    sbins_t sb;
+    memset(&sb, 0, sizeof(sb));
+    if (!brute) sbins_build(&sb, n, x, y, w, ew, hs, h, (double)hmax);
+    const double reach = 3.0 * (double)hmax * (1.0 + 1e-6); /* 9h^2 uses the float square */
     int64_t total = 0;
 #pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 1) reduction(+ : total)
     for (int64_t rr = 0; rr < nr; rr++) {
@@ -327,65 +393,64 @@ void orc_density(int64_t n, const float* x, const float* y, const float* w,
                     }
                 }
             } else {
-                const double reach = 3.0 * (double)hmax * (1.0 + 1e-6); /* 9h^2 uses the float square */
-                int64_t bx0, bx1, by0, by1;
-                bin_span((double)cx - reach, (double)cx + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
-                bin_span((double)cy - reach, (double)cy + reach, b.y0, b.side, b.nby, &by0, &by1);
-                for (int64_t by = by0; by <= by1; by++)
-                    for (int64_t bx = bx0; bx <= bx1; bx++) {
-                        const int64_t k = by * b.nbx + bx;
-                        for (int64_t t = b.start[k]; t < b.start[k + 1]; t++) {
-                            const int64_t p = b.idx[t];
-                            const double h2 = orc_h2(hs ? hs[p] : h);
-                            const double d2 = d2_exact(x[p], y[p], cx, cy);
-                            if (d2 < kCut * h2) {
-                                den += kern(h2, d2) * (double)(w ? w[p] : 1.0f) * (ew ? ew[p] : 1.0);
-                                cnt++;
-                            }
+                int64_t by0, by1;
+                sbins_rows(&sb, (double)cy, reach, &by0, &by1);
+                for (int64_t by = by0; by <= by1; by++) {
+                    int64_t t0, t1;
+                    sbins_row_range(&sb, by, (double)cx, (double)cy, reach, &t0, &t1);
+                    for (int64_t t = t0; t < t1; t++) {
+                        const double h2 = sb.h2[t];
+                        const double d2 = d2_exact(sb.x[t], sb.y[t], cx, cy);
+                        if (d2 < kCut * h2) {
+                            den += kern(h2, d2) * sb.w[t] * sb.e[t];
+                            cnt++;
                         }
                     }
+                }
             }
             *o = den;
             total += cnt;
         }
     }
-    if (!brute) bins_free(&b);
+    if (!brute) sbins_free(&sb);
     if (evals) *evals = total;
 }
 
 double orc_loo_loglik(int64_t n, const float* x, const float* y, const float* w,
                       const double* ew, float h, double* out_loo, int64_t* evals) {
     const double h2 = orc_h2(h);
-    bins_t b;
-    bins_build(&b, n, x, y, 3.0 * (double)h);
-    double logl = 0.0;
+    sbins_t sb;
+    sbins_build(&sb, n, x, y, w, ew, NULL, h, (double)h);
+    const double reach = 3.0 * (double)h * (1.0 + 1e-6); /* 9h^2 uses the float square */
+    double* loo = (double*)malloc(sizeof(double) * (size_t)(n > 0 ? n : 1));
     int64_t total = 0;
-#pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 64) reduction(+ : logl, total)
+#pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 64) reduction(+ : total)
     for (int64_t j = 0; j < n; j++) {
-        const double reach = 3.0 * (double)h * (1.0 + 1e-6); /* 9h^2 uses the float square */
-        int64_t bx0, bx1, by0, by1;
-        bin_span((double)x[j] - reach, (double)x[j] + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
-        bin_span((double)y[j] - reach, (double)y[j] + reach, b.y0, b.side, b.nby, &by0, &by1);
+        int64_t by0, by1;
+        sbins_rows(&sb, (double)y[j], reach, &by0, &by1);
         double den = 0.0;
         int64_t cnt = 0;
-        for (int64_t by = by0; by <= by1; by++)
-            for (int64_t bx = bx0; bx <= bx1; bx++) {
-                const int64_t k = by * b.nbx + bx;
-                for (int64_t t = b.start[k]; t < b.start[k + 1]; t++) {
-                    const int64_t i = b.idx[t];
-                    if (i == j) continue;
-                    const double d2 = d2_exact(x[i], y[i], x[j], y[j]);
-                    if (d2 < kCut * h2) {
-                        den += kern(h2, d2) * (double)(w ? w[i] : 1.0f) * (ew ? ew[i] : 1.0);
-                        cnt++;
-                    }
+        for (int64_t by = by0; by <= by1; by++) {
+            int64_t t0, t1;
+            sbins_row_range(&sb, by, (double)x[j], (double)y[j], reach, &t0, &t1);
+            for (int64_t t = t0; t < t1; t++) {
+                if (sb.id[t] == j) continue;
+                const double d2 = d2_exact(sb.x[t], sb.y[t], x[j], y[j]);
+                if (d2 < kCut * h2) {
+                    den += kern(h2, d2) * sb.w[t] * sb.e[t];
+                    cnt++;
                 }
             }
-        if (out_loo) out_loo[j] = den;
-        logl += log(den > kEpsDensity ? den : kEpsDensity);
+        }
+        loo[j] = den;
         total += cnt;
     }
-    bins_free(&b);
+    /* the log sum in point order (reproducible for any thread count) */
+    double logl = 0.0;
+    for (int64_t j = 0; j < n; j++) logl += log(loo[j] > kEpsDensity ? loo[j] : kEpsDensity);
+    if (out_loo) memcpy(out_loo, loo, sizeof(double) * (size_t)n);
+    free(loo);
+    sbins_free(&sb);
     if (evals) *evals = total;
     return logl;
 }
@@ -439,35 +504,33 @@ void orc_point_density(int64_t n, const float* x, const float* y, const float* w
     if (hs)
         for (int64_t i = 0; i < n; i++)
             if (hs[i] > hmax) hmax = hs[i];
-    bins_t b;
-    bins_build(&b, n, x, y, 3.0 * (double)hmax * (1.0 + 1e-6));
+    sbins_t sb;
+    sbins_build(&sb, n, x, y, w, ew, hs, h, (double)hmax);
+    const double reach = 3.0 * (double)hmax * (1.0 + 1e-6);
     int64_t total = 0;
 #pragma omp parallel for num_threads(orc_get_threads()) schedule(dynamic, 64) reduction(+ : total)
     for (int64_t j = 0; j < n; j++) {
-        const double reach = 3.0 * (double)hmax * (1.0 + 1e-6);
-        int64_t bx0, bx1, by0, by1;
-        bin_span((double)x[j] - reach, (double)x[j] + reach, b.x0, b.side, b.nbx, &bx0, &bx1);
-        bin_span((double)y[j] - reach, (double)y[j] + reach, b.y0, b.side, b.nby, &by0, &by1);
+        int64_t by0, by1;
+        sbins_rows(&sb, (double)y[j], reach, &by0, &by1);
         double den = 0.0;
         int64_t cnt = 0;
-        for (int64_t by = by0; by <= by1; by++)
-            for (int64_t bx = bx0; bx <= bx1; bx++) {
-                const int64_t k = by * b.nbx + bx;
-                for (int64_t t = b.start[k]; t < b.start[k + 1]; t++) {
-                    const int64_t i = b.idx[t];
-                    if (i == j && !self) continue;
-                    const double h2 = orc_h2(hs ? hs[i] : h);
-                    const double d2 = d2_exact(x[i], y[i], x[j], y[j]);
-                    if (d2 < kCut * h2) {
-                        den += kern(h2, d2) * (double)(w ? w[i] : 1.0f) * (ew ? ew[i] : 1.0);
-                        cnt++;
-                    }
+        for (int64_t by = by0; by <= by1; by++) {
+            int64_t t0, t1;
+            sbins_row_range(&sb, by, (double)x[j], (double)y[j], reach, &t0, &t1);
+            for (int64_t t = t0; t < t1; t++) {
+                if (sb.id[t] == j && !self) continue;
+                const double h2 = sb.h2[t];
+                const double d2 = d2_exact(sb.x[t], sb.y[t], x[j], y[j]);
+                if (d2 < kCut * h2) {
+                    den += kern(h2, d2) * sb.w[t] * sb.e[t];
+                    cnt++;
                 }
             }
+        }
         out[j] = den;
         total += cnt;
     }
-    bins_free(&b);
+    sbins_free(&sb);
     if (evals) *evals = total;
 }
 

@@ -28,7 +28,10 @@ sys.path.insert(0, REPO)
 from mgpukde_tiled_b200 import synth, tiff  # noqa: E402
 
 REF_BIN = os.path.join(REPO, "oracle", "_ref", "mgkde_ref")
-REF_SAMPLE = "/root/reference/x64/Debug"
+# the reference checkout (read-only); REFERENCE_ROOT overrides the default
+# location, as oracle/ref_build.sh reads it
+REF_ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+REF_SAMPLE = os.path.join(REF_ROOT, "x64", "Debug")
 
 
 def ensure_ref():
@@ -151,6 +154,81 @@ def main(only=()):
         dg = synth.Grid(50, 50, 0.0, 0.0, 2.0)
         em = synth.rasterize_polygon(poly, eg)
         make_case("poly_h2", x, y, w, None, eg, em, dg, synth.rasterize_polygon(poly, dg), 2, True, True)
+
+
+    # 10-11: large coordinates (the single-large workload at about 1e4 units,
+    # the out-of-core one at about 4e4), where float coordinates have ulps of
+    # 2^-10 and 2^-8, with points placed at the 3h cutoff of cell centres.
+    if want("c1_crop_h50"):
+        large_coordinate_case("c1_crop_h50", xll=9870.0, yll=10050.0, ncols=160, nrows=128, h=50.0,
+                              edge_cs=4.0, n=3000, seed=51)
+    if want("c3_crop_h30"):
+        large_coordinate_case("c3_crop_h30", xll=39620.0, yll=40010.0, ncols=144, nrows=112, h=30.0,
+                              edge_cs=5.0, n=2500, seed=61)
+
+
+def near_cutoff_points(rng, cx, cy, h, k, tol):
+    """k float points each within tol (units) of distance 3h from one of the
+    given cell centres (exact distance of the float positions)."""
+    out = []
+    r3 = 3.0 * h
+    while len(out) < k:
+        i = int(rng.integers(len(cx)))
+        t = rng.uniform(0.0, 2.0 * np.pi)
+        r = r3 + rng.uniform(-tol, tol)
+        px, py = np.float32(cx[i] + r * np.cos(t)), np.float32(cy[i] + r * np.sin(t))
+        d = np.hypot(float(px) - float(cx[i]), float(py) - float(cy[i]))
+        if abs(d - r3) <= tol:
+            out.append((px, py))
+    return np.array(out, np.float32).reshape(-1, 2)
+
+
+def large_coordinate_case(name, xll, yll, ncols, nrows, h, edge_cs, n, seed):
+    """Mixture points (three Gaussians over the window and its 3h halo, plus
+    a uniform background) with lognormal weights around a density window at
+    large coordinates, under a star-polygon mask; edge mask at a coarser cell
+    over the window grown by 4h.  Added points: 64 within 1e-5 h of the 3h
+    cutoff from valid cell centres, 8 exactly on it (offsets of a 3-4-5
+    triangle scaled to 3h) and 8 one float step inside those."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    dg = synth.Grid(ncols, nrows, np.float32(xll), np.float32(yll), np.float32(1.0))
+    pad = 4.0 * h
+    ex0, ey0 = xll - pad, yll - pad
+    ecols, erows = int(np.ceil((ncols + 2 * pad) / edge_cs)), int(np.ceil((nrows + 2 * pad) / edge_cs))
+    eg = synth.Grid(ecols, erows, np.float32(ex0), np.float32(ey0), np.float32(edge_cs))
+    side = max(ecols, erows) * edge_cs
+    # centred off the window's centre, so that its edge crosses the window
+    poly = synth.star_polygon(side, seed + 1, rmin=0.12, rmax=0.3) + np.array([ex0 + 0.4 * ncols, ey0 - 0.35 * nrows])
+    dm, em = synth.rasterize_polygon(poly, dg), synth.rasterize_polygon(poly, eg)
+    # three clusters and a uniform background over the window grown by 3h
+    lo_x, hi_x, lo_y, hi_y = xll - 3 * h, xll + ncols + 3 * h, yll - 3 * h, yll + nrows + 3 * h
+    k = rng.integers(0, 3, n)
+    mx = rng.uniform(xll, xll + ncols, 3)
+    my = rng.uniform(yll, yll + nrows, 3)
+    sg = rng.uniform(0.8 * h, 2.4 * h, 3)
+    x = mx[k] + sg[k] * rng.standard_normal(n)
+    y = my[k] + sg[k] * rng.standard_normal(n)
+    nb = n // 8
+    x[:nb] = rng.uniform(lo_x, hi_x, nb)
+    y[:nb] = rng.uniform(lo_y, hi_y, nb)
+    x, y = x.astype(np.float32), y.astype(np.float32)
+    # cell centres as the reference forms them (double, stored to float)
+    rows, cols = np.nonzero(dm != dg.nodata)
+    ccx = (np.float64(dg.xll) + (cols + 0.5) * np.float64(dg.cs)).astype(np.float32).astype(np.float64)
+    ccy = (np.float64(dg.yll) + (dg.nrows - 0.5 - rows) * np.float64(dg.cs)).astype(np.float32).astype(np.float64)
+    near = near_cutoff_points(rng, ccx, ccy, h, 64, 1e-5 * h)
+    sel = rng.integers(0, len(ccx), 8)
+    sx = np.array([1, -1, 1, -1, 1, -1, 1, -1], np.float64)
+    sy = np.array([1, 1, -1, -1, 1, 1, -1, -1], np.float64)
+    a, b = 0.6 * 3 * h, 0.8 * 3 * h  # 3-4-5: a^2 + b^2 = 9 h^2 exactly
+    on_x = (ccx[sel] + sx * np.where(np.arange(8) < 4, a, b)).astype(np.float32)
+    on_y = (ccy[sel] + sy * np.where(np.arange(8) < 4, b, a)).astype(np.float32)
+    in_x = np.nextafter(on_x, ccx[sel].astype(np.float32))  # one float step towards the centre
+    x = np.concatenate([x, near[:, 0], on_x, in_x])
+    y = np.concatenate([y, near[:, 1], on_y, on_y])
+    w = rng.lognormal(0.0, 0.5, len(x)).astype(np.float32)
+    hpp = np.full(len(x), h, np.float32)
+    make_case(name, x, y, w, hpp, eg, em, dg, dm, -1, True, True)
 
 
 if __name__ == "__main__":

@@ -65,3 +65,81 @@ def test_density_roofline_fields():
     # no measured HBM figure, no traffic capture: the FP32 view alone / no traffic rate
     assert "hbm" not in bench.density_roofline(1e9, 0.01, 148, 1965.0, "fallback", None, 1, None)
     assert bench.density_roofline(1e9, 0.01, 148, 1965.0, "measured", None, 8, 6000.0)["hbm"]["traffic_gbs"] is None
+
+
+def _oracle_study(scale):
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+
+    import bench
+    import oracle_py as o
+
+    c = bench.build_workload("single_large", scale, seed=1)
+    eg = o.grid(*c["edge_grid"].astuple())
+    d2 = o.dist2_boundary(c["x"], c["y"], eg, o.mark_boundary(eg, c["edge_mask"]))
+    ew, eev = o.edge_weights(c["x"], c["y"], c["h"], d2, eg, c["edge_mask"])
+    den, dev = o.density(c["x"], c["y"], c["w"], ew, c["h"], o.grid(*c["density_grid"].astuple()),
+                         c["density_mask"])
+    return bench, np, c, den.astype(np.float32), dev, eev
+
+
+def test_whole_raster_accuracy_fields():
+    """The single-large accuracy leg on a 1/50-scale study: a raster equal to
+    the oracle's (rounded to float) passes, one with a cell moved by 1e-5
+    relative is reported, and the pair counts are compared."""
+    bench, np, c, den, dev, eev = _oracle_study(0.02)
+    valid = c["density_mask"] != c["density_grid"].nodata
+    bad = den.copy()
+    r, k = np.argwhere(valid)[len(np.argwhere(valid)) // 2]
+    bad[r, k] *= np.float32(1 + 1e-5)
+    a = bench.single_large_accuracy(c, {"step": den, "e2e": bad}, dev, eev + 1)
+    assert a["max_rel_err_step"] <= 1e-7 and 0.9e-5 < a["max_rel_err_e2e"] < 1.1e-5
+    assert a["max_rel_err"] == a["max_rel_err_e2e"] and a["nodata_cells_equal"]
+    assert a["density_evals_equal"] and not a["edge_evals_equal"]
+    assert a["cells"] == int(valid.sum()) and a["cells"] + a["nodata_cells"] == valid.size
+
+
+def test_argmax_check_fields():
+    """The bandwidth-selection argmax leg on a 1/20-scale study: given the
+    oracle's own logL (slightly perturbed) it finds the same argmax and
+    reports the margin to the runner-up."""
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+
+    import bench
+    import oracle_py as o
+    from mgpukde_tiled_b200 import synth
+
+    c = synth.bandwidth_select(scale=0.05, seed=2, nh=8)
+    eg = o.grid(*c["edge_grid"].astuple())
+    d2 = o.dist2_boundary(c["x"], c["y"], eg, o.mark_boundary(eg, c["edge_mask"]))
+    ll = np.array([o.loglik_at(c["x"], c["y"], c["w"], d2, eg, c["edge_mask"], float(h))[0] for h in c["hgrid"]])
+    best = int(np.argmax(ll))
+    a = bench.loo_argmax_check(c, c["hgrid"], ll * (1 + 1e-12), best)
+    assert a["argmax_equal"] and a["argmax_gpu"] == best and best in a["indices_checked"]
+    assert a["logl_max_rel_err"] < 1e-11
+    assert a["margin_gpu"] > 0 and a["margin_oracle"] > 0 and a["runner_up_gpu"] != best
+
+
+def test_out_of_core_accuracy_fields():
+    """The out-of-core accuracy leg on a 1/100-scale study (400^2 raster) in
+    tiles of 128: five tiles, the ragged corner one included."""
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(REPO, "oracle"))
+    import numpy as np
+
+    import bench
+    import oracle_py as o
+    from mgpukde_tiled_b200 import synth
+
+    c = synth.out_of_core(scale=0.01, seed=3)
+    dg = c["density_grid"]
+    eg = o.grid(*c["edge_grid"].astuple())
+    d2 = o.dist2_boundary(c["x"], c["y"], eg, o.mark_boundary(eg, c["edge_mask"]))
+    ew, _ = o.edge_weights(c["x"], c["y"], c["h"], d2, eg, c["edge_mask"])
+    den, _ = o.density(c["x"], c["y"], c["w"], ew, c["h"], o.grid(*dg.astuple()), None)
+    a = bench.out_of_core_accuracy(c, den.astype(np.float32), 128)
+    assert len(a["tiles"]) == 5 and a["tiles"][-1]["tile"] == [3, 3] and a["tiles"][-1]["cells"] == 16 * 16
+    assert a["max_rel_err"] <= 1e-7

@@ -13,12 +13,19 @@ REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CLI = os.path.join(REPO, "mgpukde_tiled_b200", "_lib", "mgkde_tiled")
 
 
-def write_case_files(d, case):
+def write_case_files(d, case, with_h=False):
+    """The case's points CSV (x,y,w; or x,y,h,w with the per-point bandwidth
+    column that h_option -1 reads) and its two masks as GeoTIFFs."""
     g = load(case)
     with open(os.path.join(d, "p.csv"), "w") as f:
-        f.write("x,y,w\n")
-        for a, b, w in zip(g["x"], g["y"], g["w"]):
-            f.write("%.9g,%.9g,%.9g\n" % (a, b, w))
+        if with_h:
+            f.write("x,y,h,w\n")
+            for a, b, hh, w in zip(g["x"], g["y"], g["h_pp"], g["w"]):
+                f.write("%.9g,%.9g,%.9g,%.9g\n" % (a, b, hh, w))
+        else:
+            f.write("x,y,w\n")
+            for a, b, w in zip(g["x"], g["y"], g["w"]):
+                f.write("%.9g,%.9g,%.9g\n" % (a, b, w))
     for name, grid, mask in (("e.tif", g["eg"], g["edge_mask"]), ("d.tif", g["dg"], g["density_mask"])):
         gt = (float(grid.xll), float(grid.cs), 0.0, float(grid.yll) + grid.nrows * float(grid.cs), 0.0,
               -float(grid.cs))

@@ -38,6 +38,33 @@ def test_cli_mode1_matches_oracle(tmp_path, case, hopt):
         assert np.all(np.abs(pts[:, 2] - ref["hs"]) <= 6e-7 + 4e-7 * np.abs(ref["hs"]))
 
 
+@pytest.mark.parametrize("case", ["poly_varh", "uniform_c0"])
+def test_cli_per_point_bandwidths_match_oracle(tmp_path, case):
+    """h_option -1: the bandwidths come from the CSV's h column (the
+    reference reads it at kde_cuda_kdtr_tiled.cu:413-421), with sample
+    weights and edge correction on.  The density GeoTIFF and pntsCUDA.csv
+    (x, y, h, edge weight in input order; written at :1857-1870) agree with
+    the FP64 oracle run of the same case."""
+    g = write_case_files(str(tmp_path), case, with_h=True)
+    ref = oracle_run(g)
+    p = subprocess.run([CLI] + "1 p.csv e.tif d.tif -1 1 1 1 0 1 1 a.tif b.tif 0 --tile=64".split(),
+                       cwd=tmp_path, capture_output=True, text=True, timeout=600)
+    assert p.returncode == 0, p.stdout[-2000:]
+    den = tiff.read(str(tmp_path / "b.tif")).data
+    nd = g["density_mask"] == g["dg"].nodata
+    assert np.array_equal(den[nd], g["density_mask"][nd])
+    rel = np.abs(den[~nd] - ref["density"][~nd]) / np.maximum(np.abs(ref["density"][~nd]), 1e-300)
+    assert rel.max() <= 1e-6, rel.max()
+    pts = np.loadtxt(str(tmp_path / "pntsCUDA.csv"), delimiter=",", skiprows=1, ndmin=2)
+    assert pts.shape == (len(g["x"]), 4)
+    # printed with 6 decimals, input order
+    assert np.all(np.abs(pts[:, 0] - g["x"]) <= 6e-7 + 1e-7 * np.abs(g["x"]))
+    assert np.all(np.abs(pts[:, 1] - g["y"]) <= 6e-7 + 1e-7 * np.abs(g["y"]))
+    assert np.all(np.abs(pts[:, 2] - g["h_pp"]) <= 6e-7)
+    assert np.all(np.abs(pts[:, 3] - ref["ew"]) <= 6e-7 + 3e-6 * np.abs(ref["ew"]))
+    assert np.array_equal(pts[:, 3] == 1.0, ref["ew"] == 1.0)
+
+
 def test_cli_mode0_runs(tmp_path):
     p = subprocess.run([CLI] + "0 2000 1.0 0.5 0 1 0 1 0 1 1 a.tif b.tif 0".split(), cwd=tmp_path,
                        capture_output=True, text=True, timeout=600)

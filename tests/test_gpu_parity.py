@@ -80,6 +80,27 @@ def test_golden_case_components(ctx, case):
         assert r["edge_evals"] == ref["edge_evals"]
 
 
+@pytest.mark.parametrize("case", ["c1_crop_h50", "c3_crop_h30"])
+def test_large_coordinates_fixed_h(ctx, case):
+    """The fixed-h kernels (one bandwidth for all points) at coordinates of
+    about 1e4 and 4e4 units, with points on and within 1e-5 h of the 3h
+    cutoff of cell centres; the fixtures' per-point h are all that h, so the
+    oracle's answer is the same."""
+    d = load(case)
+    ref = oracle_run(d)
+    h = float(d["h_pp"][0])
+    assert np.all(d["h_pp"] == np.float32(h))
+    r = run_components(ctx, dict(d, hs=None), h)
+    nd = d["density_mask"] == d["dg"].nodata
+    assert np.array_equal(r["density"][nd], d["density_mask"][nd])
+    assert rel_err(r["density"][~nd], ref["density"][~nd]).max() <= RTOL
+    assert r["density_evals"] == ref["density_evals"]
+    assert np.array_equal(r["dist2"], ref["dist2"])
+    assert np.array_equal(r["ew"] == 1.0, ref["ew"] == 1.0)
+    assert rel_err(r["ew"], ref["ew"]).max() <= RTOL
+    assert r["edge_evals"] == ref["edge_evals"]
+
+
 @pytest.mark.parametrize("case", ["uniform_c0", "poly_fixed", "poly_varh"])
 def test_golden_case_end_to_end(ctx, case):
     """mgk_kde_raster from host buffers, tiled into odd tile sizes."""

@@ -19,7 +19,7 @@ def runs():
 
 def test_cases_present():
     assert {"redwood_h0", "redwood_h1", "uniform_c0", "poly_fixed", "poly_varh",
-            "uniform_h0_noedge", "loo_h1", "redwood_h2", "poly_h2"} <= set(CASES)
+            "uniform_h0_noedge", "loo_h1", "redwood_h2", "poly_h2", "c1_crop_h50", "c3_crop_h30"} <= set(CASES)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -103,3 +103,69 @@ def test_adaptive_likelihood_is_the_loo_of_the_pilot_bandwidths():
     ew2, _ = o.edge_weights(x, y, 0.0, d2, eg, em, hs=hs)
     den1, _ = o.point_density(x, y, w, ew2, 0.0, hs=hs, self_term=False)
     assert abs(ll - np.sum(np.log(np.maximum(den1, float(np.float32(1e-14)))))) <= 1e-9 * abs(ll)
+
+
+def cutoff_rule_disagreements(x, y, hs, g, mask):
+    """Pairs (point, valid cell of g) that the oracle's cutoff test and the
+    reference's classify differently.  The oracle forms dx = x_cell - x_p
+    exactly in double; the reference's Distance2 (kde_cuda_kdtr_tiled.cu:50-55)
+    subtracts the two floats in float and widens the rounded difference.
+    Both then test dx^2 + dy^2 < 9 h^2 in double with h^2 a float product.
+    Returns (disagreements, pairs within 3h + one cell of each other, those
+    of the pairs whose float dx or dy was rounded)."""
+    nd = g.nodata
+    diff = 0
+    pairs = 0
+    rounded = 0
+    cs = np.float64(g.cs)
+    for px, py, hp in zip(x, y, hs):
+        h2 = np.float64(np.float32(hp) * np.float32(hp))
+        reach = 3.0 * float(hp) + float(cs)
+        c0 = max(0, int(np.floor((float(px) - reach - float(g.xll)) / float(cs))))
+        c1 = min(g.ncols - 1, int(np.ceil((float(px) + reach - float(g.xll)) / float(cs))))
+        r0 = max(0, int(np.floor(g.nrows - 0.5 - (float(py) + reach - float(g.yll)) / float(cs))))
+        r1 = min(g.nrows - 1, int(np.ceil(g.nrows - 0.5 - (float(py) - reach - float(g.yll)) / float(cs))))
+        if c0 > c1 or r0 > r1:
+            continue
+        cols = np.arange(c0, c1 + 1)
+        rows = np.arange(r0, r1 + 1)
+        cx = (np.float64(g.xll) + (cols + 0.5) * cs).astype(np.float32)
+        cy = (np.float64(g.yll) + (g.nrows - 0.5 - rows) * cs).astype(np.float32)
+        ok = mask[r0:r1 + 1, c0:c1 + 1] != nd
+        dxe = cx.astype(np.float64) - np.float64(px)
+        dye = cy.astype(np.float64) - np.float64(py)
+        dxr = (cx - np.float32(px)).astype(np.float64)
+        dyr = (cy - np.float32(py)).astype(np.float64)
+        ine = (dxe[None, :] ** 2 + dye[:, None] ** 2) < 9.0 * h2
+        inr = (dxr[None, :] ** 2 + dyr[:, None] ** 2) < 9.0 * h2
+        diff += int(np.count_nonzero((ine != inr) & ok))
+        pairs += int(np.count_nonzero(ok))
+        rounded += int(np.count_nonzero(((dxe != dxr)[None, :] | (dye != dyr)[:, None]) & ok))
+    return diff, pairs, rounded
+
+
+@pytest.mark.parametrize("case", CASES)
+def test_cutoff_rules_agree_on_every_fixture(runs, case):
+    """The oracle's exact dx and the reference's float-rounded dx classify
+    every (point, cell) pair of the fixtures the same way.  Float subtraction
+    of two floats within a factor of two of each other is exact (Sterbenz),
+    so the rules can differ only for pairs whose difference exceeds one of
+    the two coordinates, i.e. near the coordinate origin; the counts here
+    cover the density and the edge-mask rasters with each case's bandwidths.
+    At the large coordinates of the c1/c3 crops no float difference rounds at
+    all (the two rules see the same d^2); near the origin of the small cases
+    with cells within 3h of it many do, and none of those flips a cutoff
+    decision."""
+    d, r = runs[case]
+    x, y = d["x"], d["y"]
+    hs = r.get("hs") if r.get("hs") is not None else d["hs"]
+    if hs is None:
+        hs = np.full(len(x), r["h"], np.float32)
+    dd, dp, dr = cutoff_rule_disagreements(x, y, hs, d["dg"], d["density_mask"])
+    ed, ep, er = cutoff_rule_disagreements(x, y, hs, d["eg"], d["edge_mask"]) if int(d["edge"]) else (0, 0, 0)
+    assert dp > 0
+    assert dd == 0 and ed == 0, (case, dd, dp, ed, ep)
+    if case.startswith(("c1_", "c3_")):
+        assert dr == 0 and er == 0, (case, dr, er)
+    elif case in ("poly_fixed", "uniform_c0", "redwood_h0"):  # cells within 3h of the origin
+        assert dr + er > 0, case
