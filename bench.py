@@ -16,9 +16,12 @@ over the full raster.  Unit of work = one kernel evaluation, i.e. one
 valid edge-mask cell; the count is algorithmic (the kernels count exactly the
 oracle's pairs).  value = evals of all ranks / max-over-ranks step time.
 
-Multi-GPU (torchrun): the path shards by tiles with no exchange; rank r runs
-its own tile band of the study (a workload with seed 1 + r), so per-GPU work
-is fixed (weak scaling) and no collective touches the data path.
+Multi-GPU (torchrun): one study is split into contiguous row ranges of
+balanced work, one per rank; a rank keeps the points within 3h of its rows
+and computes their boundary distances, edge weights, index and density (no
+collective touches the data path; strong scaling).  The bandwidth-selection
+workload splits its edge weights by points (all-gather) and its
+leave-one-out sums by queries (all-reduce of the nh partial sums).
 
 --impl reference times the reference program's own CPU path (built from its
 sources into oracle/_ref; the FP64 oracle port if that binary is absent) on
@@ -408,10 +411,12 @@ def run_reference_arm(args):
 
 
 def config_of(args):
+    split = ("whole raster (one tile)" if args.gpus <= 1 else
+             f"one study split into {args.gpus} row ranges of balanced work, one per GPU (no exchange)")
     return {"workload": f"{args.workload}: 1e6 mixture points (50 comps) in 1e4^2, lognormal weights, "
                         f"density 1e4^2 @ cell 1 polygon mask, edge mask 2500^2 @ cell 4, h=50"
                         + ("" if args.scale == 1.0 else f" (scaled x{args.scale})"),
-            "scale": args.scale, "tile": "whole raster (one tile)", "parallelism": f"tiles x{args.gpus} (no exchange)",
+            "scale": args.scale, "tile": split, "parallelism": f"rows x{args.gpus} (no exchange)",
             "l2": "inputs larger than L2 (density mask and output 400 MB each)",
             "host_numa_node": getattr(args, "numa_node", None)}
 
@@ -423,13 +428,24 @@ def run_mgk(args):
 
     import mgpukde_tiled_b200 as mk
 
+    from mgpukde_tiled_b200 import shard
+
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
-    c = build_workload(args.workload, args.scale, seed=1 + rank)
+    # one study; with N ranks each takes a contiguous range of rows of balanced work
+    c = build_workload(args.workload, args.scale, seed=1)
     dg, eg = mk.Grid.of(c["density_grid"]), mk.Grid.of(c["edge_grid"])
     h = float(c["h"])
+    row0, nrows = 0, dg.nrows
+    if world > 1:
+        row0, nrows = shard.split_rows(dg.nrows, world, shard.row_costs(c["x"], c["y"], h, c["density_grid"],
+                                                                         c["density_mask"]))[rank]
+    # the rows' halo: points within 3h of their cell centres (mgk_kde_raster_rows keeps the same)
+    reach = 3.0 * h * (1.0 + 1e-6) + 1e-6 * float(dg.cs)
+    y_top = float(np.float32(float(dg.yll) + (dg.nrows - 0.5 - row0) * float(dg.cs)))
+    y_bot = float(np.float32(float(dg.yll) + (dg.nrows - 0.5 - (row0 + max(nrows, 1) - 1)) * float(dg.cs)))
     stream = torch.cuda.current_stream()
     ctx = mk.Context(local, stream=stream)
     dev = "cuda"
@@ -438,20 +454,29 @@ def run_mgk(args):
     dw = torch.from_numpy(c["w"]).to(dev)
     demask = torch.from_numpy(c["edge_mask"]).to(dev)
     ddmask = torch.from_numpy(c["density_mask"]).to(dev)
-    dout = torch.empty((dg.nrows, dg.ncols), dtype=torch.float32, device=dev)
+    dout = torch.empty((max(nrows, 1), dg.ncols), dtype=torch.float32, device=dev)
     pts = mk.Points.wrap(ctx, dx, dy, dw)
     em = mk.Raster.wrap(ctx, eg, demask)
 
     def step(count=False):
         mk.mark_boundary(ctx, em)
-        mk.calc_dist2_boundary(ctx, pts, em)
-        ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=count)
-        idx = mk.Index(ctx, pts, h)
-        ev_d = mk.density_tile(ctx, idx, dg, 0, 0, dg.nrows, dg.ncols, ddmask, dout, count=count)
+        p = pts if world == 1 else pts.select(ylo=y_bot - reach, yhi=y_top + reach)
+        mk.calc_dist2_boundary(ctx, p, em)
+        ev_e = mk.edge_correction_weights(ctx, p, em, h, count=count)
+        idx = mk.Index(ctx, p, h)
+        ev_d = (mk.density_tile(ctx, idx, dg, row0, 0, nrows, dg.ncols, ddmask[row0:row0 + nrows], dout,
+                                count=count) if nrows else 0)
         idx.close()
+        if p is not pts:
+            p.close()
         return ev_e, ev_d
 
     ev_e, ev_d = step(count=True)
+    if world > 1:
+        # the study's units: its density pairs (the ranks' rows partition them) and
+        # its edge-correction pairs counted once (halo points repeat across ranks)
+        mk.calc_dist2_boundary(ctx, pts, em)
+        ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=True)
     evals = ev_e + ev_d
     for _ in range(args.warmup):
         step()
@@ -481,10 +506,10 @@ def run_mgk(args):
     # the last timed step's raster, for the whole-raster accuracy check
     step_raster = dout.cpu().numpy() if (rank == 0 and world == 1 and not args.no_accuracy) else None
     total_evals = evals
-    if world > 1:  # each rank ran its own study: the job's evals are the sum over ranks
-        ev_t = torch.tensor([float(evals)], device=dev, dtype=torch.float64)
+    if world > 1:  # the study's evals: every rank's density pairs plus the edge pairs once
+        ev_t = torch.tensor([float(ev_d)], device=dev, dtype=torch.float64)
         dist.all_reduce(ev_t, op=dist.ReduceOp.SUM)
-        total_evals = int(ev_t.item())
+        total_evals = int(ev_t.item()) + ev_e
     value = total_evals / (ms_max / 1e3)
 
     # end to end: the C ABI from pinned host buffers (inputs H2D and the raster D2H every step)
@@ -493,12 +518,16 @@ def run_mgk(args):
     hw = torch.from_numpy(c["w"]).pin_memory()
     hem = torch.from_numpy(c["edge_mask"]).pin_memory()
     hdm = torch.from_numpy(c["density_mask"]).pin_memory()
-    hout = torch.empty((dg.nrows, dg.ncols), dtype=torch.float32).pin_memory()
+    hout = torch.empty((max(nrows, 1), dg.ncols), dtype=torch.float32).pin_memory()
     e2e_steps = max(1, min(args.steps, 5))
 
     def e2e_step():
-        mk.kde_raster(ctx, hx.numpy(), hy.numpy(), hw.numpy(), h, dg, hdm.numpy(), eg, hem.numpy(),
-                      out=hout.numpy())
+        if world == 1:
+            mk.kde_raster(ctx, hx.numpy(), hy.numpy(), hw.numpy(), h, dg, hdm.numpy(), eg, hem.numpy(),
+                          out=hout.numpy())
+        elif nrows:
+            mk.kde_raster_rows(ctx, hx.numpy(), hy.numpy(), hw.numpy(), h, dg, row0, nrows,
+                               hdm.numpy()[row0:row0 + nrows], eg, hem.numpy(), out=hout.numpy())
 
     e2e_step()
     torch.cuda.synchronize()
@@ -513,12 +542,13 @@ def run_mgk(args):
     if world > 1:
         dist.all_reduce(e2e_ms, op=dist.ReduceOp.MAX)
     e2e_val = total_evals / (float(e2e_ms.item()) / 1e3)
-    h2d = 4 * (3 * len(c["x"]) + c["edge_mask"].size + c["density_mask"].size)
+    # bytes of the whole job (every rank uploads all points and the edge mask, and its own rows)
+    h2d = 4 * (world * (3 * len(c["x"]) + c["edge_mask"].size) + c["density_mask"].size)
     d2h = 4 * dg.nrows * dg.ncols
 
     # the plain FP64 GPU form of the density gather on the same raster (one launch, after warm-up)
     fp64_form = None
-    if not args.no_fp64_form:
+    if not args.no_fp64_form and world == 1:
         idx = mk.Index(ctx, pts, h)
         mk.density_tile(ctx, idx, dg, 0, 0, dg.nrows, dg.ncols, ddmask, dout, fp64=True)
         f64_ms = []
@@ -546,9 +576,11 @@ def run_mgk(args):
                     traffic = int(line.split(":", 1)[1].split()[0])
     out = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+        "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True,
+        "scaling": "strong",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)", "config": config_of(args),
-        "evals_per_step_per_gpu": evals, "density_evals": ev_d, "edge_evals": ev_e,
+        "evals_per_step": total_evals, "density_evals": total_evals - ev_e, "edge_evals": ev_e,
+        "rows": [int(row0), int(nrows)] if world > 1 else None,
         "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
                 "ms_per_step": float(e2e_ms.item())},
         "gpu_launches": launches,
@@ -644,13 +676,15 @@ def run_bandwidth_select(args):
     h in [5, 500] and the argmax, in one graph launch.  Evals = edge-mask
     cells plus point pairs inside the cutoff, summed over the 64 h."""
     import torch
+    import torch.distributed as dist
 
     import mgpukde_tiled_b200 as mk
+    from mgpukde_tiled_b200 import shard
 
     rank, world, local = env_rank()
-    if world > 1:
-        raise SystemExit("bandwidth_select runs on one GPU (replicas only)")
     torch.cuda.set_device(local)
+    if world > 1:  # one selection split over the ranks (edge weights by points, queries by groups)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=300))
     c = synth.bandwidth_select(scale=args.scale, seed=2, nh=64)
     eg = mk.Grid.of(c["edge_grid"])
     stream = torch.cuda.current_stream()
@@ -661,23 +695,37 @@ def run_bandwidth_select(args):
     demask = torch.from_numpy(c["edge_mask"]).cuda()
     pts = mk.Points.wrap(ctx, dx, dy, dw)
     em = mk.Raster.wrap(ctx, eg, demask)
+    mk.mark_boundary(ctx, em)
     hgrid = c["hgrid"]
+    shared_ev = [0, 0]
 
     def step():
         mk.calc_dist2_boundary(ctx, pts, em)
-        return mk.log_likelihood_batch(ctx, pts, em, hgrid)
+        if world == 1:
+            return mk.log_likelihood_batch(ctx, pts, em, hgrid)
+        tot, am, ev = shard.loo_loglik_shared(ctx, pts, em, hgrid, rank, world)
+        shared_ev[:] = ev
+        return tot, am
 
     logl, best = step()
-    ev_edge, ev_loo = ctx.last_loo_evals
+    if world == 1:
+        ev_edge, ev_loo = ctx.last_loo_evals
+    else:  # the shares partition both counts: sum them over ranks
+        t = torch.tensor([float(v) for v in shared_ev], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        ev_edge, ev_loo = int(t[0].item()), int(t[1].item())
     evals = ev_edge + ev_loo
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
     sampler = ClockSampler(local)
     sampler.start()
     l0 = ctx.kernel_launches
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     loo_ms, batch_ms = [], []
+    torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(args.steps):
         step()
@@ -686,26 +734,38 @@ def run_bandwidth_select(args):
     torch.cuda.synchronize()
     clocks = sampler.stop()
     ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
     launches = (ctx.kernel_launches - l0) / args.steps
-    out = {"metric": METRIC, "value": evals / (ms / 1e3), "unit": UNIT, "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+    out = {"metric": METRIC, "value": evals / (ms / 1e3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded PCG64)",
            "config": {"workload": f"bandwidth_select: {len(c['x'])} mixture points (20 comps) in "
                                   f"{c['edge_grid'].ncols * 4}^2, unit weights, edge mask "
                                   f"{c['edge_grid'].ncols}^2 @ cell 4, 64 log-spaced h in [5, 500]",
-                      "scale": args.scale, "l2": "per-h edge weights and point records stay L2-resident"},
+                      "scale": args.scale, "l2": "per-h edge weights and point records stay L2-resident",
+                      "parallelism": ("one GPU" if world == 1 else
+                                      f"one selection over {world} GPUs: edge weights by point share + "
+                                      f"all-gather, leave-one-out sums by query share + all-reduce")},
            "evals_per_step": evals, "edge_evals": ev_edge, "loo_evals": ev_loo,
            "batch_ms": float(np.mean(loo_ms)), "argmax": best, "h_best": float(hgrid[best]),
            "gpu_launches": launches, "clocks": clocks}
-    unbind_numa()
-    if not args.no_cpu_baseline:
-        out["cpu_baseline"], out["accuracy"] = loo_cpu_check(c, hgrid, logl, pts)
-    if not args.no_accuracy:
-        out.setdefault("accuracy", {})["argmax"] = loo_argmax_check(c, hgrid, logl, best)
-    print(json.dumps(out))
+    if rank == 0:
+        if world == 1:
+            unbind_numa()
+            if not args.no_cpu_baseline:
+                out["cpu_baseline"], out["accuracy"] = loo_cpu_check(c, hgrid, logl, pts)
+            if not args.no_accuracy:
+                out.setdefault("accuracy", {})["argmax"] = loo_argmax_check(c, hgrid, logl, best)
+        print(json.dumps(out))
     pts.close()
     em.close()
     ctx.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 

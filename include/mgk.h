@@ -100,6 +100,18 @@ int mgk_points_upload(mgk_ctx* ctx, int64_t n, const float* x, const float* y,
 int mgk_points_wrap(mgk_ctx* ctx, int64_t n, const float* d_x, const float* d_y,
                     const float* d_w, const float* d_h, mgk_points** out);
 int mgk_points_destroy(mgk_points* pts);
+/* The points of src inside [xlo, xhi] x [ylo, yhi], in their input order, as
+ * a new device point set (x, y and, when src has them, w and per-point h;
+ * boundary distances and edge weights are computed afresh on it).  It is the
+ * device form of the reference's halo filter ExtractSamplePointsCurTile
+ * (kde_cuda_kdtr_tiled.cu:4672-4747): a rank of a multi-GPU study keeps the
+ * points within 3h of its rows, whose densities need no others.  One read
+ * back of the count synchronises the context stream. */
+int mgk_points_select(mgk_ctx* ctx, const mgk_points* src, double xlo, double xhi, double ylo, double yhi,
+                      mgk_points** out);
+/* Number of points of a point set (NULL: 0).  No reference counterpart (the
+ * reference reads SamplePoints.numberOfPoints). */
+int64_t mgk_points_size(const mgk_points* pts);
 /* Device pointers of a point set (any may be NULL on output when absent):
  * x, y, w, h (float), dist2 (double, squared distance to the boundary),
  * ew (float, edge-correction weight). */
@@ -249,6 +261,31 @@ int mgk_copy_sink(void* target, int64_t tile, int64_t row0, int64_t col0, int64_
  * of the largest logL. */
 int mgk_loo_loglik_batch(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask,
                          const float* h_grid, int nh, double* logL, int* argmax);
+/* Multi-GPU form of mgk_loo_loglik_batch, one process per GPU.  The
+ * reference's LogLikelihood splits the points over its GPUs (each GPU
+ * computes the edge weights of Points[i].start..end and the densities they
+ * scatter) and merges through host memory (ReformECWeights,
+ * ReformGPUDensities, ReductionSumGPU; kde_cuda_kdtr_tiled.cu:3223-3297).
+ * Here rank `part` of `nparts` (c = ceil(n / nparts)):
+ *  1. mgk_loo_share_edge_weights: e_i(h_k) of its points
+ *     [part c, min(n, (part + 1) c)) for every h of h_grid, into its chunk of
+ *     d_ew_all (device, nparts * nh * c floats; chunk `part` holds nh rows of
+ *     c floats: e of point part c + j at h_k is d_ew_all[part nh c + k c + j]).
+ *     Needs mgk_boundary_dist.  The caller then all-gathers the chunks (one
+ *     ncclAllGather of nh c floats per rank, in place).
+ *  2. mgk_loo_share_loglik: for every h_k, the FP64 sum of
+ *     log(max(loo_j(h_k), 1e-14f)) over this rank's share of the queries
+ *     (every point is a source): the query groups
+ *     [part G / nparts, (part + 1) G / nparts) of h_k's index, G = ceil(n / 128)
+ *     groups of 128 points in Z-order of the index bins.  d_ew_all: the
+ *     gathered edge weights, or NULL without edge correction.  The shares of
+ *     parts 0 .. nparts-1 cover every query exactly once per h, so the sum of
+ *     partial_logL over ranks (one all-reduce of nh doubles) is logL(h); its
+ *     argmax is the bandwidth.  evals (optional): this share's pair count. */
+int mgk_loo_share_edge_weights(mgk_ctx* ctx, mgk_points* pts, const mgk_raster* mask, const float* h_grid,
+                               int nh, int part, int nparts, float* d_ew_all, int64_t* evals);
+int mgk_loo_share_loglik(mgk_ctx* ctx, mgk_points* pts, const float* h_grid, int nh, int part, int nparts,
+                         const float* d_ew_all, double* partial_logL, int64_t* evals);
 /* MLE_FixedBandWidth (kde_cuda_kdtr_tiled.cu:3044-3093): golden-section
  * search on [h0/20, 2 h0], at most 30 iterations, two logL evaluations per
  * iteration (each one batched launch of nh=2); returns the bracket midpoint. */
@@ -363,6 +400,21 @@ int mgk_kde_raster(mgk_ctx* ctx, int64_t n, const float* x, const float* y, cons
                    const float* h_pp, float h, int edge_correction, const mgk_grid* edge_g,
                    const float* edge_mask, const mgk_grid* dens_g, const float* dens_mask,
                    int64_t tile_side, float* out_density, float* out_ew, int64_t* evals);
+/* The same path for rows [row0, row0 + nrows) of dens_g only: one rank's
+ * share of a study split over GPUs by rows, with no exchange between ranks
+ * (the densities of these rows need only the points within 3h of them).
+ * The reference splits the points instead and sums whole tiles from every GPU
+ * through host memory (kde_cuda_kdtr_tiled.cu:1320-1351, ReformGPUAsciiRaster
+ * :2468-2567).  All n points are passed; after the upload only those within
+ * 3 h_max of the rows are kept (mgk_points_select), so the boundary
+ * distances, edge weights and index cover only them.  dens_mask_rows and
+ * out_rows: host, nrows x ncols, the rows' part of the raster.  evals
+ * (optional): the rows' density pairs plus the edge-correction pairs of the
+ * kept points. */
+int mgk_kde_raster_rows(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* w,
+                        const float* h_pp, float h, int edge_correction, const mgk_grid* edge_g,
+                        const float* edge_mask, const mgk_grid* dens_g, int64_t row0, int64_t nrows,
+                        const float* dens_mask_rows, int64_t tile_side, float* out_rows, int64_t* evals);
 
 #ifdef __cplusplus
 }

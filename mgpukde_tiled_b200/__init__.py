@@ -10,7 +10,8 @@ from ._native import EXPORTS, LIB_PATH, MgkError, MgkGrid, lib  # noqa: F401
 from .kde import (Context, Grid, Index, Points, Raster, autotune, calc_dist2_boundary, density_tile,  # noqa: F401
                   get_tuning, set_tuning,
                   density_stream, density_tiles, edge_correction_weights, kde_raster, log_likelihood_batch, mark_boundary,
-                  mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights, loglik_adaptive, adaptive_bandwidths)
+                  mle_fixed_bandwidth, rule_of_thumb, unit_edge_weights, loglik_adaptive, adaptive_bandwidths,
+                  kde_raster_rows, loo_share_edge_weights, loo_share_loglik)
 from .serve import Server  # noqa: F401
 
 __all__ = [
@@ -18,4 +19,5 @@ __all__ = [
     "density_stream", "density_tiles", "autotune", "get_tuning", "set_tuning",
     "edge_correction_weights", "kde_raster", "log_likelihood_batch", "mark_boundary",
     "mle_fixed_bandwidth", "rule_of_thumb", "unit_edge_weights", "loglik_adaptive", "adaptive_bandwidths", "lib",
+    "kde_raster_rows", "loo_share_edge_weights", "loo_share_loglik",
 ]

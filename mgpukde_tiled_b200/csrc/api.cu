@@ -276,6 +276,44 @@ int mgk_points_wrap(mgk_ctx* c, int64_t n, const float* d_x, const float* d_y, c
     return MGK_OK;
 }
 
+int64_t mgk_points_size(const mgk_points* p) { return p ? p->n : 0; }
+
+int mgk_points_select(mgk_ctx* c, const mgk_points* src, double xlo, double xhi, double ylo, double yhi,
+                      mgk_points** out) {
+    if (!c || !src || !out || !(xlo <= xhi) || !(ylo <= yhi))
+        return mgk_fail(c, MGK_ERR_INVALID, "points_select: bad arguments");
+    *out = nullptr;
+    const size_t bs = sizeof(unsigned) * (size_t)mgk_points_select_scratch(src->n);
+    unsigned* scr = nullptr;
+    int st = mgk_alloc(c, (void**)&scr, bs);
+    if (st) return st;
+    int64_t m = 0;
+    st = mgk_launch_points_select(c, src, xlo, xhi, ylo, yhi, scr, &m, nullptr);
+    mgk_points* p = nullptr;
+    if (st == MGK_OK) {
+        p = new (std::nothrow) mgk_points();
+        if (!p) st = MGK_ERR_INVALID;
+    }
+    if (st == MGK_OK) {
+        p->ctx = c;
+        p->n = m;
+        p->owns_xywh = true;
+        const size_t b = sizeof(float) * (size_t)std::max<int64_t>(m, 1);
+        if ((st = mgk_alloc(c, (void**)&p->x, b)) == MGK_OK && (st = mgk_alloc(c, (void**)&p->y, b)) == MGK_OK &&
+            (!src->w || (st = mgk_alloc(c, (void**)&p->w, b)) == MGK_OK) &&
+            (!src->h || (st = mgk_alloc(c, (void**)&p->h, b)) == MGK_OK))
+            st = points_alloc_results(c, p);
+        if (st == MGK_OK) st = mgk_launch_points_select(c, src, xlo, xhi, ylo, yhi, scr, &m, p);
+    }
+    mgk_free(c, scr, bs);  // stream-ordered reuse: later users run after the scatter
+    if (st) {
+        mgk_points_destroy(p);
+        return st;
+    }
+    *out = p;
+    return MGK_OK;
+}
+
 int mgk_points_destroy(mgk_points* p) {
     if (!p) return MGK_OK;
     mgk_ctx* c = p->ctx;
@@ -578,6 +616,52 @@ int mgk_loo_loglik_batch(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const f
     return st;
 }
 
+// ---------------------------------------------- multi-GPU bandwidth selection --
+static inline int64_t share_chunk(int64_t n, int nparts) { return (n + nparts - 1) / nparts; }
+
+int mgk_loo_share_edge_weights(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const float* h_grid, int nh,
+                               int part, int nparts, float* d_ew_all, int64_t* evals) {
+    if (!c || !p || !r || !h_grid || nh <= 0 || !d_ew_all || nparts <= 0 || part < 0 || part >= nparts)
+        return mgk_fail(c, MGK_ERR_INVALID, "loo_share_edge_weights: bad arguments");
+    if (!p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
+    float lo, hi;
+    int st = check_bandwidths(c, h_grid, nh, &lo, &hi);
+    if (st) return st;
+    const int64_t ch = share_chunk(p->n, nparts);
+    const int64_t p0 = std::min<int64_t>(p->n, (int64_t)part * ch), p1 = std::min<int64_t>(p->n, p0 + ch);
+    float* d_h = nullptr;
+    if ((st = mgk_alloc(c, (void**)&d_h, sizeof(float) * nh))) return st;
+    cudaError_t ce = cudaMemcpyAsync(d_h, h_grid, sizeof(float) * nh, cudaMemcpyHostToDevice, c->stream);
+    if (ce == cudaSuccess && evals) ce = cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream);
+    if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "loo_share_edge_weights");
+    if (st == MGK_OK && p1 > p0)
+        st = mgk_launch_edge_weights_multi(c, p1 - p0, p->x + p0, p->y + p0, nullptr, 0.0f, d_h, nh, p->dist2 + p0,
+                                           r, d_ew_all + (int64_t)part * nh * ch, ch,
+                                           evals ? c->d_counter : nullptr);
+    // the host copy of h_grid above is pageable: it has been staged before
+    // the call returned, so the buffer can go back to the pool (stream order)
+    mgk_free(c, d_h, sizeof(float) * nh);
+    if (st) return st;
+    if (evals) return fetch_counter(c, evals);
+    return MGK_OK;
+}
+
+int mgk_loo_share_loglik(mgk_ctx* c, mgk_points* p, const float* h_grid, int nh, int part, int nparts,
+                         const float* d_ew_all, double* partial_logL, int64_t* evals) {
+    if (!c || !p || !h_grid || nh <= 0 || !partial_logL || nparts <= 0 || part < 0 || part >= nparts)
+        return mgk_fail(c, MGK_ERR_INVALID, "loo_share_loglik: bad arguments");
+    float lo, hi;
+    int st = check_bandwidths(c, h_grid, nh, &lo, &hi);
+    if (st) return st;
+    mgk_loo_batch* B = nullptr;
+    if ((st = mgk_loo_batch_create_share(c, p, nullptr, lo, hi, nh, part, nparts, d_ew_all,
+                                         share_chunk(p->n, nparts), &B)))
+        return st;
+    st = mgk_loo_batch_run(B, h_grid, partial_logL, nullptr, nullptr, evals);
+    mgk_loo_batch_destroy(B);
+    return st;
+}
+
 int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h0, float* h_opt, int* iterations) {
     if (!c || !p || !h_opt || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "mle_fixed_bandwidth: bad arguments");
     if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
@@ -649,30 +733,38 @@ struct RasterPipe {
 };
 }  // namespace
 
-int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp, float h,
-                   int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
-                   const float* dmask, int64_t tile_side, float* out_density, float* out_ew, int64_t* evals) {
+// The whole path over rows [row_lo, row_hi) of dg (dmask and out_density
+// hold those rows only).  A strict row range keeps, on the device, only the
+// points within 3 h_max of its rows (the densities of its cells need no
+// others), and out_ew must then be NULL.
+static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp,
+                           float h, int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
+                           int64_t row_lo, int64_t row_hi, const float* dmask, int64_t tile_side,
+                           float* out_density, float* out_ew, int64_t* evals) {
     if (!c || !grid_ok(dg) || !out_density || (edge_correction && (!grid_ok(eg) || !emask)) ||
-        (!h_pp && !(h > 0.0f)))
+        (!h_pp && !(h > 0.0f)) || row_lo < 0 || row_hi > dg->nrows || row_lo >= row_hi)
         return mgk_fail(c, MGK_ERR_INVALID, "kde_raster: bad arguments");
+    const bool part_rows = row_lo > 0 || row_hi < dg->nrows;
+    if (part_rows && out_ew) return mgk_fail(c, MGK_ERR_INVALID, "kde_raster_rows: out_ew needs the whole raster");
+    const int64_t nrows = row_hi - row_lo;
     // tile grid (kde_cuda_kdtr_tiled.cu:1373-1517 walks tiles row-major)
     int64_t tr, tc;
     const int64_t T = tile_side > 0 ? tile_side : c->tile_side;
-    std::vector<int64_t> band_r0;  // full-width bands: first row of band k, then nrows
+    std::vector<int64_t> band_r0;  // full-width bands: first row of band k, then row_hi
     if (T > 0) {
-        tr = std::min<int64_t>(T, dg->nrows);
+        tr = std::min<int64_t>(T, nrows);
         tc = std::min<int64_t>(T, dg->ncols);
     } else {
-        tr = std::max<int64_t>(256, ((dg->nrows + kRasterBands - 1) / kRasterBands + 63) / 64 * 64);
-        tr = std::min<int64_t>(tr, dg->nrows);
+        tr = std::max<int64_t>(256, ((nrows + kRasterBands - 1) / kRasterBands + 63) / 64 * 64);
+        tr = std::min<int64_t>(tr, nrows);
         tc = dg->ncols;
-        const int64_t tail = dg->nrows > 2 * 256 ? 256 : 0;
-        for (int64_t r0 = 0; r0 < dg->nrows - tail; r0 += tr) band_r0.push_back(r0);
-        if (tail) band_r0.push_back(dg->nrows - tail);
-        band_r0.push_back(dg->nrows);
+        const int64_t tail = nrows > 2 * 256 ? 256 : 0;
+        for (int64_t r0 = row_lo; r0 < row_hi - tail; r0 += tr) band_r0.push_back(r0);
+        if (tail) band_r0.push_back(row_hi - tail);
+        band_r0.push_back(row_hi);
     }
     const int64_t ntc = (dg->ncols + tc - 1) / tc;
-    const int64_t ntiles = band_r0.empty() ? (dg->nrows + tr - 1) / tr * ntc : (int64_t)band_r0.size() - 1;
+    const int64_t ntiles = band_r0.empty() ? (nrows + tr - 1) / tr * ntc : (int64_t)band_r0.size() - 1;
     const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
     RasterPipe pipe;
     cudaError_t ce = pipe.init();
@@ -697,9 +789,9 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
             nc = dg->ncols;
             return;
         }
-        r0 = (k / ntc) * tr;
+        r0 = row_lo + (k / ntc) * tr;
         c0 = (k % ntc) * tc;
-        nr = std::min<int64_t>(tr, dg->nrows - r0);
+        nr = std::min<int64_t>(tr, row_hi - r0);
         nc = std::min<int64_t>(tc, dg->ncols - c0);
     };
     // mask of tile k into buffer k % 2, after the density of tile k - 2 read it
@@ -710,7 +802,7 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         const int b = (int)(k & 1);
         cudaError_t e = k >= 2 ? cudaStreamWaitEvent(pipe.h2d, pipe.done[b], 0) : cudaSuccess;
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(d_mask[b], sizeof(float) * nc, dmask + r0 * dg->ncols + c0,
+            e = cudaMemcpy2DAsync(d_mask[b], sizeof(float) * nc, dmask + (r0 - row_lo) * dg->ncols + c0,
                                   sizeof(float) * dg->ncols, sizeof(float) * nc, nr, cudaMemcpyHostToDevice, pipe.h2d);
         if (e == cudaSuccess) e = cudaEventRecord(pipe.mask_ready[b], pipe.h2d);
         return e;
@@ -721,6 +813,19 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
                             cudaSuccess)
         st = mgk_cuda_fail(c, ce, "kde_raster counters");
     if (st == MGK_OK) st = mgk_points_upload(c, n, x, y, w, h_pp, &p);
+    if (st == MGK_OK && part_rows) {
+        // the halo of the rows: points within 3 h_max of their cell centres
+        float hmax = h;
+        if (h_pp)
+            for (int64_t i = 0; i < n; i++) hmax = std::max(hmax, h_pp[i]);
+        const double reach = 3.0 * (double)hmax * (1.0 + 1e-6) + 1e-6 * (double)dg->cs;
+        const double y_top = (double)mgk_cell_y(dg->yll, dg->cs, dg->nrows, row_lo);
+        const double y_bot = (double)mgk_cell_y(dg->yll, dg->cs, dg->nrows, row_hi - 1);
+        mgk_points* q = nullptr;
+        st = mgk_points_select(c, p, -DBL_MAX, DBL_MAX, y_bot - reach, y_top + reach, &q);
+        mgk_points_destroy(p);
+        p = q;
+    }
     if (st == MGK_OK && edge_correction) st = mgk_raster_upload(c, eg, emask, &em);
     // the first tile's mask travels while the points are prepared
     if (st == MGK_OK && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
@@ -745,7 +850,7 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
         const int b = (int)(k & 1);
         cudaError_t e = cudaStreamWaitEvent(pipe.d2h, pipe.done[b], 0);
         if (e == cudaSuccess)
-            e = cudaMemcpy2DAsync(out_density + r0 * dg->ncols + c0, sizeof(float) * dg->ncols, d_out[b],
+            e = cudaMemcpy2DAsync(out_density + (r0 - row_lo) * dg->ncols + c0, sizeof(float) * dg->ncols, d_out[b],
                                   sizeof(float) * nc, sizeof(float) * nc, nr, cudaMemcpyDeviceToHost, pipe.d2h);
         if (e == cudaSuccess) e = cudaEventRecord(pipe.out_free[b], pipe.d2h);
         return e;
@@ -842,6 +947,23 @@ int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const 
     mgk_points_destroy(p);
     if (st == MGK_OK && evals) *evals = ev_den + ev_edge;
     return st;
+}
+
+int mgk_kde_raster(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp, float h,
+                   int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
+                   const float* dmask, int64_t tile_side, float* out_density, float* out_ew, int64_t* evals) {
+    if (!dg) return mgk_fail(c, MGK_ERR_INVALID, "kde_raster: bad arguments");
+    return kde_raster_rows(c, n, x, y, w, h_pp, h, edge_correction, eg, emask, dg, 0, dg->nrows, dmask, tile_side,
+                           out_density, out_ew, evals);
+}
+
+int mgk_kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp,
+                        float h, int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
+                        int64_t row0, int64_t nrows, const float* dmask_rows, int64_t tile_side, float* out_rows,
+                        int64_t* evals) {
+    if (!dg) return mgk_fail(c, MGK_ERR_INVALID, "kde_raster_rows: bad arguments");
+    return kde_raster_rows(c, n, x, y, w, h_pp, h, edge_correction, eg, emask, dg, row0, row0 + nrows, dmask_rows,
+                           tile_side, out_rows, nullptr, evals);
 }
 
 }  // extern "C"

@@ -233,7 +233,111 @@ __global__ void k_morton_keys(int64_t n, const MgkPt* __restrict__ pts, double o
     vals[i] = (int32_t)i;
 }
 
+// ---- halo selection: the points inside a rectangle, in input order -------
+constexpr int kSelThreads = 256;
+constexpr int kSelRounds = 16;
+constexpr int kSelTile = kSelThreads * kSelRounds;
+
+struct SelRect {
+    double xlo, xhi, ylo, yhi;
+};
+
+__device__ __forceinline__ bool sel_in(const SelRect& R, float x, float y) {
+    const double dx = (double)x, dy = (double)y;
+    return dx >= R.xlo && dx <= R.xhi && dy >= R.ylo && dy <= R.yhi;
+}
+
+// Kept points per tile of kSelTile points; counts[ntiles] = 0 (the scan's total slot).
+__global__ void __launch_bounds__(kSelThreads) k_sel_count(int64_t n, const float* __restrict__ x,
+                                                           const float* __restrict__ y, SelRect R, int ntiles,
+                                                           unsigned* __restrict__ counts) {
+    __shared__ unsigned s_c;
+    if (threadIdx.x == 0) s_c = 0;
+    __syncthreads();
+    const int64_t base = (int64_t)blockIdx.x * kSelTile;
+    unsigned c = 0;
+    for (int r = 0; r < kSelRounds; r++) {
+        const int64_t i = base + (int64_t)r * kSelThreads + threadIdx.x;
+        c += (i < n && sel_in(R, x[i], y[i])) ? 1u : 0u;
+    }
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(&s_c, c);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        counts[blockIdx.x] = s_c;
+        if (blockIdx.x == 0) counts[ntiles] = 0;
+    }
+}
+
+// Stable scatter: round-major, thread-minor order is the input order; the
+// rank of a kept point is its warp ballot rank plus the kept points of lower
+// warps in the round and of earlier rounds.
+__global__ void __launch_bounds__(kSelThreads) k_sel_scatter(
+    int64_t n, const float* __restrict__ x, const float* __restrict__ y, const float* __restrict__ w,
+    const float* __restrict__ h, SelRect R, const unsigned* __restrict__ offsets, float* __restrict__ ox,
+    float* __restrict__ oy, float* __restrict__ ow, float* __restrict__ oh) {
+    __shared__ unsigned s_w[kSelThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t base = (int64_t)blockIdx.x * kSelTile;
+    unsigned run = offsets[blockIdx.x];
+    for (int r = 0; r < kSelRounds; r++) {
+        const int64_t i = base + (int64_t)r * kSelThreads + threadIdx.x;
+        const bool keep = i < n && sel_in(R, x[i], y[i]);
+        const unsigned bal = __ballot_sync(0xffffffffu, keep);
+        if (lane == 0) s_w[warp] = __popc(bal);
+        __syncthreads();
+        unsigned before = 0, total = 0;
+        for (int k = 0; k < kSelThreads / 32; k++) {
+            before += k < warp ? s_w[k] : 0u;
+            total += s_w[k];
+        }
+        if (keep) {
+            const unsigned o = run + before + __popc(bal & ((1u << lane) - 1u));
+            ox[o] = x[i];
+            oy[o] = y[i];
+            if (ow) ow[o] = w[i];
+            if (oh) oh[o] = h[i];
+        }
+        run += total;
+        __syncthreads();  // s_w is rewritten next round
+    }
+}
+
 }  // namespace
+
+// The points of src inside [xlo, xhi] x [ylo, yhi] (input order) into dst,
+// whose arrays the caller allocates after the count: first call with dst ==
+// NULL returns the count in *count (one read back), then with dst.
+int mgk_launch_points_select(mgk_ctx* ctx, const mgk_points* src, double xlo, double xhi, double ylo, double yhi,
+                             unsigned* d_scratch, int64_t* count, mgk_points* dst) {
+    const int64_t n = src->n;
+    const int ntiles = (int)((n + kSelTile - 1) / kSelTile);
+    const SelRect R{xlo, xhi, ylo, yhi};
+    cudaStream_t s = ctx->stream;
+    if (!dst) {
+        if (n == 0) {
+            *count = 0;
+            return MGK_OK;
+        }
+        k_sel_count<<<ntiles, kSelThreads, 0, s>>>(n, src->x, src->y, R, ntiles, d_scratch);
+        k_scan_exclusive<<<1, 1024, 0, s>>>(d_scratch, ntiles + 1);
+        MGK_CHECK_LAUNCH(ctx, "points select count");
+        MGK_COUNT_LAUNCH(ctx, 2);
+        unsigned tot = 0;
+        MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&tot, d_scratch + ntiles, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+        *count = (int64_t)tot;
+        return MGK_OK;
+    }
+    if (n == 0 || dst->n == 0) return MGK_OK;
+    k_sel_scatter<<<ntiles, kSelThreads, 0, s>>>(n, src->x, src->y, src->w, src->h, R, d_scratch, dst->x, dst->y,
+                                                 src->w ? dst->w : nullptr, src->h ? dst->h : nullptr);
+    MGK_CHECK_LAUNCH(ctx, "points select scatter");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    return MGK_OK;
+}
+
+int64_t mgk_points_select_scratch(int64_t n) { return (n + kSelTile - 1) / kSelTile + 1; }
 
 // Positions of the index records in Z-order of their bins (stable: records
 // of one bin keep their order).  Consecutive runs of this order are compact

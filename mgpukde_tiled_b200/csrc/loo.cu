@@ -56,12 +56,18 @@ struct LooParams {
     int nlev;
     int64_t n;
     int ngroups;
+    int g0, gcount;       // this share's query groups [g0, g0 + gcount) (all groups: 0, ngroups)
     int nh;
     const float* hgrid;   // [nh]
     int* korder;          // [nh] processing order (largest h first)
     int* klevel;          // [nh] level of each h
-    const float* ew;      // [nh][n] input order, or null (no edge correction)
-    double* part;         // [nh][ngroups]
+    // edge weights, or null (no edge correction): e_i(h_k) of point i (input
+    // order) is ew[(i / ew_chunk) * ew_cstride + k * ew_chunk + i % ew_chunk],
+    // i.e. chunks of ew_chunk points, each nh rows of ew_chunk floats (one
+    // chunk of n points, [nh][n], in a single-process batch)
+    const float* ew;
+    int64_t ew_chunk, ew_cstride;
+    double* part;         // [nh][gcount]
     unsigned* counter;    // work-item queue head
     unsigned long long* evals;
     unsigned long long* err;
@@ -140,15 +146,15 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
     }
     __syncthreads();
     unsigned ph0 = 0u, ph1 = 0u;  // mbarrier phase parities of the two buffers
-    const unsigned total = (unsigned)P.nh * (unsigned)P.ngroups;
+    const unsigned total = (unsigned)P.nh * (unsigned)P.gcount;
     unsigned long long cnt_all = 0;
     for (;;) {
         if (tid == 0) s_item = (int)atomicAdd(P.counter, 1u);
         __syncthreads();
         const unsigned item = (unsigned)s_item;
         if (item >= total) break;
-        const int k = P.korder[item / (unsigned)P.ngroups];
-        const int grp = (int)(item % (unsigned)P.ngroups);
+        const int k = P.korder[item / (unsigned)P.gcount];
+        const int grp = P.g0 + (int)(item % (unsigned)P.gcount);
         const LevelDesc L = P.lev[P.klevel[k]];
         const float h = P.hgrid[k];
         const double h2 = mgk_h2(h);
@@ -160,7 +166,7 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
         const double k2 = MGK_LOG2E / (2.0 * h2);
         const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
         const double reach = sqrt(cut) * (1.0 + 1e-9);
-        const float* ewk = P.ew ? P.ew + (int64_t)k * P.n : nullptr;
+        const float* ewk = P.ew ? P.ew + (int64_t)k * P.ew_chunk : nullptr;
 
         // this item's query
         // the group's queries: 128 consecutive records of the Z-order, a
@@ -228,7 +234,12 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
             }
             if (tid < m) {
                 const int64_t i = src + tid;
-                sw[buf][tid] = L.pts[i].wk * (ewk ? ewk[L.perm[i]] : 1.0f);
+                float e = 1.0f;
+                if (ewk) {
+                    const int64_t pi = L.perm[i], ch = pi / P.ew_chunk;
+                    e = ewk[ch * P.ew_cstride + (pi - ch * P.ew_chunk)];
+                }
+                sw[buf][tid] = L.pts[i].wk * e;
             }
             const unsigned par = buf ? ph1 : ph0;
             const bool ok = mbar_wait(&mbar[buf], par);
@@ -279,7 +290,7 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
             lg = log(loo > fl ? loo : fl);
         }
         const double sum = block_sum_fixed(lg, red);
-        if (tid == 0) P.part[(int64_t)k * P.ngroups + grp] = sum;
+        if (tid == 0) P.part[(int64_t)k * P.gcount + (grp - P.g0)] = sum;
         cnt_all += cnt;
         __syncthreads();  // s_item is rewritten next
     }
@@ -324,6 +335,7 @@ struct mgk_loo_batch {
     int64_t n = 0;
     int nh = 0;
     int ngroups = 0;
+    int g0 = 0, gcount = 0;  // the share's query groups
     std::vector<mgk_index*> lev;
     std::vector<int32_t*> qord;  // per level
     float* d_h = nullptr;
@@ -359,10 +371,10 @@ static int loo_enqueue(mgk_loo_batch* B) {
     }
     k_loo_prep<<<1, 256, 0, s>>>(B->P);
     const int occ = 8;  // resident CTAs of 128 threads per SM targeted by the persistent grid
-    const unsigned items = (unsigned)B->nh * (unsigned)B->ngroups;
+    const unsigned items = (unsigned)B->nh * (unsigned)std::max(B->P.gcount, 1);
     const unsigned grid = std::max(1u, std::min(items, (unsigned)(ctx->sm_count * occ)));
     k_loo_multi<<<grid, kLooQ, 0, s>>>(B->P);
-    k_loo_finish<<<B->nh, 256, 0, s>>>(B->d_part, B->ngroups, B->d_logl);
+    k_loo_finish<<<B->nh, 256, 0, s>>>(B->d_part, B->P.gcount, B->d_logl);
     k_argmax<<<1, 32, 0, s>>>(B->d_logl, B->nh, B->d_best);
     MGK_CHECK_LAUNCH(ctx, "loo batch");
     MGK_COUNT_LAUNCH(ctx, 4);
@@ -398,6 +410,16 @@ void mgk_loo_batch_destroy(mgk_loo_batch* B) {
 // bandwidth octave, buffers, and the captured graph.
 int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi, int nh,
                          mgk_loo_batch** out) {
+    return mgk_loo_batch_create_share(c, p, r, h_lo, h_hi, nh, 0, 1, nullptr, 0, out);
+}
+
+// Share `part` of `nparts` of a batch: the query groups
+// [part G / nparts, (part + 1) G / nparts) of every h, G = ceil(n / 128).
+// ew_ext (device, optional, with r == NULL): the edge weights of every point
+// and h in chunks of ew_chunk points, each nh rows of ew_chunk floats.
+int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi,
+                               int nh, int part, int nparts, const float* ew_ext, int64_t ew_chunk,
+                               mgk_loo_batch** out) {
     mgk_loo_batch* B = new (std::nothrow) mgk_loo_batch();
     if (!B) return mgk_fail(c, MGK_ERR_INVALID, "loo batch: out of host memory");
     B->ctx = c;
@@ -406,6 +428,8 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
     B->n = p->n;
     B->nh = nh;
     B->ngroups = (int)((p->n + kLooQ - 1) / kLooQ);
+    B->g0 = (int)((int64_t)B->ngroups * part / nparts);
+    B->gcount = (int)((int64_t)B->ngroups * (part + 1) / nparts) - B->g0;
     int st = MGK_OK;
     // levels: bin sides 0.75 h_lo * 2^l up to the side for h_hi
     mgk_points view = *p;  // index over w only; e(h) is applied per h
@@ -431,7 +455,7 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
     }
     const size_t n1 = (size_t)std::max<int64_t>(p->n, 1);
     B->bytes_ew = r ? sizeof(float) * n1 * (size_t)nh : 16;
-    B->bytes_part = sizeof(double) * (size_t)nh * (size_t)std::max(B->ngroups, 1);
+    B->bytes_part = sizeof(double) * (size_t)nh * (size_t)std::max(B->gcount, 1);
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_h, sizeof(float) * nh);
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_ew, B->bytes_ew);
     if (st == MGK_OK) st = mgk_alloc(c, (void**)&B->d_korder, sizeof(int) * nh);
@@ -468,11 +492,23 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
     P.lev = B->d_lev;
     P.n = p->n;
     P.ngroups = B->ngroups;
+    P.g0 = B->g0;
+    P.gcount = B->gcount;
     P.nh = nh;
     P.hgrid = B->d_h;
     P.korder = B->d_korder;
     P.klevel = B->d_klevel;
-    P.ew = r ? B->d_ew : nullptr;
+    if (r) {
+        P.ew = B->d_ew;
+        P.ew_chunk = std::max<int64_t>(p->n, 1);
+    } else if (ew_ext) {
+        P.ew = ew_ext;
+        P.ew_chunk = std::max<int64_t>(ew_chunk, 1);
+    } else {
+        P.ew = nullptr;
+        P.ew_chunk = 1;
+    }
+    P.ew_cstride = P.ew_chunk * (int64_t)nh;
     P.part = B->d_part;
     P.counter = B->d_counter;
     P.evals = B->d_evals + 1;

@@ -268,10 +268,20 @@ int mgk_launch_edge_weights_multi(mgk_ctx* ctx, int64_t n, const float* x, const
                                   const mgk_raster* r, float* ew_out, int64_t ew_stride,
                                   unsigned long long* d_evals);
 
+// Halo selection (index.cu): points of src inside a rectangle, input order.
+// With dst == NULL: counts them into *count (d_scratch holds the per-tile
+// offsets for the second call, mgk_points_select_scratch(n) unsigned).
+int mgk_launch_points_select(mgk_ctx* ctx, const mgk_points* src, double xlo, double xhi, double ylo, double yhi,
+                             unsigned* d_scratch, int64_t* count, mgk_points* dst);
+int64_t mgk_points_select_scratch(int64_t n);
+
 // Batched leave-one-out likelihood (loo.cu).
 struct mgk_loo_batch;
 int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi, int nh,
                          mgk_loo_batch** out);
+int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi,
+                               int nh, int part, int nparts, const float* ew_ext, int64_t ew_chunk,
+                               mgk_loo_batch** out);
 int mgk_loo_batch_run(mgk_loo_batch* B, const float* hs, double* logl, int* best, int64_t* edge_evals,
                       int64_t* loo_evals);
 void mgk_loo_batch_destroy(mgk_loo_batch* B);

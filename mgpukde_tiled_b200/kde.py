@@ -141,6 +141,15 @@ class Points:
         ctx.check(lib().mgk_points_wrap(ctx.handle, n, _ptr(x), _ptr(y), _ptr(w), _ptr(h), C.byref(out)))
         return cls(ctx, out, n, keep=(x, y, w, h))
 
+    def select(self, xlo=-np.inf, xhi=np.inf, ylo=-np.inf, yhi=np.inf) -> "Points":
+        """The points inside [xlo, xhi] x [ylo, yhi] (input order) as a new
+        device point set (mgk_points_select: a rank's halo points)."""
+        big = np.finfo(np.float64).max
+        out = C.c_void_p()
+        self.ctx.check(lib().mgk_points_select(self.ctx.handle, self._h, max(float(xlo), -big), min(float(xhi), big),
+                                               max(float(ylo), -big), min(float(yhi), big), C.byref(out)))
+        return Points(self.ctx, out, int(lib().mgk_points_size(out)))
+
     def device_arrays(self):
         ps = [C.c_void_p() for _ in range(6)]
         self.ctx.check(lib().mgk_points_device_arrays(self._h, *[C.byref(p) for p in ps]))
@@ -347,6 +356,31 @@ def log_likelihood_batch(ctx: Context, points: Points, raster: Raster | None, hg
     return out, am.value
 
 
+def loo_share_edge_weights(ctx: Context, points: Points, raster: Raster, hgrid, part: int, nparts: int, d_ew_all,
+                           count=False):
+    """Multi-GPU bandwidth selection, step 1 on rank `part` of `nparts`: the
+    edge weights of this rank's points for every h into its chunk of d_ew_all
+    (device float32, nparts * nh * ceil(n / nparts)); returns the eval count
+    when count is set."""
+    hs = _f32(hgrid)
+    ev = C.c_int64()
+    ctx.check(lib().mgk_loo_share_edge_weights(ctx.handle, points._h, raster._h, _ptr(hs), len(hs), int(part),
+                                               int(nparts), _ptr(d_ew_all), C.byref(ev) if count else None))
+    return ev.value if count else None
+
+
+def loo_share_loglik(ctx: Context, points: Points, hgrid, part: int, nparts: int, d_ew_all=None):
+    """Multi-GPU bandwidth selection, step 2 on rank `part` of `nparts`: the
+    FP64 partial log likelihoods (nh) of this rank's share of the queries, and
+    its pair count; summed over ranks they are logL."""
+    hs = _f32(hgrid)
+    out = np.zeros(len(hs), np.float64)
+    ev = C.c_int64()
+    ctx.check(lib().mgk_loo_share_loglik(ctx.handle, points._h, _ptr(hs), len(hs), int(part), int(nparts),
+                                         _ptr(d_ew_all), _ptr(out), C.byref(ev)))
+    return out, ev.value
+
+
 def mle_fixed_bandwidth(ctx: Context, points: Points, raster: Raster | None, h0: float):
     """MLE_FixedBandWidth (golden section); returns (h_opt, iterations)."""
     h = C.c_float()
@@ -396,3 +430,23 @@ def kde_raster(ctx: Context, x, y, w, h, dens_grid: Grid, dens_mask=None, edge_g
                                    C.byref(eg), _ptr(em), C.byref(dg), _ptr(dm), int(tile), _ptr(out), _ptr(ew),
                                    C.byref(ev) if count else None))
     return out, ew, (ev.value if count else None)
+
+
+def kde_raster_rows(ctx: Context, x, y, w, h, dens_grid: Grid, row0: int, nrows: int, dens_mask_rows=None,
+                    edge_grid: Grid | None = None, edge_mask=None, h_pp=None, tile=0, out=None, count=False):
+    """Rows [row0, row0 + nrows) of the whole path from host buffers (one
+    rank's share of a study split by rows); returns (density[nrows, ncols],
+    evals|None).  dens_mask_rows: the rows' part of the density mask."""
+    x, y, w, h_pp = _f32(x), _f32(y), _f32(w), _f32(h_pp)
+    dm = None if dens_mask_rows is None else _f32(dens_mask_rows).reshape(-1)
+    em = None if edge_mask is None else _f32(edge_mask).reshape(-1)
+    if out is None:
+        out = np.empty((nrows, dens_grid.ncols), np.float32)
+    dg = dens_grid.c()
+    eg = edge_grid.c() if edge_grid is not None else MgkGrid()
+    ev = C.c_int64()
+    ctx.check(lib().mgk_kde_raster_rows(ctx.handle, len(x), _ptr(x), _ptr(y), _ptr(w), _ptr(h_pp),
+                                        float(h if h is not None else 0.0), int(edge_grid is not None),
+                                        C.byref(eg), _ptr(em), C.byref(dg), int(row0), int(nrows), _ptr(dm),
+                                        int(tile), _ptr(out), C.byref(ev) if count else None))
+    return out, (ev.value if count else None)
