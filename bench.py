@@ -288,6 +288,54 @@ def run_reference_binary(c, crop, threads):
         return (t_den + t_edge) / 1e3
 
 
+def run_reference_gpu(c, crop, threads):
+    """The reference program's own CUDA path (KernelDesityEstimation_pPoints,
+    kde_kernel_kdtr.cu:461-574, after CalcEdgeCorrectionWeights, :192-265) on
+    the crop: mode 1, h_option -1, the OpenMP path skipped, one GPU.  Returns
+    its printed edge-weight and tile-density times (ms, host clock around its
+    launches, copies and halo extraction) and its density raster."""
+    from mgpukde_tiled_b200 import tiff
+    with tempfile.TemporaryDirectory() as d:
+        with open(os.path.join(d, "p.csv"), "w") as f:
+            f.write("x,y,h,w\n")
+            for a, b, w in zip(crop["x"], crop["y"], crop["w"]):
+                f.write("%.9g,%.9g,%.9g,%.9g\n" % (a, b, c["h"], w))
+        eg = c["edge_grid"]
+        tiff.write(os.path.join(d, "e.tif"), tiff.GeoRaster(c["edge_mask"], (float(eg.xll), float(eg.cs), 0.0,
+                   float(eg.yll) + eg.nrows * float(eg.cs), 0.0, -float(eg.cs)), eg.nodata))
+        g = crop["grid"]
+        tiff.write(os.path.join(d, "d.tif"), tiff.GeoRaster(crop["mask"], (float(g.xll), float(g.cs), 0.0,
+                   float(g.yll) + g.nrows * float(g.cs), 0.0, -float(g.cs)), g.nodata))
+        p = subprocess.run([REF_BIN, "1", "p.csv", "e.tif", "d.tif", "-1", "1", "1", "1", "0", str(threads), "1",
+                            "den_cpu.tif", "den_gpu.tif", "0"], cwd=d, capture_output=True, text=True, timeout=600)
+        if p.returncode != 0:
+            raise RuntimeError(p.stdout[-1000:] + p.stderr[-1000:])
+        t_edge = float(re.search(r"CalcEdgeCorrectionWeights took (\d+) ms", p.stdout).group(1))
+        t_den = sum(float(v) for v in re.findall(r"KernelDesityEstimation on tile \d+ took (\d+) ms", p.stdout))
+        den = tiff.read(os.path.join(d, "den_gpu.tif")).data
+        return t_edge, t_den, den
+
+
+def reference_gpu_baseline(c, side=2048):
+    """The reference's own CUDA kernels on this GPU, on a side x side crop of
+    the workload with its halo points: evals/s of its edge weights plus tile
+    density, and its raster's largest relative error against the FP64 oracle
+    (its sums are float atomics)."""
+    threads = os.cpu_count() or 1
+    crop = crop_inputs(c, side)
+    dev, eev, ew, den_ref = crop_evals(c, crop)
+    t_edge, t_den, den = run_reference_gpu(c, crop, threads)
+    valid = crop["mask"] != crop["grid"].nodata
+    rel = np.abs(den[valid].astype(np.float64) - den_ref[valid]) / np.maximum(np.abs(den_ref[valid]), 1e-300)
+    t = (t_edge + t_den) / 1e3
+    return {"value": (dev + eev) / max(t, 1e-9), "unit": UNIT, "edge_ms": t_edge, "density_ms": t_den,
+            "density_value": dev / max(t_den / 1e3, 1e-9), "evals": int(dev + eev),
+            "max_rel_err": float(rel.max()), "kernels": "CalcEdgeCorrectionWeights + KernelDesityEstimation_pPoints",
+            "sample": f"{side}x{side} density window with its {len(crop['x'])} halo points; the reference program "
+                      f"(mode 1, h_option -1, OpenMP path skipped, 1 GPU), its printed edge-weight and tile-density "
+                      f"times (host clock, ms)"}
+
+
 def cpu_baseline(c, side=1024):
     """The reference's CPU path (or the FP64 oracle port) on a crop of the
     workload: a side x side density window with its halo points."""
@@ -596,6 +644,14 @@ def run_mgk(args):
                 out["cpu_baseline"] = cpu_baseline(c)
             except Exception as e:  # reported, not fatal
                 out["cpu_baseline"] = {"value": None, "error": str(e)[:200]}
+        if not args.no_reference_gpu and os.path.exists(REF_BIN):
+            try:
+                rg = reference_gpu_baseline(c)
+                rg["ratio_step"] = value / rg["value"]
+                rg["ratio_density_kernel"] = (ev_d / dens_s) / rg["density_value"]
+                out["reference_gpu"] = rg
+            except Exception as e:  # reported, not fatal
+                out["reference_gpu"] = {"value": None, "error": str(e)[:200]}
         if step_raster is not None:
             out["accuracy"] = single_large_accuracy(c, {"step": step_raster, "e2e": hout.numpy()}, ev_d, ev_e)
     if rank == 0:
@@ -1115,6 +1171,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-form", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip timing the reference program's own CUDA kernels on a crop")
     ap.add_argument("--no-accuracy", action="store_true",
                     help="skip the FP64 oracle check of the whole output (minutes of host CPU at full scale)")
     args = ap.parse_args()

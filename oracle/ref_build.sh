@@ -1,9 +1,11 @@
 #!/usr/bin/env bash
 # Builds the reference program (mGPUKDE_tiled) from its own, unmodified
 # sources where they lie, into oracle/_ref/mgkde_ref.  Test infrastructure:
-# the binary pins the FP64 oracle (tests/golden/make_golden.py) and is the
-# timed "reference" CPU baseline.  Its CPU path (skip_gpu_parallel=1) is the
-# only part ever run.
+# the binary pins the FP64 oracle (tests/golden/make_golden.py), is the timed
+# "reference" CPU baseline (its OpenMP path, skip_gpu_parallel=1), and its
+# own CUDA path (skip_omp_parallel=1, mode 1, h_option -1: the edge-weight and
+# tile-density kernels, read for bounds before it first ran) is the bench's
+# second comparator on the GPU.
 #
 # What it takes to compile the Windows/GDAL sources on Linux, without editing
 # them:
