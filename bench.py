@@ -509,7 +509,7 @@ def run_mgk(args):
     def step(count=False):
         mk.mark_boundary(ctx, em)
         p = pts if world == 1 else pts.select(ylo=y_bot - reach, yhi=y_top + reach)
-        mk.calc_dist2_boundary(ctx, p, em)
+        mk.calc_dist2_boundary(ctx, p, em, reach=reach)  # exact up to 3h: what the edge weights read
         ev_e = mk.edge_correction_weights(ctx, p, em, h, count=count)
         idx = mk.Index(ctx, p, h)
         ev_d = (mk.density_tile(ctx, idx, dg, row0, 0, nrows, dg.ncols, ddmask[row0:row0 + nrows], dout,
@@ -523,7 +523,7 @@ def run_mgk(args):
     if world > 1:
         # the study's units: its density pairs (the ranks' rows partition them) and
         # its edge-correction pairs counted once (halo points repeat across ranks)
-        mk.calc_dist2_boundary(ctx, pts, em)
+        mk.calc_dist2_boundary(ctx, pts, em, reach=reach)
         ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=True)
     evals = ev_e + ev_d
     for _ in range(args.warmup):
@@ -672,8 +672,8 @@ def loo_cpu_check(c, hgrid, logl, pts, nsmall=16):
     import oracle_py as o
     threads = os.cpu_count() or 1
     o.set_threads(threads)
-    d2, _ = pts.download(dist2=True, ew=False)
     eg = o.grid(*c["edge_grid"].astuple())
+    d2 = o.dist2_boundary(c["x"], c["y"], eg, o.mark_boundary(eg, c["edge_mask"]))
     ks = list(np.argsort(hgrid)[:nsmall])
     t0 = time.perf_counter()
     refs = [o.loglik_at(c["x"], c["y"], c["w"], d2, eg, c["edge_mask"], float(hgrid[k])) for k in ks]
@@ -755,8 +755,10 @@ def run_bandwidth_select(args):
     hgrid = c["hgrid"]
     shared_ev = [0, 0]
 
+    reach = 3.0 * float(np.max(hgrid)) * (1.0 + 1e-6)  # distances exact up to 3 h_max
+
     def step():
-        mk.calc_dist2_boundary(ctx, pts, em)
+        mk.calc_dist2_boundary(ctx, pts, em, reach=reach)
         if world == 1:
             return mk.log_likelihood_batch(ctx, pts, em, hgrid)
         tot, am, ev = shard.loo_loglik_shared(ctx, pts, em, hgrid, rank, world)
@@ -993,7 +995,7 @@ def run_out_of_core(args):
 
     def step(count=False):
         mk.mark_boundary(ctx, em)
-        mk.calc_dist2_boundary(ctx, pts, em)
+        mk.calc_dist2_boundary(ctx, pts, em, reach=3.0 * h * (1.0 + 1e-6))
         ev_e = mk.edge_correction_weights(ctx, pts, em, h, count=count)
         idx = mk.Index(ctx, pts, h)
         ev_d = mk.density_stream(ctx, idx, dg, tile, host, count=count)

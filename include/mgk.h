@@ -144,6 +144,17 @@ int mgk_raster_boundary_download(mgk_raster* mask, uint8_t* out);
  * point to the nearest boundary-cell centre (DBL_MAX when there is none).
  * Marks the boundary first if mgk_mark_boundary has not run. */
 int mgk_boundary_dist(mgk_ctx* ctx, mgk_points* pts, mgk_raster* mask);
+/* The same distances made exact only for points whose nearest boundary cell
+ * lies within `reach` (coordinate units); the others get a value above
+ * reach^2.  The distances matter only through the edge-weight short-circuit
+ * (weight 1 when dist2 >= 9 h^2, kde_cuda_kdtr_tiled.cu:2704-2708), so a reach
+ * of 3 h_max gives the same edge weights as mgk_boundary_dist at a fraction
+ * of the search (points deep inside the study area skip it).  The calls that
+ * read the distances (edge weights, likelihoods) check that the reach covers
+ * 3h for every bandwidth they use and fail with MGK_ERR_INVALID otherwise;
+ * the adaptive-bandwidth calls need mgk_boundary_dist.  No reference
+ * counterpart (the reference computes every distance exactly, brute force). */
+int mgk_boundary_dist_within(mgk_ctx* ctx, mgk_points* pts, mgk_raster* mask, double reach);
 
 /* ---- edge correction --------------------------------------------------- */
 

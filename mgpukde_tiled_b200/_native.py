@@ -29,7 +29,7 @@ EXPORTS = [
     "mgk_serve_create", "mgk_serve_submit", "mgk_serve_poll", "mgk_serve_wait", "mgk_serve_stats",
     "mgk_serve_destroy", "mgk_density_stream", "mgk_copy_sink", "mgk_ctx_get_tuning", "mgk_ctx_set_tuning",
     "mgk_autotune", "mgk_loglik_adaptive", "mgk_adaptive_bandwidths",
-    "mgk_points_select", "mgk_points_size", "mgk_kde_raster_rows", "mgk_loo_share_edge_weights", "mgk_loo_share_loglik",
+    "mgk_boundary_dist_within", "mgk_points_select", "mgk_points_size", "mgk_kde_raster_rows", "mgk_loo_share_edge_weights", "mgk_loo_share_loglik",
 ]
 
 
@@ -145,6 +145,7 @@ def lib():
         "mgk_kde_raster": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, P, I64, P, P, C.POINTER(I64)]),
         "mgk_points_select": (I, [P, P, C.c_double, C.c_double, C.c_double, C.c_double, PP]),
         "mgk_points_size": (I64, [P]),
+        "mgk_boundary_dist_within": (I, [P, P, P, C.c_double]),
         "mgk_kde_raster_rows": (I, [P, I64, P, P, P, P, C.c_float, I, G, P, G, I64, I64, P, I64, P,
                                     C.POINTER(I64)]),
         "mgk_loo_share_edge_weights": (I, [P, P, P, P, I, I, I, P, C.POINTER(I64)]),

@@ -414,6 +414,8 @@ extern "C" {
 int mgk_loglik_adaptive(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, float alpha, double* logl) {
     if (!c || !p || !logl || !(h > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "loglik_adaptive: bad arguments");
     if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loglik_adaptive: run mgk_boundary_dist first");
+    if (r && std::isfinite(p->dist2_cap))  // the adaptive bandwidths are not known in advance
+        return mgk_fail(c, MGK_ERR_INVALID, "loglik_adaptive: needs the exact boundary distances of mgk_boundary_dist");
     int st;
     if ((st = ensure_h(c, p))) return st;
     double *d_den = nullptr, *d_scal = nullptr;
@@ -440,6 +442,8 @@ int mgk_adaptive_bandwidths(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
                             float* alpha_opt, double* lmax, int* iterations, float* hs_out) {
     if (!c || !p || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "adaptive_bandwidths: bad arguments");
     if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "adaptive_bandwidths: run mgk_boundary_dist first");
+    if (r && std::isfinite(p->dist2_cap))  // the adaptive bandwidths are not known in advance
+        return mgk_fail(c, MGK_ERR_INVALID, "adaptive_bandwidths: needs the exact boundary distances of mgk_boundary_dist");
     int st;
     if ((st = ensure_h(c, p))) return st;
     double *d_den = nullptr, *d_scal = nullptr;

@@ -437,12 +437,52 @@ int mgk_raster_boundary_download(mgk_raster* r, uint8_t* out) {
     return MGK_OK;
 }
 
-int mgk_boundary_dist(mgk_ctx* c, mgk_points* p, mgk_raster* r) {
-    if (!c || !p || !r) return mgk_fail(c, MGK_ERR_INVALID, "boundary_dist: bad arguments");
+static int boundary_dist(mgk_ctx* c, mgk_points* p, mgk_raster* r, double cap) {
     int st;
     if (!r->marked && (st = mgk_launch_mark_boundary(c, r))) return st;
-    if ((st = mgk_launch_dist2(c, p, r))) return st;
+    if ((st = mgk_launch_dist2(c, p, r, cap))) return st;
     p->has_dist2 = true;
+    p->dist2_cap = cap;
+    return MGK_OK;
+}
+
+int mgk_boundary_dist(mgk_ctx* c, mgk_points* p, mgk_raster* r) {
+    if (!c || !p || !r) return mgk_fail(c, MGK_ERR_INVALID, "boundary_dist: bad arguments");
+    return boundary_dist(c, p, r, INFINITY);
+}
+
+int mgk_boundary_dist_within(mgk_ctx* c, mgk_points* p, mgk_raster* r, double reach) {
+    if (!c || !p || !r || !(reach > 0.0)) return mgk_fail(c, MGK_ERR_INVALID, "boundary_dist_within: bad arguments");
+    return boundary_dist(c, p, r, reach);
+}
+
+// The edge-weight short-circuit (weight 1 when dist2 >= 9 h^2, h^2 a float
+// product) decides exactly from distances that are exact up to dist2_cap
+// only if 9 h^2 <= dist2_cap^2 for every bandwidth used.
+static bool cap_covers(const mgk_points* p, float hmax) {
+    if (!std::isfinite(p->dist2_cap)) return true;
+    return 9.0 * (double)(hmax * hmax) <= p->dist2_cap * p->dist2_cap;
+}
+
+__global__ static void k_max_h(int64_t n, const float* __restrict__ h, unsigned* out) {
+    unsigned m = 0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = max(m, __float_as_uint(fmaxf(h[i], 0.0f)));  // non-negative floats order as their bits
+    for (int o = 16; o; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
+// Largest per-point bandwidth (device reduction, one read back).
+static int points_hmax(mgk_ctx* c, const mgk_points* p, float* out) {
+    unsigned* d = reinterpret_cast<unsigned*>(c->d_counter);
+    MGK_CHECK_CUDA(c, cudaMemsetAsync(d, 0, sizeof(unsigned), c->stream));
+    if (p->n) k_max_h<<<(unsigned)std::min<int64_t>((p->n + 255) / 256, 4 * c->sm_count), 256, 0, c->stream>>>(
+        p->n, p->h, d);
+    MGK_CHECK_LAUNCH(c, "k_max_h");
+    unsigned v = 0;
+    MGK_CHECK_CUDA(c, cudaMemcpyAsync(&v, d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    MGK_CHECK_CUDA(c, cudaStreamSynchronize(c->stream));
+    memcpy(out, &v, sizeof(float));
     return MGK_OK;
 }
 
@@ -459,6 +499,14 @@ int mgk_edge_weights(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h, in
     if (!c || !p || !r) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: bad arguments");
     if (!p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: run mgk_boundary_dist first");
     if (h <= 0.0f && !p->h) return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: no bandwidth");
+    float hmax = h;
+    if (h <= 0.0f && std::isfinite(p->dist2_cap)) {
+        int st = points_hmax(c, p, &hmax);
+        if (st) return st;
+    }
+    if (!cap_covers(p, hmax))
+        return mgk_fail(c, MGK_ERR_INVALID, "edge_weights: the boundary distances are exact only within " +
+                                                std::to_string(p->dist2_cap) + " (< 3h); use a larger reach");
     if (evals) MGK_CHECK_CUDA(c, cudaMemsetAsync(c->d_counter, 0, sizeof(unsigned long long), c->stream));
     int st = mgk_launch_edge_weights(c, p->n, p->x, p->y, h > 0.0f ? nullptr : p->h, h, p->dist2, r, p->ew,
                                      evals ? c->d_counter : nullptr);
@@ -609,6 +657,9 @@ int mgk_loo_loglik_batch(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const f
     float lo, hi;
     int st = check_bandwidths(c, h_grid, nh, &lo, &hi);
     if (st) return st;
+    if (r && !cap_covers(p, hi))
+        return mgk_fail(c, MGK_ERR_INVALID, "loo: the boundary distances are exact only within " +
+                                                std::to_string(p->dist2_cap) + ", less than 3 h_max");
     mgk_loo_batch* B = nullptr;
     if ((st = mgk_loo_batch_create(c, p, r, lo, hi, nh, &B))) return st;
     st = mgk_loo_batch_run(B, h_grid, logl, argmax, nullptr, nullptr);
@@ -627,6 +678,9 @@ int mgk_loo_share_edge_weights(mgk_ctx* c, mgk_points* p, const mgk_raster* r, c
     float lo, hi;
     int st = check_bandwidths(c, h_grid, nh, &lo, &hi);
     if (st) return st;
+    if (!cap_covers(p, hi))
+        return mgk_fail(c, MGK_ERR_INVALID, "loo: the boundary distances are exact only within " +
+                                                std::to_string(p->dist2_cap) + ", less than 3 h_max");
     const int64_t ch = share_chunk(p->n, nparts);
     const int64_t p0 = std::min<int64_t>(p->n, (int64_t)part * ch), p1 = std::min<int64_t>(p->n, p0 + ch);
     float* d_h = nullptr;
@@ -665,6 +719,9 @@ int mgk_loo_share_loglik(mgk_ctx* c, mgk_points* p, const float* h_grid, int nh,
 int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, float h0, float* h_opt, int* iterations) {
     if (!c || !p || !h_opt || !(h0 > 0.0f)) return mgk_fail(c, MGK_ERR_INVALID, "mle_fixed_bandwidth: bad arguments");
     if (r && !p->has_dist2) return mgk_fail(c, MGK_ERR_INVALID, "loo: run mgk_boundary_dist first");
+    if (r && !cap_covers(p, 2 * h0))  // every probe lies in [h0/20, 2 h0]
+        return mgk_fail(c, MGK_ERR_INVALID, "loo: the boundary distances are exact only within " +
+                                                std::to_string(p->dist2_cap) + ", less than 3 h_max");
     // MLE_FixedBandWidth, kde_cuda_kdtr_tiled.cu:3044-3093 (float bracket arithmetic)
     float hA = h0 / 20;
     float hD = 2 * h0;
@@ -831,7 +888,12 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     if (st == MGK_OK && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
     if (st == MGK_OK) {
         if (edge_correction) {
-            if ((st = mgk_boundary_dist(c, p, em)) == MGK_OK)
+            // distances exact up to 3 h_max: all the edge-weight short-circuit reads
+            float hmax = h;
+            if (h_pp)
+                for (int64_t i = 0; i < n; i++) hmax = std::max(hmax, h_pp[i]);
+            const double reach = 3.0 * (double)hmax * (1.0 + 1e-6);
+            if ((st = mgk_boundary_dist_within(c, p, em, reach)) == MGK_OK)
                 st = mgk_edge_weights(c, p, em, hfix, evals ? &ev_edge : nullptr);
         } else {
             st = mgk_edge_weights_unit(c, p);

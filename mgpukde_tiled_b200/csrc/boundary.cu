@@ -18,6 +18,7 @@
 // order independent, so the result is the brute-force minimum bit for bit.
 #include <algorithm>
 #include <cfloat>
+#include <cmath>
 
 #include "mgk_internal.cuh"
 
@@ -222,9 +223,11 @@ __device__ __forceinline__ double maxd2(double x0, double y0, double x1, double 
 
 // mode 0: UB per bin; mode 1: candidate count per bin; mode 2: fill the lists
 // (one warp per bin; the lanes share each ring's perimeter bins)
+// cap2: only cells within sqrt(cap2) of the bin rectangle are listed (points
+// farther than that from every boundary cell get a distance above cap2).
 template <int MODE>
 __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restrict__ start,
-                            const int* __restrict__ near, BinGrid B, double* __restrict__ ub,
+                            const int* __restrict__ near, BinGrid B, double cap2, double* __restrict__ ub,
                             int* __restrict__ cnt, const int* __restrict__ cstart, float2* __restrict__ cand) {
     const int lane = threadIdx.x & 31;
     const int k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -238,7 +241,7 @@ __global__ void k_bin_cands(const float2* __restrict__ cells, const int* __restr
     x1 += widen;
     y1 += widen;
     const int rmax = max(B.nbx, B.nby);
-    double lim = MODE == 0 ? DBL_MAX : ub[k] * (1.0 + 1e-9);
+    double lim = MODE == 0 ? cap2 : ub[k] * (1.0 + 1e-9);
     int n = 0;
     int base = MODE == 2 ? cstart[k] : 0;
     for (int r = near[k]; r <= rmax; r++) {
@@ -494,39 +497,8 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     if (r->bnear) mgk_free(ctx, r->bnear, b_start);
     r->bnear = cursor;
     cursor = nullptr;
-    // per-bin candidate lists
-    if (r->bub) mgk_free(ctx, r->bub, sizeof(double) * (size_t)r->nbins);
-    if (r->cstart) mgk_free(ctx, r->cstart, b_start);
-    if (r->cand) mgk_free(ctx, r->cand, sizeof(float2) * (size_t)std::max<int64_t>(r->ncand, 1));
-    r->bub = nullptr;
-    r->cstart = nullptr;
-    r->cand = nullptr;
-    r->ncand = 0;
-    if ((st = mgk_alloc(ctx, (void**)&r->bub, sizeof(double) * (size_t)r->nbins)) ||
-        (st = mgk_alloc(ctx, (void**)&r->cstart, b_start))) {
-        mgk_free(ctx, cells, sizeof(float2) * ncell);
-        return st;
-    }
-    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->cstart, 0, b_start, s));
-    if (nb > 0) {
-        const unsigned gbin = (unsigned)((r->nbins * 32 + 127) / 128);  // one warp per bin
-        k_bin_cands<0><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, nullptr, nullptr, nullptr);
-        k_bin_cands<1><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, r->cstart, nullptr, nullptr);
-        k_scan_small<<<1, 1024, 0, s>>>(r->cstart, (int)r->nbins);
-        MGK_CHECK_LAUNCH(ctx, "boundary candidate lists");
-        MGK_COUNT_LAUNCH(ctx, 3);
-        int total = 0;
-        MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&total, r->cstart + r->nbins, sizeof(int), cudaMemcpyDeviceToHost, s));
-        MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-        r->ncand = total;
-        if ((st = mgk_alloc(ctx, (void**)&r->cand, sizeof(float2) * (size_t)std::max(total, 1)))) {
-            mgk_free(ctx, cells, sizeof(float2) * ncell);
-            return st;
-        }
-        k_bin_cands<2><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, r->bub, nullptr, r->cstart, r->cand);
-        MGK_CHECK_LAUNCH(ctx, "boundary candidate fill");
-        MGK_COUNT_LAUNCH(ctx, 1);
-    }
+    // the per-bin candidate lists are built by the distance search, for its reach
+    r->cand_cap = -1.0;
     MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
     mgk_free(ctx, cells, sizeof(float2) * ncell);
     r->marked = true;
@@ -535,7 +507,57 @@ int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r) {
     return mgk_raster_runs(ctx, r);
 }
 
-int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r) {
+// Per-bin candidate lists for distances exact up to `cap` (coordinate units;
+// infinite: every distance exact).  Bins whose nearest boundary cells lie
+// beyond the cap get short or empty lists, so a small cap (3h: what the
+// edge-weight short-circuit asks) makes the lists and the search cheap.
+static int build_cands(mgk_ctx* ctx, mgk_raster* r, double cap) {
+    cudaStream_t s = ctx->stream;
+    const mgk_grid& g = r->g;
+    BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};
+    const size_t b_start = sizeof(int) * (size_t)(r->nbins + 1);
+    const double cap2 = std::isfinite(cap) ? cap * cap * (1.0 + 1e-9) : DBL_MAX;
+    if (r->bub) mgk_free(ctx, r->bub, sizeof(double) * (size_t)r->nbins);
+    if (r->cstart) mgk_free(ctx, r->cstart, b_start);
+    if (r->cand) mgk_free(ctx, r->cand, sizeof(float2) * (size_t)std::max<int64_t>(r->ncand, 1));
+    r->bub = nullptr;
+    r->cstart = nullptr;
+    r->cand = nullptr;
+    r->ncand = 0;
+    r->cand_cap = -1.0;
+    int st;
+    if ((st = mgk_alloc(ctx, (void**)&r->bub, sizeof(double) * (size_t)r->nbins)) ||
+        (st = mgk_alloc(ctx, (void**)&r->cstart, b_start)))
+        return st;
+    MGK_CHECK_CUDA(ctx, cudaMemsetAsync(r->cstart, 0, b_start, s));
+    if (r->nb > 0) {
+        const unsigned gbin = (unsigned)((r->nbins * 32 + 127) / 128);  // one warp per bin
+        k_bin_cands<0><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, cap2, r->bub, nullptr, nullptr, nullptr);
+        k_bin_cands<1><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, cap2, r->bub, r->cstart, nullptr, nullptr);
+        k_scan_small<<<1, 1024, 0, s>>>(r->cstart, (int)r->nbins);
+        MGK_CHECK_LAUNCH(ctx, "boundary candidate lists");
+        MGK_COUNT_LAUNCH(ctx, 3);
+        int total = 0;
+        MGK_CHECK_CUDA(ctx, cudaMemcpyAsync(&total, r->cstart + r->nbins, sizeof(int), cudaMemcpyDeviceToHost, s));
+        MGK_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+        r->ncand = total;
+        if ((st = mgk_alloc(ctx, (void**)&r->cand, sizeof(float2) * (size_t)std::max(total, 1)))) return st;
+        if (total > 0) {
+            k_bin_cands<2><<<gbin, 128, 0, s>>>(r->bcells, r->bstart, r->bnear, B, cap2, r->bub, nullptr, r->cstart,
+                                                r->cand);
+            MGK_CHECK_LAUNCH(ctx, "boundary candidate fill");
+            MGK_COUNT_LAUNCH(ctx, 1);
+        }
+    }
+    r->cand_cap = std::isfinite(cap) ? cap : INFINITY;
+    return MGK_OK;
+}
+
+int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, mgk_raster* r, double cap) {
+    if (!(r->cand_cap >= cap)) {  // no lists yet, or lists for a shorter reach
+        int st = build_cands(ctx, r, cap);
+        if (st) return st;
+    }
     if (p->n == 0) return MGK_OK;
     const mgk_grid& g = r->g;
     BinGrid B{(double)g.xll, (double)g.yll, (double)kBinCells * (double)g.cs, r->bnx, r->bny};

@@ -390,10 +390,42 @@ constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab;
 #ifndef MGK_DENSITY_MIN_CTAS
 #define MGK_DENSITY_MIN_CTAS 2  // resident CTAs per SM (shared memory allows two)
 #endif
+// Phase A builds the cutoff thresholds and ambiguity flags of a row only when
+// a sub-block that sums the point is partial in that row's warp row (fully
+// inside sub-blocks read neither).
+#ifndef MGK_DENSITY_ROWSKIP
+#define MGK_DENSITY_ROWSKIP 1
+#endif
+// Phase B takes a half-batch's fully-inside points in one loop and its
+// partial ones in another, and decides the Kahan flush once per half-batch.
+#ifndef MGK_DENSITY_SPLITLOOP
+#define MGK_DENSITY_SPLITLOOP 1
+#endif
 
 // Block column of cell j (0..7) of lane column tc in warp column wc.
 __device__ __forceinline__ int lane_col(int wc, int tc, int j) {
     return wc * 64 + (j < 4 ? tc * 4 + j : 32 + tc * 4 + (j - 4));
+}
+
+// The thread's FP32 partial sums into its Kahan-compensated accumulators in
+// tensor memory (sum at tS, compensation at tC), then zeroed.
+__device__ __forceinline__ void flush_partials(unsigned tS, unsigned tC, float (&part)[32]) {
+    __syncwarp();
+    tmem_wait_st();  // the previous flush's stores have landed
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+        float sv[8], cv[8];
+        tmem_ld8(tS + 8u * c, sv);
+        tmem_ld8(tC + 8u * c, cv);
+        tmem_wait_ld(sv, cv);
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            kahan_add(sv[u], cv[u], part[c * 8 + u]);
+            part[c * 8 + u] = 0.0f;
+        }
+        tmem_st8(tS + 8u * c, sv);
+        tmem_st8(tC + 8u * c, cv);
+    }
 }
 
 // One work item: the gather of the candidate range [it.k0, it.k1) of one
@@ -553,6 +585,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             // other entries are never read (the warps that would read them skip
             // the point)
             const unsigned pb = (bal >> (8 * (qa & 3))) & 0xffu;
+            // sub-blocks that sum point pq with the cutoff test (all of them in the counting variant)
+            const unsigned pbp = (MGK_DENSITY_ROWSKIP && !COUNT) ? pb & ~((balf >> (8 * (qa & 3))) & 0xffu) : pb;
             if (pb) {
                 float* cE = colE + pq * kFStrideC;
                 float* rF = rowF + pq * kFStride;
@@ -584,6 +618,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
                     const float fb = exp2_pair(bh, bl);
                     rF[i] = __fmul_rn(r.wk, fb);
+                    if (!((pbp >> (2 * (c >> 1))) & 3u)) continue;  // no partial sub-block reads the row's G
                     // a_j < cutl - b_i  <=>  E_j > G_i = 2^-cutl / 2^-b_i (2^-x is decreasing);
                     // G = inf for rows off the disc (2^-b_i flushed to zero)
                     rG[i] = __fmul_rn(P.gcut, rcp_approx(fb));
@@ -657,87 +692,113 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 unsigned todo = __ballot_sync(0xffffffffu, pm);
                 const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
                 const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
-                while (todo) {
-                    const int q = __ffs(todo) - 1, qq = q + 32 * hq;
-                    todo &= todo - 1u;
-                    const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
-                    const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
-                    const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                    const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
-                    const float4 f4 = *reinterpret_cast<const float4*>(pF);
-                    const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
-                    const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
-                    if (!COUNT && ((fullb >> q) & 1u)) {
-                        // the whole sub-block is inside the cutoff: one FFMA per cell
+#if MGK_DENSITY_SPLITLOOP
+                // the partials hold at most 32 points: flush before a half that would exceed that
+                const unsigned nh = (unsigned)__popc(todo);
+                if (pc + nh > 32u) {
+                    flush_partials(tS, tC, part);
+                    pc = 0;
+                }
+                pc += nh;
+                // fully-inside points first, then the partial ones; the counting
+                // variant takes the same order (through the compare path), so
+                // its raster is bitwise the plain variant's
+                unsigned rest = todo & ~fullb;
+                todo &= fullb;
+                if (!COUNT) {
+                    while (todo) {
+                        const int q = __ffs(todo) - 1, qq = q + 32 * hq;
+                        todo &= todo - 1u;
+                        const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
+                        const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
+                        const float4 e4a = *reinterpret_cast<const float4*>(pE);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
+                        const float4 f4 = *reinterpret_cast<const float4*>(pF);
+                        const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
+                        const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
                             for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
-                    } else {
-                        const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * 16 + tr * 4);
-                        const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
-                        unsigned inm = 0;
-                        if (COUNT) {
+                    }
+                    todo = rest;
+                    rest = 0u;
+                }
+#endif
+                for (;;) {  // one pass; with the split loops, a second over `rest`
+                    while (todo) {
+                        const int q = __ffs(todo) - 1, qq = q + 32 * hq;
+                        todo &= todo - 1u;
+                        const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
+                        const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
+                        const float4 e4a = *reinterpret_cast<const float4*>(pE);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
+                        const float4 f4 = *reinterpret_cast<const float4*>(pF);
+                        const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
+                        const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
+                        if (!COUNT && ((fullb >> q) & 1u)) {
+                            // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
                             for (int i = 0; i < 4; i++)
 #pragma unroll
-                                for (int j = 0; j < 8; j++) {
-                                    const bool in = rg[i] < ce[j];
-                                    if (in) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
-                                    inm |= (unsigned)in << (i * 8 + j);
-                                }
+                                for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
                         } else {
+                            const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * 16 + tr * 4);
+                            const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
+                            unsigned inm = 0;
+                            if (COUNT) {
 #pragma unroll
-                            for (int i = 0; i < 4; i++)
-#pragma unroll
-                                for (int j = 0; j < 8; j++) fma_if_less(part[i * 8 + j], rg[i], ce[j], ce[j], rv[i]);
-                        }
-                        if ((ambb >> q) & 1u) {
-                            // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
-                            const unsigned fl = (__shfl_sync(0xffffffffu, myflag, q) >> (tr * 4)) & 0xfu;
-                            if (fl) {
-                                const MgkPt r = st[qq];
-                                const float px = r.xh + r.xl, py = r.yh + r.yl;
-                                const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
-#pragma unroll
-                                for (int i = 0; i < 4; i++) {
-                                    if (!((fl >> i) & 1u)) continue;
+                                for (int i = 0; i < 4; i++)
 #pragma unroll
                                     for (int j = 0; j < 8; j++) {
-                                        const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
-                                                                     s_cyg[wr * 16 + tr * 4 + i]) < cut;
-                                        const bool fi = rg[i] < ce[j];
-                                        if (ex != fi) {
-                                            const float t = __fmul_rn(ce[j], rv[i]);
-                                            part[i * 8 + j] = __fadd_rn(part[i * 8 + j], ex ? t : -t);
-                                            if (COUNT) inm ^= 1u << (i * 8 + j);
+                                        const bool in = rg[i] < ce[j];
+                                        if (in) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
+                                        inm |= (unsigned)in << (i * 8 + j);
+                                    }
+                            } else {
+#pragma unroll
+                                for (int i = 0; i < 4; i++)
+#pragma unroll
+                                    for (int j = 0; j < 8; j++) fma_if_less(part[i * 8 + j], rg[i], ce[j], ce[j], rv[i]);
+                            }
+                            if ((ambb >> q) & 1u) {
+                                // some row of this sub-block has a column in the cutoff band: exact FP64 re-decision
+                                const unsigned fl = (__shfl_sync(0xffffffffu, myflag, q) >> (tr * 4)) & 0xfu;
+                                if (fl) {
+                                    const MgkPt r = st[qq];
+                                    const float px = r.xh + r.xl, py = r.yh + r.yl;
+                                    const double cut = VARH ? MGK_CUT * (double)r.hh : P.cut_d2;
+#pragma unroll
+                                    for (int i = 0; i < 4; i++) {
+                                        if (!((fl >> i) & 1u)) continue;
+#pragma unroll
+                                        for (int j = 0; j < 8; j++) {
+                                            const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
+                                                                         s_cyg[wr * 16 + tr * 4 + i]) < cut;
+                                            const bool fi = rg[i] < ce[j];
+                                            if (ex != fi) {
+                                                const float t = __fmul_rn(ce[j], rv[i]);
+                                                part[i * 8 + j] = __fadd_rn(part[i * 8 + j], ex ? t : -t);
+                                                if (COUNT) inm ^= 1u << (i * 8 + j);
+                                            }
                                         }
                                     }
                                 }
                             }
+                            if (COUNT) cnt += __popc(inm & valid);
                         }
-                        if (COUNT) cnt += __popc(inm & valid);
+#if !MGK_DENSITY_SPLITLOOP
+                        pc++;
+                        if ((pc & 31u) == 0) flush_partials(tS, tC, part);  // 32-point partials
+#endif
                     }
-                    pc++;
-                    if ((pc & 31u) == 0) {
-                        // 32-point partials into the Kahan accumulators in tensor memory
-                        __syncwarp();
-                        tmem_wait_st();  // the previous flush's stores have landed
-#pragma unroll
-                        for (int c = 0; c < 4; c++) {
-                            float sv[8], cv[8];
-                            tmem_ld8(tS + 8u * c, sv);
-                            tmem_ld8(tC + 8u * c, cv);
-                            tmem_wait_ld(sv, cv);
-#pragma unroll
-                            for (int u = 0; u < 8; u++) {
-                                kahan_add(sv[u], cv[u], part[c * 8 + u]);
-                                part[c * 8 + u] = 0.0f;
-                            }
-                            tmem_st8(tS + 8u * c, sv);
-                            tmem_st8(tC + 8u * c, cv);
-                        }
-                    }
+#if MGK_DENSITY_SPLITLOOP
+                    if (!rest) break;
+                    todo = rest;
+                    rest = 0u;
+#else
+                    break;
+#endif
                 }
             }
         }

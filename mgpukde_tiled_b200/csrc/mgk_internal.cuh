@@ -63,6 +63,9 @@ struct mgk_points {
     bool owns_h = false;  // h allocated by the adaptive search on points that do not own x/y/w/h
     double* dist2 = nullptr;
     bool has_dist2 = false;
+    // dist2 is exact for the points whose nearest boundary cell lies within
+    // dist2_cap (coordinate units); the others hold a value above dist2_cap^2
+    double dist2_cap = 0.0;
     float* ew = nullptr;
     bool has_ew = false;
 };
@@ -80,6 +83,7 @@ struct mgk_raster {
     int* cstart = nullptr;        // per bin: offsets of its candidate list in cand (nbins + 1)
     float2* cand = nullptr;       // candidate boundary-cell centres, bin by bin
     int64_t ncand = 0;
+    double cand_cap = -1.0;       // the lists hold the cells within this reach of each bin (< 0: no lists)
     int bnx = 0, bny = 0;         // boundary bins per row / column
     int64_t nbins = 0;
     int64_t nb = 0;
@@ -259,7 +263,7 @@ int mgk_density_plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid*
 int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
 int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
-int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, const mgk_raster* r);
+int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, mgk_raster* r, double cap);
 int mgk_launch_edge_weights(mgk_ctx* ctx, int64_t n, const float* x, const float* y, const float* hpp,
                             float h, const double* dist2, const mgk_raster* r, float* ew_out,
                             unsigned long long* d_evals);

@@ -181,7 +181,8 @@ int prepare(mgk_server* S, Job* J) {
     if (r.edge) {
         int64_t ev = 0;
         if ((st = mgk_raster_upload(c, &r.edge_grid, r.edge_mask, &J->em))) return st;
-        if ((st = mgk_boundary_dist(c, J->p, J->em))) return st;
+        // distances exact up to 3h: all the edge-weight short-circuit reads
+        if ((st = mgk_boundary_dist_within(c, J->p, J->em, 3.0 * (double)r.h * (1.0 + 1e-6)))) return st;
         if ((st = mgk_edge_weights(c, J->p, J->em, r.h, &ev))) return st;
         J->evals += ev;
     } else if ((st = mgk_edge_weights_unit(c, J->p))) {

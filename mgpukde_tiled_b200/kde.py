@@ -239,9 +239,15 @@ def mark_boundary(ctx: Context, raster: Raster) -> int:
     return nb.value
 
 
-def calc_dist2_boundary(ctx: Context, points: Points, raster: Raster) -> None:
-    """CalcDist2Boundary: exact FP64 squared distance of each point to the boundary."""
-    ctx.check(lib().mgk_boundary_dist(ctx.handle, points._h, raster._h))
+def calc_dist2_boundary(ctx: Context, points: Points, raster: Raster, reach=None) -> None:
+    """CalcDist2Boundary: exact FP64 squared distance of each point to the
+    boundary.  reach: exact only for points within that distance of the
+    boundary (the others get a value above reach^2); 3 h_max is all the edge
+    weights and likelihoods need (mgk_boundary_dist_within)."""
+    if reach is None:
+        ctx.check(lib().mgk_boundary_dist(ctx.handle, points._h, raster._h))
+    else:
+        ctx.check(lib().mgk_boundary_dist_within(ctx.handle, points._h, raster._h, float(reach)))
 
 
 def edge_correction_weights(ctx: Context, points: Points, raster: Raster, h: float, count=False):
