@@ -56,7 +56,7 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
                                                         const int32_t* __restrict__ bin_start, double ox,
                                                         double oy, double side, int64_t nbx, int64_t nby,
                                                         double reach, double h2, const float* __restrict__ bin_r2,
-                                                        double* __restrict__ psum,
+                                                        double quantum, double* __restrict__ psum,
                                                         unsigned long long* __restrict__ evals) {
     __shared__ __align__(16) MgkPt st[kPdB];
     __shared__ float bb[4][kPdQ / 32];
@@ -97,6 +97,10 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
     const float cutf = (float)cut;
     const double k2 = MGK_LOG2E / (2.0 * h2);
     const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
+    // squared hi-part distance beyond which a candidate is outside every
+    // cutoff of the window (the hi parts' difference is exact, the lo parts
+    // move d by at most two quanta; 1e-5 covers the float rounding)
+    const float far2 = (float)((reach + 2.0 * quantum) * (reach + 2.0 * quantum) * (1.0 + 1e-5));
     float s = 0.0f, c = 0.0f;
     unsigned cnt = 0;
     for (int64_t by = by0 + blockIdx.y; by <= by1 && bx0 <= bx1; by += gridDim.y) {
@@ -136,6 +140,8 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
             float part = 0.0f;
             for (int t = 0; t < m; t++) {
                 const MgkPt p = st[t];
+                const float dxh = __fsub_rn(p.xh, q.xh), dyh = __fsub_rn(p.yh, q.yh);
+                if (__fmaf_rn(dxh, dxh, __fmul_rn(dyh, dyh)) > far2) continue;
                 const float dx = __fadd_rn(__fsub_rn(p.xh, q.xh), __fsub_rn(p.xl, q.xl));
                 const float dy = __fadd_rn(__fsub_rn(p.yh, q.yh), __fsub_rn(p.yl, q.yl));
                 const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
@@ -280,15 +286,18 @@ int point_density(mgk_ctx* c, const mgk_index* idx, bool self, double* d_den, do
         k_bin_reach2<<<(unsigned)((nbins + 255) / 256), 256, 0, s>>>(nbins, idx->bin_start, idx->pts, r2);
         k_point_density<true, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
                                                            idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, r2, psum, pair_count(c));
+                                                           idx->h2, r2, std::ldexp(1.0, -idx->qexp), psum,
+                                                           pair_count(c));
     } else if (self) {
         k_point_density<false, true><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
                                                            idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
-                                                           idx->h2, nullptr, psum, pair_count(c));
+                                                           idx->h2, nullptr, std::ldexp(1.0, -idx->qexp), psum,
+                                                           pair_count(c));
     } else {
         k_point_density<false, false><<<grid, kPdQ, 0, s>>>(idx->n, idx->pts, idx->bin_start, idx->ox,
                                                             idx->oy, idx->side, idx->nbx, idx->nby, idx->reach,
-                                                            idx->h2, nullptr, psum, pair_count(c));
+                                                            idx->h2, nullptr, std::ldexp(1.0, -idx->qexp), psum,
+                                                            pair_count(c));
     }
     k_pd_combine<<<(unsigned)g, kPdQ, 0, s>>>(idx->n, nsplit, psum, idx->perm, idx->varh, idx->h2, floor_v, d_den,
                                               part);

@@ -763,13 +763,19 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
 #ifndef MGK_RASTER_BANDS
 #define MGK_RASTER_BANDS 8
 #endif
+// device buffers of each kind (mask in, density out) in flight
+#ifndef MGK_RASTER_DEPTH
+#define MGK_RASTER_DEPTH 3
+#endif
+
 namespace {
 constexpr int64_t kRasterBands = MGK_RASTER_BANDS;  // full-width bands without an explicit tile side
+constexpr int kDepth = MGK_RASTER_DEPTH;
 struct RasterPipe {
     cudaStream_t h2d = nullptr, d2h = nullptr;
-    cudaEvent_t mask_ready[2] = {}, done[2] = {}, out_free[2] = {};
+    cudaEvent_t mask_ready[kDepth] = {}, done[kDepth] = {}, out_free[kDepth] = {};
     ~RasterPipe() {
-        for (int i = 0; i < 2; i++) {
+        for (int i = 0; i < kDepth; i++) {
             if (mask_ready[i]) cudaEventDestroy(mask_ready[i]);
             if (done[i]) cudaEventDestroy(done[i]);
             if (out_free[i]) cudaEventDestroy(out_free[i]);
@@ -780,7 +786,7 @@ struct RasterPipe {
     cudaError_t init() {
         cudaError_t e = cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking);
-        for (int i = 0; i < 2 && e == cudaSuccess; i++) {
+        for (int i = 0; i < kDepth && e == cudaSuccess; i++) {
             e = cudaEventCreateWithFlags(&mask_ready[i], cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&out_free[i], cudaEventDisableTiming);
@@ -829,12 +835,12 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     mgk_points* p = nullptr;
     mgk_raster* em = nullptr;
     mgk_index* idx = nullptr;
-    float* d_mask[2] = {nullptr, nullptr};
-    float* d_out[2] = {nullptr, nullptr};
+    float* d_mask[kDepth] = {};
+    float* d_out[kDepth] = {};
     int64_t ev_edge = 0, ev_den = 0;
     const float hfix = h_pp ? 0.0f : h;
     int st = MGK_OK;
-    for (int i = 0; i < (ntiles > 1 ? 2 : 1) && st == MGK_OK; i++) {
+    for (int i = 0; i < (int)std::min<int64_t>(ntiles, kDepth) && st == MGK_OK; i++) {
         st = mgk_alloc(c, (void**)&d_out[i], tb);
         if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask[i], tb);
     }
@@ -851,13 +857,13 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         nr = std::min<int64_t>(tr, row_hi - r0);
         nc = std::min<int64_t>(tc, dg->ncols - c0);
     };
-    // mask of tile k into buffer k % 2, after the density of tile k - 2 read it
+    // mask of tile k into buffer k % kDepth, after the density of tile k - kDepth read it
     auto mask_in = [&](int64_t k) -> cudaError_t {
         if (!dmask || k >= ntiles) return cudaSuccess;
         int64_t r0, c0, nr, nc;
         tile_of(k, r0, c0, nr, nc);
-        const int b = (int)(k & 1);
-        cudaError_t e = k >= 2 ? cudaStreamWaitEvent(pipe.h2d, pipe.done[b], 0) : cudaSuccess;
+        const int b = (int)(k % kDepth);
+        cudaError_t e = k >= kDepth ? cudaStreamWaitEvent(pipe.h2d, pipe.done[b], 0) : cudaSuccess;
         if (e == cudaSuccess)
             e = cudaMemcpy2DAsync(d_mask[b], sizeof(float) * nc, dmask + (r0 - row_lo) * dg->ncols + c0,
                                   sizeof(float) * dg->ncols, sizeof(float) * nc, nr, cudaMemcpyHostToDevice, pipe.h2d);
@@ -909,7 +915,7 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         if (k < 0) return cudaSuccess;
         int64_t r0, c0, nr, nc;
         tile_of(k, r0, c0, nr, nc);
-        const int b = (int)(k & 1);
+        const int b = (int)(k % kDepth);
         cudaError_t e = cudaStreamWaitEvent(pipe.d2h, pipe.done[b], 0);
         if (e == cudaSuccess)
             e = cudaMemcpy2DAsync(out_density + (r0 - row_lo) * dg->ncols + c0, sizeof(float) * dg->ncols, d_out[b],
@@ -931,10 +937,10 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     auto plan_of = [&](int64_t k) -> int {  // after tile k's counting kernel has finished
         int64_t r0, c0, nr, nc;
         tile_of(k, r0, c0, nr, nc);
-        const int b = (int)(k & 1);
+        const int b = (int)(k & 1), db = (int)(k % kDepth);
         mgk_density_discard(c, plans[b]);  // tile k - 2's
         plans[b] = nullptr;
-        return mgk_density_plan_counted(c, idx, dg, r0, c0, nr, nc, d_mask[b], d_out[b], d_ev, 1 + b, &plans[b]);
+        return mgk_density_plan_counted(c, idx, dg, r0, c0, nr, nc, d_mask[db], d_out[db], d_ev, 1 + b, &plans[b]);
     };
     auto count_of = [&](int64_t k) -> int {
         int64_t r0, c0, nr, nc;
@@ -953,9 +959,14 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster plan");
         else st = plan_of(0);
     }
+    // the masks of the first kDepth - 1 tiles are on their way; tile k's loop
+    // step sends the one of tile k + kDepth - 1 (its buffer's last reader is
+    // tile k - 1's density)
+    for (int64_t k = 1; k < kDepth - 1 && st == MGK_OK; k++)
+        if ((ce = mask_in(k)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
     for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
-        const int b = (int)(k & 1);
-        ce = mask_in(k + 1);  // after tile k - 1's density has read that buffer
+        const int b = (int)(k & 1), db = (int)(k % kDepth);
+        ce = mask_in(k + kDepth - 1);
         if (ce != cudaSuccess) {
             st = mgk_cuda_fail(c, ce, "kde_raster mask");
             break;
@@ -967,14 +978,15 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
                 break;
             }
         }
-        if (dmask) ce = cudaStreamWaitEvent(c->stream, pipe.mask_ready[b], 0);
-        if (ce == cudaSuccess && k >= 2) ce = cudaStreamWaitEvent(c->stream, pipe.out_free[b], 0);
+        const cudaStream_t ks = c->stream;
+        if (dmask) ce = cudaStreamWaitEvent(ks, pipe.mask_ready[db], 0);
+        if (ce == cudaSuccess && k >= kDepth) ce = cudaStreamWaitEvent(ks, pipe.out_free[db], 0);
         if (ce != cudaSuccess) {
             st = mgk_cuda_fail(c, ce, "kde_raster tile");
             break;
         }
-        if ((st = mgk_density_launch_plan(c, plans[b], c->stream))) break;
-        ce = cudaEventRecord(pipe.done[b], c->stream);
+        if ((st = mgk_density_launch_plan(c, plans[b], ks))) break;
+        ce = cudaEventRecord(pipe.done[db], ks);
         if (ce == cudaSuccess) ce = out_copy(k);
         if (ce != cudaSuccess) {
             st = mgk_cuda_fail(c, ce, "kde_raster tile");
@@ -1000,7 +1012,7 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         else if (c->h_counter[7]) st = mgk_fail(c, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
         else ev_den = (int64_t)c->h_counter[4];
     }
-    for (int i = 0; i < 2; i++) {
+    for (int i = 0; i < kDepth; i++) {
         if (d_out[i]) mgk_free(c, d_out[i], tb);
         if (d_mask[i]) mgk_free(c, d_mask[i], tb);
     }

@@ -48,7 +48,14 @@ struct LevelDesc {
     const int32_t* qord;  // query order: record positions in Z-order of the bins
     double ox, oy, side, inv_side;
     int64_t nbx, nby;
+    double quantum;       // coordinate quantum of the records' hi/lo split
 };
+
+// Rejects most out-of-cutoff candidates on their hi parts (4 instructions)
+// before the exact pair arithmetic.
+#ifndef MGK_LOO_PREFILTER
+#define MGK_LOO_PREFILTER 1
+#endif
 
 struct LooParams {
     const LevelDesc* lev;  // [nlev], device
@@ -166,6 +173,9 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
         const double k2 = MGK_LOG2E / (2.0 * h2);
         const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
         const double reach = sqrt(cut) * (1.0 + 1e-9);
+        // squared hi-part distance beyond which a candidate is surely outside
+        // the cutoff (|lo parts| <= q / 2 each; 1e-5 covers the float rounding)
+        const float far2 = (float)((reach + 2.0 * L.quantum) * (reach + 2.0 * L.quantum) * (1.0 + 1e-5));
         const float* ewk = P.ew ? P.ew + (int64_t)k * P.ew_chunk : nullptr;
 
         // this item's query
@@ -261,6 +271,13 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
                 const MgkPt* st = stage[buf];
                 for (int t = 0; t < m; t++) {
                     const float4 cp = *reinterpret_cast<const float4*>(&st[t]);
+#if MGK_LOO_PREFILTER
+                    // the hi parts alone first: their difference is exact and
+                    // the lo parts move d by at most 2 quanta, so a candidate
+                    // beyond far2 is outside the cutoff (2 of 3 tested are)
+                    const float dxh = __fsub_rn(cp.x, q.xh), dyh = __fsub_rn(cp.y, q.yh);
+                    if (__fmaf_rn(dxh, dxh, __fmul_rn(dyh, dyh)) > far2) continue;
+#endif
                     const float dx = __fadd_rn(__fsub_rn(cp.x, q.xh), __fsub_rn(cp.z, q.xl));
                     const float dy = __fadd_rn(__fsub_rn(cp.y, q.yh), __fsub_rn(cp.w, q.yl));
                     const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));
@@ -482,7 +499,7 @@ int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster
     for (int l = 0; l < P.nlev; l++) {
         const mgk_index* I = B->lev[l];
         hl[l] = LevelDesc{I->pts, I->bin_start, I->perm, B->qord[l], I->ox, I->oy, I->side, 1.0 / I->side, I->nbx,
-                          I->nby};
+                          I->nby, std::ldexp(1.0, -I->qexp)};
         P.side[l] = I->side;
     }
     if (cudaMemcpy(B->d_lev, hl, sizeof(LevelDesc) * P.nlev, cudaMemcpyHostToDevice) != cudaSuccess) {
