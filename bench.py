@@ -1111,7 +1111,7 @@ def run_serving(args):
     if world > 1:
         raise SystemExit("serving runs one server per GPU (replicas only)")
     torch.cuda.set_device(local)
-    count = max(4, int(round(24 * args.scale)))
+    count = max(4, int(round(args.serve_requests * args.scale)))
     reqs = synth.serving_requests(count, seed=4)
     rates = [8.0, 32.0, 128.0, 512.0, 2048.0]
     rng = np.random.default_rng(7)
@@ -1155,7 +1155,9 @@ def run_serving(args):
            "data": "synthetic (seeded PCG64)",
            "config": {"workload": f"serving: {count} requests per rate, N lognormal [1e3, 2e6], side U[256, 8192], "
                                   f"h U[5, 100], edge correction on half; Poisson arrivals; one untimed "
-                                  f"pass of the request set first",
+                                  f"pass of the request set first; largest-first admission, up to 4 tiles per "
+                                  f"tick",
+                      "output_bytes": int(sum(o.nbytes for o in outs)),
                       "tile": 2048, "max_active": 8, "host_numa_node": getattr(args, "numa_node", None)},
            "p50_ms": top["p50_ms"], "p99_ms": top["p99_ms"], "sweep": rows,
            "server": {k: st[k] for k in ("ticks", "tiles", "max_batch", "completed")}}
@@ -1173,6 +1175,8 @@ def main():
     ap.add_argument("--scale", type=float, default=1.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp64-form", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=200,
+                    help="serving workload: requests per offered rate (p99 is taken over them)")
     ap.add_argument("--no-reference-gpu", action="store_true",
                     help="skip timing the reference program's own CUDA kernels on a crop")
     ap.add_argument("--no-accuracy", action="store_true",

@@ -97,10 +97,12 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
     const float cutf = (float)cut;
     const double k2 = MGK_LOG2E / (2.0 * h2);
     const float k2h = (float)k2, k2l = (float)(k2 - (double)k2h);
-    // squared hi-part distance beyond which a candidate is outside every
-    // cutoff of the window (the hi parts' difference is exact, the lo parts
-    // move d by at most two quanta; 1e-5 covers the float rounding)
+    // squared hi-part distance beyond which a candidate is outside its cutoff:
+    // the hi parts' difference is exact and the lo parts move d by at most
+    // two quanta, so (3h + 2q)^2 = 9h^2 + 12 h q + 4 q^2 bounds it (h <= the
+    // widest reach / 3; 1e-5 covers the float rounding).  Fixed h: one bound.
     const float far2 = (float)((reach + 2.0 * quantum) * (reach + 2.0 * quantum) * (1.0 + 1e-5));
+    const float far_add = (float)((4.0 * reach * quantum + 4.0 * quantum * quantum) * (1.0 + 1e-5));
     float s = 0.0f, c = 0.0f;
     unsigned cnt = 0;
     for (int64_t by = by0 + blockIdx.y; by <= by1 && bx0 <= bx1; by += gridDim.y) {
@@ -141,7 +143,8 @@ __global__ void __launch_bounds__(kPdQ) k_point_density(int64_t n, const MgkPt* 
             for (int t = 0; t < m; t++) {
                 const MgkPt p = st[t];
                 const float dxh = __fsub_rn(p.xh, q.xh), dyh = __fsub_rn(p.yh, q.yh);
-                if (__fmaf_rn(dxh, dxh, __fmul_rn(dyh, dyh)) > far2) continue;
+                const float lim = VARH ? __fmaf_rn(9.0f * p.hh, 1.00001f, far_add) : far2;
+                if (__fmaf_rn(dxh, dxh, __fmul_rn(dyh, dyh)) > lim) continue;
                 const float dx = __fadd_rn(__fsub_rn(p.xh, q.xh), __fsub_rn(p.xl, q.xl));
                 const float dy = __fadd_rn(__fsub_rn(p.yh, q.yh), __fsub_rn(p.yl, q.yl));
                 const float d2 = __fmaf_rn(dx, dx, __fmul_rn(dy, dy));

@@ -8,17 +8,22 @@
 //
 //  * admission: a queued request becomes active when the number of active
 //    requests is below the slot count and its estimated device footprint fits
-//    beside the active ones inside the budget;
+//    beside the active ones inside the budget; among the queued requests the
+//    one with the most tiles goes first (largest first keeps a big request
+//    from running alone at the end of a burst);
 //  * preparation: its points, index (and edge-correction weights) are built
 //    and stay resident on the device while it is active.  A second thread
 //    with a context of its own does this (admission, preparation, and the
 //    release of finished requests' memory), so new requests are prepared on
 //    the GPU while the worker's ticks run;
-//  * ticks: each tick takes the next tile of every active request (row-major
-//    tiles of tile_side x tile_side cells) and runs all of them in one density
-//    launch (mgk_launch_density_jobs).  Each request has two device output
-//    tiles: a tick's results are copied to the requests' host outputs on a
-//    second stream while the next tick computes into the other tiles.
+//  * ticks: each tick takes the next tiles of every active request (row-major
+//    tiles of tile_side x tile_side cells; one each when kTickTiles or more
+//    requests are active, else up to kTickTiles / active each, so that a
+//    request running alone still fills the GPU) and runs all of them in one
+//    density launch (mgk_launch_density_jobs).  Each request has
+//    2 kTickTiles device output tiles: a tick's results are copied to the
+//    requests' host outputs on a second stream while the next tick computes
+//    into the other tiles.
 //    Requests admitted between ticks join the next tick, so a short request
 //    that arrives while a large one is running finishes after a few ticks
 //    instead of waiting for the large one.  A request is complete when the
@@ -44,6 +49,10 @@ namespace {
 
 using Clock = std::chrono::steady_clock;
 
+// Tiles a tick takes in all: one per active request when that many are
+// active, else up to kTickTiles / active from each.
+constexpr int kTickTiles = 4;
+
 double ms_between(Clock::time_point a, Clock::time_point b) {
     return std::chrono::duration<double, std::milli>(b - a).count();
 }
@@ -68,10 +77,10 @@ struct Job {
     mgk_points* p = nullptr;
     mgk_raster* em = nullptr;
     mgk_index* idx = nullptr;
-    float* d_mask = nullptr;
-    float* d_out[2] = {nullptr, nullptr};  // tile k computes into d_out[k & 1]
-    cudaEvent_t out_free[2] = {nullptr, nullptr};  // the copy out of d_out[b] has finished
-    bool used[2] = {false, false};
+    float* d_mask[kTickTiles] = {};  // the masks of a tick's tiles
+    float* d_out[2 * kTickTiles] = {};  // tile k computes into d_out[k % (2 kTickTiles)]
+    cudaEvent_t out_free[2 * kTickTiles] = {};  // the copy out of d_out[b] has finished
+    bool used[2 * kTickTiles] = {};
     size_t tile_bytes = 0;
     int64_t tiles_x = 0, tiles_y = 0, next_tile = 0;
     int64_t evals = 0;
@@ -86,9 +95,9 @@ struct Res {
     mgk_points* p = nullptr;
     mgk_raster* em = nullptr;
     mgk_index* idx = nullptr;
-    float* d_mask = nullptr;
-    float* d_out[2] = {nullptr, nullptr};
-    cudaEvent_t out_free[2] = {nullptr, nullptr};
+    float* d_mask[kTickTiles] = {};
+    float* d_out[2 * kTickTiles] = {};
+    cudaEvent_t out_free[2 * kTickTiles] = {};
     size_t tile_bytes = 0;
 };
 }  // namespace
@@ -133,17 +142,23 @@ uint64_t estimate_bytes(const mgk_request& r, int64_t tile) {
     b += (uint64_t)(bins * 4.0);
     if (r.edge) b += (uint64_t)r.edge_grid.ncols * (uint64_t)r.edge_grid.nrows * 24;
     const uint64_t tr = (uint64_t)std::min<int64_t>(tile, r.grid.nrows), tc = (uint64_t)std::min<int64_t>(tile, r.grid.ncols);
-    b += 3 * tr * tc * 4;                                 // mask and two output tiles
+    b += 3 * kTickTiles * tr * tc * 4;                    // masks and output tiles
     b += ((tr + 63) / 64) * ((tc + 63) / 64) * 64 * 1024;  // split-block scratch and work list
     return b + b / 4 + (16u << 20);
+}
+
+// Density tiles of a request.
+int64_t tile_count(const mgk_server* S, const mgk_request& r) {
+    const int64_t tr = std::min<int64_t>(S->tile, r.grid.nrows), tc = std::min<int64_t>(S->tile, r.grid.ncols);
+    return ((r.grid.nrows + tr - 1) / tr) * ((r.grid.ncols + tc - 1) / tc);
 }
 
 void release(mgk_ctx* pc, Res& R) {
     mgk_index_destroy(R.idx);
     mgk_raster_destroy(R.em);
     mgk_points_destroy(R.p);
-    mgk_free(pc, R.d_mask, R.tile_bytes);
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kTickTiles; b++) mgk_free(pc, R.d_mask[b], R.tile_bytes);
+    for (int b = 0; b < 2 * kTickTiles; b++) {
         mgk_free(pc, R.d_out[b], R.tile_bytes);
         if (R.out_free[b]) cudaEventDestroy(R.out_free[b]);
     }
@@ -156,9 +171,12 @@ Res take(Job* J) {
     R.p = J->p;
     R.em = J->em;
     R.idx = J->idx;
-    R.d_mask = J->d_mask;
     R.tile_bytes = J->tile_bytes;
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kTickTiles; b++) {
+        R.d_mask[b] = J->d_mask[b];
+        J->d_mask[b] = nullptr;
+    }
+    for (int b = 0; b < 2 * kTickTiles; b++) {
         R.d_out[b] = J->d_out[b];
         R.out_free[b] = J->out_free[b];
         J->d_out[b] = nullptr;
@@ -167,7 +185,6 @@ Res take(Job* J) {
     J->p = nullptr;
     J->em = nullptr;
     J->idx = nullptr;
-    J->d_mask = nullptr;
     return R;
 }
 
@@ -193,13 +210,15 @@ int prepare(mgk_server* S, Job* J) {
     J->tile_bytes = sizeof(float) * (size_t)tr * (size_t)tc;
     J->tiles_x = (r.grid.ncols + tc - 1) / tc;
     J->tiles_y = (r.grid.nrows + tr - 1) / tr;
-    const int nbuf = J->tiles_x * J->tiles_y > 1 ? 2 : 1;
+    const int64_t ntiles = J->tiles_x * J->tiles_y;
+    const int nbuf = (int)std::min<int64_t>(ntiles, 2 * kTickTiles);
     for (int b = 0; b < nbuf; b++) {
         if ((st = mgk_alloc(c, (void**)&J->d_out[b], J->tile_bytes))) return st;
         const cudaError_t e = cudaEventCreateWithFlags(&J->out_free[b], cudaEventDisableTiming);
         if (e != cudaSuccess) return mgk_cuda_fail(c, e, "serve: event");
     }
-    if (r.mask && (st = mgk_alloc(c, (void**)&J->d_mask, J->tile_bytes))) return st;
+    for (int b = 0; r.mask && b < (int)std::min<int64_t>(ntiles, kTickTiles); b++)
+        if ((st = mgk_alloc(c, (void**)&J->d_mask[b], J->tile_bytes))) return st;
     J->next_tile = 0;
     const cudaError_t e = cudaStreamSynchronize(c->stream);  // the worker's stream reads all of it
     if (e != cudaSuccess) return mgk_cuda_fail(c, e, "serve: preparation");
@@ -224,7 +243,7 @@ void finish(mgk_server* S, Job* J, int status) {
 }
 
 // The copy out of a job's last tile: its buffer's out_free event.
-cudaEvent_t last_copy(const Job* J) { return J->out_free[(J->next_tile - 1) & 1]; }
+cudaEvent_t last_copy(const Job* J) { return J->out_free[(J->next_tile - 1) % (2 * kTickTiles)]; }
 
 // Completes the draining jobs whose last copy has landed (all of them when
 // wait is set).
@@ -244,41 +263,49 @@ void reap(mgk_server* S, bool wait) {
     }
 }
 
-// One tick: the next tile of every active, prepared request in one launch;
-// the tiles' copies to the host are queued on the copy stream and overlap the
-// next tick.
+// One tick: the next tiles of every active, prepared request in one launch
+// (up to kTickTiles / active each, at least one); the tiles' copies to the
+// host are queued on the copy stream and overlap the next tick.
 void tick(mgk_server* S, std::vector<Job*>& act) {
     mgk_ctx* c = S->ctx;
     cudaStream_t s = c->stream;
     std::vector<mgk_tile_job> tj;
     std::vector<Job*> owner;
-    std::vector<int64_t> r0s, c0s;
+    std::vector<int64_t> r0s, c0s, tiles;
+    const int quota = std::max(1, kTickTiles / std::max(1, (int)act.size()));
     int st = MGK_OK;
     for (Job* J : act) {
         const mgk_request& r = J->req;
         const int64_t tr = std::min<int64_t>(S->tile, r.grid.nrows), tc = std::min<int64_t>(S->tile, r.grid.ncols);
-        const int64_t ty = J->next_tile / J->tiles_x, tx = J->next_tile % J->tiles_x;
-        const int64_t r0 = ty * tr, c0 = tx * tc;
-        const int64_t nr = std::min(tr, r.grid.nrows - r0), nc = std::min(tc, r.grid.ncols - c0);
-        const int b = (int)(J->next_tile & 1);
-        // the tile buffer's previous copy out must have finished before it is rewritten
-        if (J->used[b] && cudaStreamWaitEvent(s, J->out_free[b], 0) != cudaSuccess) {
-            st = MGK_ERR_CUDA;
-            break;
-        }
-        if (r.mask) {
-            const cudaError_t e = cudaMemcpy2DAsync(J->d_mask, sizeof(float) * nc, r.mask + r0 * r.grid.ncols + c0,
-                                                    sizeof(float) * r.grid.ncols, sizeof(float) * nc, nr,
-                                                    cudaMemcpyHostToDevice, s);
-            if (e != cudaSuccess) {
-                st = mgk_cuda_fail(c, e, "serve: tile mask");
+        const int64_t ntiles = J->tiles_x * J->tiles_y;
+        for (int q = 0; q < quota && J->next_tile + q < ntiles && st == MGK_OK; q++) {
+            const int64_t t = J->next_tile + q;
+            const int64_t ty = t / J->tiles_x, tx = t % J->tiles_x;
+            const int64_t r0 = ty * tr, c0 = tx * tc;
+            const int64_t nr = std::min(tr, r.grid.nrows - r0), nc = std::min(tc, r.grid.ncols - c0);
+            const int b = (int)(t % (2 * kTickTiles));
+            // the tile buffer's previous copy out must have finished before it is rewritten
+            if (J->used[b] && cudaStreamWaitEvent(s, J->out_free[b], 0) != cudaSuccess) {
+                st = MGK_ERR_CUDA;
                 break;
             }
+            // a tick's masks: the previous tick's kernels read these buffers earlier on this stream
+            if (r.mask) {
+                const cudaError_t e = cudaMemcpy2DAsync(J->d_mask[q], sizeof(float) * nc, r.mask + r0 * r.grid.ncols + c0,
+                                                        sizeof(float) * r.grid.ncols, sizeof(float) * nc, nr,
+                                                        cudaMemcpyHostToDevice, s);
+                if (e != cudaSuccess) {
+                    st = mgk_cuda_fail(c, e, "serve: tile mask");
+                    break;
+                }
+            }
+            tj.push_back(mgk_tile_job{J->idx, r.grid, r0, c0, nr, nc, r.mask ? J->d_mask[q] : nullptr, J->d_out[b]});
+            owner.push_back(J);
+            r0s.push_back(r0);
+            c0s.push_back(c0);
+            tiles.push_back(t);
         }
-        tj.push_back(mgk_tile_job{J->idx, r.grid, r0, c0, nr, nc, r.mask ? J->d_mask : nullptr, J->d_out[b]});
-        owner.push_back(J);
-        r0s.push_back(r0);
-        c0s.push_back(c0);
+        if (st) break;
     }
     unsigned long long* d_ev = nullptr;
     const size_t bev = sizeof(unsigned long long) * std::max<size_t>(tj.size(), 1);
@@ -305,7 +332,7 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
     for (size_t k = 0; k < tj.size() && st == MGK_OK; k++) {
         Job* J = owner[k];
         const mgk_request& r = J->req;
-        const int b = (int)(J->next_tile & 1);
+        const int b = (int)(tiles[k] % (2 * kTickTiles));
         cudaError_t e = cudaMemcpy2DAsync(r.out + r0s[k] * r.grid.ncols + c0s[k], sizeof(float) * r.grid.ncols,
                                           tj[k].d_out, sizeof(float) * tj[k].ncols, sizeof(float) * tj[k].ncols,
                                           tj[k].nrows, cudaMemcpyDeviceToHost, S->d2h);
@@ -319,15 +346,18 @@ void tick(mgk_server* S, std::vector<Job*>& act) {
         S->tiles += tj.size();
         S->max_batch = std::max<uint64_t>(S->max_batch, tj.size());
     }
-    for (size_t k = 0; k < owner.size(); k++) {
-        Job* J = owner[k];
+    for (Job* J : act) {
         if (st) {
             cudaStreamSynchronize(S->d2h);  // nothing of the job stays in flight
             finish(S, J, st);
             continue;
         }
-        J->evals += (int64_t)ev[k];
-        if (++J->next_tile == J->tiles_x * J->tiles_y) {
+        for (size_t k = 0; k < owner.size(); k++)
+            if (owner[k] == J) {
+                J->evals += (int64_t)ev[k];
+                J->next_tile++;
+            }
+        if (J->next_tile == J->tiles_x * J->tiles_y) {
             std::lock_guard<std::mutex> lk(S->mu);
             S->active.erase(std::remove(S->active.begin(), S->active.end(), J), S->active.end());
             S->draining.push_back(J);
@@ -371,11 +401,18 @@ void prep_main(mgk_server* S) {
         std::vector<Job*> fresh;
         {
             std::unique_lock<std::mutex> lk(S->mu);
+            // the queued request with the most tiles (the earliest on ties) goes first
+            auto pick = [&]() -> std::deque<Job*>::iterator {
+                auto best = S->queue.begin();
+                for (auto it = S->queue.begin(); it != S->queue.end(); ++it)
+                    if (tile_count(S, (*it)->req) > tile_count(S, (*best)->req)) best = it;
+                return best;
+            };
             auto admissible = [&] {
                 if (S->queue.empty()) return false;
                 const int held = (int)(S->active.size() + S->draining.size()) + S->preparing;
                 if (held >= S->max_active) return false;
-                return held == 0 || S->reserved + S->queue.front()->est <= S->budget;
+                return held == 0 || S->reserved + (*pick())->est <= S->budget;
             };
             auto idle = [&] {
                 return S->stop && S->queue.empty() && S->preparing == 0 && S->active.empty() &&
@@ -387,8 +424,9 @@ void prep_main(mgk_server* S) {
             }
             rel.swap(S->to_release);
             while (admissible()) {
-                Job* J = S->queue.front();
-                S->queue.pop_front();
+                const auto it = pick();
+                Job* J = *it;
+                S->queue.erase(it);
                 J->state = 1;
                 J->t_start = Clock::now();
                 S->reserved += J->est;
@@ -437,9 +475,9 @@ int mgk_serve_create(int device, uint64_t hbm_budget_bytes, int64_t tile_side, i
     S->tile = tile_side;
     S->max_active = max_active;
     S->budget = c->budget;
-    S->ev_cap = max_active;
+    S->ev_cap = std::max(max_active, kTickTiles);
     if (cudaStreamCreateWithFlags(&S->d2h, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaHostAlloc((void**)&S->h_ev, sizeof(unsigned long long) * (size_t)max_active, cudaHostAllocMapped) !=
+        cudaHostAlloc((void**)&S->h_ev, sizeof(unsigned long long) * (size_t)S->ev_cap, cudaHostAllocMapped) !=
             cudaSuccess ||
         cudaHostGetDevicePointer((void**)&S->d_ev_map, S->h_ev, 0) != cudaSuccess) {
         if (S->h_ev) cudaFreeHost(S->h_ev);
