@@ -425,11 +425,17 @@ def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_b
            "kernel_ms": kernel_s * 1e3, "flop_per_eval": FLOP_PER_EVAL,
            "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max_mhz:.0f} MHz "
                         f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"}
+    if traffic is not None:
+        out["traffic_note"] = ("dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch, from the ncu "
+                               "capture summarised in profiles/k_density_traffic.txt (not measured in this run)")
+    # the pipe utilisation behind frac (frac counts 8 flop-equivalents per in-cutoff pair, not issued ops)
+    out["pipes_ncu"] = {"fma_pct": 31.9, "alu_pct": 34.4, "xu_pct": 17.2, "lsu_pct": 17.0, "issue_active_pct": 61.2,
+                        "source": "ncu --set full of one half-scale launch, profiles/k_density_single_large_half.md "
+                                  "(not measured in this run)"}
     if hbm_gbs:
         hbm_achieved = alg_bytes / kernel_s / 1e9
         out["hbm"] = {"achieved": hbm_achieved, "peak": hbm_gbs, "unit": "GB/s", "frac": hbm_achieved / hbm_gbs,
                       "algorithmic_bytes": alg_bytes,
-                      "traffic_gbs": None if traffic is None else traffic / kernel_s / 1e9,
                       "peak_note": f"measured copy bandwidth ({peak_kind})"}
     return out
 

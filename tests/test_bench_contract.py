@@ -60,11 +60,14 @@ def test_density_roofline_fields():
     assert r["traffic"] == 850_600_000 and abs(r["kernel_ms"] - 10.0) < 1e-9
     h = r["hbm"]
     assert h["unit"] == "GB/s" and h["peak"] == 6454.6
-    assert abs(h["achieved"] - 80.0) < 1e-9 and abs(h["traffic_gbs"] - 85.06) < 1e-9
+    assert abs(h["achieved"] - 80.0) < 1e-9 and "traffic_gbs" not in h
     assert abs(h["frac"] - 80.0 / 6454.6) < 1e-12
-    # no measured HBM figure, no traffic capture: the FP32 view alone / no traffic rate
+    # the captured traffic and pipe figures say where they come from
+    assert "profiles/k_density_traffic.txt" in r["traffic_note"]
+    assert r["pipes_ncu"]["fma_pct"] > 0 and "profiles/" in r["pipes_ncu"]["source"]
+    # no measured HBM figure, no traffic capture: the FP32 view alone, no traffic note
     assert "hbm" not in bench.density_roofline(1e9, 0.01, 148, 1965.0, "fallback", None, 1, None)
-    assert bench.density_roofline(1e9, 0.01, 148, 1965.0, "measured", None, 8, 6000.0)["hbm"]["traffic_gbs"] is None
+    assert "traffic_note" not in bench.density_roofline(1e9, 0.01, 148, 1965.0, "measured", None, 8, 6000.0)
 
 
 def _oracle_study(scale):
