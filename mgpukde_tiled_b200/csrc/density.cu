@@ -863,8 +863,8 @@ __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DPar
     density_item<VARH, COUNT>(P, P.items[blockIdx.x]);
 }
 
-// The job parameters live in mapped host memory: each CTA copies its job's
-// into shared memory once instead of reading them over the bus.
+// Each CTA copies its job's parameters (device memory) into shared memory
+// once; the item loop then reads them from there.
 __device__ __forceinline__ void load_job(const DParams* jobs, int j, DParams& dst) {
     static_assert(sizeof(DParams) % 8 == 0, "DParams is copied in 8-byte words");
     const unsigned long long* src = reinterpret_cast<const unsigned long long*>(jobs + j);
@@ -1095,9 +1095,9 @@ void sort_items(std::vector<Item>& items) {
 
 }  // namespace
 
-// A planned density launch: work items and split tables in the context's
-// mapped staging (read by the kernels in place), scratch allocated, kernels
-// not yet launched.
+// A planned density launch: work items and split tables written to the
+// context's mapped staging (copied to device memory ahead of each launch),
+// scratch allocated, kernels not yet launched.
 struct mgk_dplan {
     const mgk_index* idx = nullptr;
     bool fp64 = false, count = false;
@@ -1106,12 +1106,40 @@ struct mgk_dplan {
     const int32_t *d_sb = nullptr, *d_sbeg = nullptr;
     unsigned long long *h_err = nullptr, *d_err = nullptr;
     size_t b_scr = 0;
+    // device copy of the work list and split tables, refreshed from the
+    // staging ahead of each launch
+    void* d_tab = nullptr;
+    const void* src_tab = nullptr;
+    size_t b_tab = 0;
 };
 
 static void dplan_release(mgk_ctx* ctx, mgk_dplan* D) {
     if (!D) return;
     if (D->T.nslots) mgk_free(ctx, D->P.scratch, D->b_scr);
+    if (D->d_tab) mgk_free(ctx, D->d_tab, D->b_tab);
     delete D;
+}
+
+// n16 16-byte words from the mapped staging to device memory.
+__global__ void k_stage_copy(uint4* __restrict__ dst, const uint4* src, size_t n16) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n16; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = src[i];
+}
+
+// The kernels read the work list and split tables from device memory: a
+// copy kernel moves them there from the mapped staging ahead of each launch,
+// on the launch's stream.  Read in place, each CTA's item would cross the
+// bus on its own, slowly while bulk copies (masks in, densities out) load it.
+static int stage_tables(mgk_ctx* ctx, const mgk_dplan* D, cudaStream_t s) {
+    if (!D->d_tab) return MGK_OK;
+    const size_t n16 = D->b_tab / 16;
+    const unsigned grid = (unsigned)std::max<size_t>(1, std::min<size_t>((size_t)ctx->sm_count, (n16 + 255) / 256));
+    k_stage_copy<<<grid, 256, 0, s>>>(reinterpret_cast<uint4*>(D->d_tab), reinterpret_cast<const uint4*>(D->src_tab),
+                                      n16);
+    const cudaError_t ce = cudaGetLastError();
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density work list");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    return MGK_OK;
 }
 
 void mgk_density_discard(mgk_ctx* ctx, mgk_dplan* D) { dplan_release(ctx, D); }
@@ -1186,9 +1214,17 @@ static int plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
         memcpy(h_st + o_sb, T.split_blocks.data(), b_sb);
         memcpy(h_st + o_sbeg, T.split_begin.data(), b_sbeg);
     }
-    P.items = reinterpret_cast<const Item*>(d_st);
-    D->d_sb = reinterpret_cast<const int32_t*>(d_st + o_sb);
-    D->d_sbeg = reinterpret_cast<const int32_t*>(d_st + o_sbeg);
+    D->b_tab = o_err;  // items and split tables (a 16-byte multiple)
+    if ((st = mgk_alloc(ctx, &D->d_tab, D->b_tab))) {
+        D->d_tab = nullptr;
+        dplan_release(ctx, D);
+        return st;
+    }
+    D->src_tab = d_st;
+    const char* d_tab = static_cast<const char*>(D->d_tab);
+    P.items = reinterpret_cast<const Item*>(d_tab);
+    D->d_sb = reinterpret_cast<const int32_t*>(d_tab + o_sb);
+    D->d_sbeg = reinterpret_cast<const int32_t*>(d_tab + o_sbeg);
     D->h_err = reinterpret_cast<unsigned long long*>(h_st + o_err);
     D->d_err = reinterpret_cast<unsigned long long*>(d_st + o_err);
     *D->h_err = 0;
@@ -1224,6 +1260,8 @@ int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
     const DParams& P = D->P;
     const bool varh = D->idx->varh;
     const unsigned grid = (unsigned)D->T.items.size();
+    const int st = stage_tables(ctx, D, s);
+    if (st) return st;
     if (D->count) {
         if (varh) launch_density<true, true>(grid, s, P);
         else launch_density<false, true>(grid, s, P);
@@ -1250,6 +1288,7 @@ int mgk_density_execute(mgk_ctx* ctx, mgk_dplan* D) {
     int rc = MGK_OK;
     do {
         const unsigned grid = (unsigned)D->T.items.size();
+        if ((rc = stage_tables(ctx, D, s))) break;
         cudaEventRecord(ctx->ev_a, s);
         if (D->fp64) {
             if (idx->varh) k_density_fp64<true><<<grid, kThreads, 0, s>>>(P);
@@ -1372,10 +1411,20 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
     if (!merges.empty()) memcpy(h_st + o_mg, merges.data(), sizeof(int4) * merges.size());
     volatile unsigned long long* h_err = reinterpret_cast<unsigned long long*>(h_st + o_err);
     *h_err = 0;
-    const DParams* d_jobs = reinterpret_cast<const DParams*>(d_st);
-    const Item* d_items = reinterpret_cast<const Item*>(d_st + o_items);
-    const int4* d_mg = reinterpret_cast<const int4*>(d_st + o_mg);
+    // the job parameters, items and merges in device memory (stage_tables)
+    mgk_dplan tabs;
+    tabs.b_tab = o_err;
+    tabs.src_tab = d_st;
+    if ((st = mgk_alloc(ctx, &tabs.d_tab, tabs.b_tab))) {
+        mgk_free(ctx, d_scr, b_scr);
+        return st;
+    }
+    const char* d_tab = static_cast<const char*>(tabs.d_tab);
+    const DParams* d_jobs = reinterpret_cast<const DParams*>(d_tab);
+    const Item* d_items = reinterpret_cast<const Item*>(d_tab + o_items);
+    const int4* d_mg = reinterpret_cast<const int4*>(d_tab + o_mg);
     do {
+        if ((st = stage_tables(ctx, &tabs, s))) break;
         cudaEventRecord(ctx->ev_a, s);
         if (!items_fix.empty()) {
             if (d_evals) launch_density_jobs<false, true>((unsigned)items_fix.size(), s, d_jobs, d_items);
@@ -1403,8 +1452,11 @@ int mgk_launch_density_jobs(mgk_ctx* ctx, int njobs, const mgk_tile_job* jobs, u
         if (ce == cudaSuccess) cudaEventElapsedTime(&ctx->last_density_ms, ctx->ev_a, ctx->ev_b);
     } while (0);
     if (ce != cudaSuccess) st = mgk_cuda_fail(ctx, ce, "density jobs");
-    else if (*h_err) st = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    else if (st == MGK_OK && *h_err) st = mgk_fail(ctx, MGK_ERR_TIMEOUT, "density: a shared-memory staging wait timed out");
+    if (st != MGK_OK && ce == cudaSuccess) (void)cudaStreamSynchronize(s);  // nothing in flight reads the tables
     mgk_free(ctx, d_scr, b_scr);
+    mgk_free(ctx, tabs.d_tab, tabs.b_tab);
+    tabs.d_tab = nullptr;
     return st;
 }
 
