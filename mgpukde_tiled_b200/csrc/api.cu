@@ -1,10 +1,13 @@
 // C ABI of libmgk (include/mgk.h): contexts, device-resident objects, and the
 // host-side sequencing of the path (the GPU section of the reference's
 // main(), kde_cuda_kdtr_tiled.cu:877-1521, for one GPU).
+#include <cudaTypedefs.h>
+
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -771,25 +774,84 @@ int mgk_mle_fixed_bandwidth(mgk_ctx* c, mgk_points* p, const mgk_raster* r, floa
 namespace {
 constexpr int64_t kRasterBands = MGK_RASTER_BANDS;  // full-width bands without an explicit tile side
 constexpr int kDepth = MGK_RASTER_DEPTH;
+
+// cuStreamWaitValue32 / cuStreamWriteValue32 through the runtime's driver
+// entry points (no link-time dependency on the driver library).
+struct StreamMemOps {
+    PFN_cuStreamWaitValue32_v11070 wait = nullptr;
+    PFN_cuStreamWriteValue32_v11070 write = nullptr;
+};
+const StreamMemOps& stream_memops() {
+    static StreamMemOps ops;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *w = nullptr, *v = nullptr;
+        cudaDriverEntryPointQueryResult q1 = cudaDriverEntryPointSymbolNotFound, q2 = q1;
+        if (cudaGetDriverEntryPointByVersion("cuStreamWaitValue32", &w, 11070, cudaEnableDefault, &q1) ==
+                cudaSuccess &&
+            q1 == cudaDriverEntryPointSuccess &&
+            cudaGetDriverEntryPointByVersion("cuStreamWriteValue32", &v, 11070, cudaEnableDefault, &q2) ==
+                cudaSuccess &&
+            q2 == cudaDriverEntryPointSuccess) {
+            ops.wait = reinterpret_cast<PFN_cuStreamWaitValue32_v11070>(w);
+            ops.write = reinterpret_cast<PFN_cuStreamWriteValue32_v11070>(v);
+        }
+        (void)cudaGetLastError();
+    });
+    return ops;
+}
+
+// Whether stream memory operations work on the context's device: checked
+// once per device with a write and a wait that the write satisfies.
+bool stream_memops_work(mgk_ctx* c) {
+    static std::mutex mu;
+    static std::map<int, bool> ok_by_device;
+    std::lock_guard<std::mutex> lk(mu);
+    auto f = ok_by_device.find(c->device);
+    if (f != ok_by_device.end()) return f->second;
+    const StreamMemOps& ops = stream_memops();
+    bool ok = false;
+    void* d = nullptr;
+    if (ops.wait && ops.write && mgk_alloc(c, &d, 256) == MGK_OK) {
+        const CUdeviceptr a = (CUdeviceptr)(uintptr_t)d;
+        ok = ops.write((CUstream)c->stream, a, 1u, CU_STREAM_WRITE_VALUE_DEFAULT) == CUDA_SUCCESS &&
+             ops.wait((CUstream)c->stream, a, 1u, CU_STREAM_WAIT_VALUE_GEQ) == CUDA_SUCCESS &&
+             cudaStreamSynchronize(c->stream) == cudaSuccess;
+        (void)cudaGetLastError();
+        mgk_free(c, d, 256);
+    }
+    ok_by_device[c->device] = ok;
+    return ok;
+}
 struct RasterPipe {
-    cudaStream_t h2d = nullptr, d2h = nullptr;
-    cudaEvent_t mask_ready[kDepth] = {}, done[kDepth] = {}, out_free[kDepth] = {};
+    cudaStream_t h2d = nullptr, d2h = nullptr, alt = nullptr, mrg = nullptr;
+    cudaEvent_t mask_ready[kDepth] = {}, done[kDepth] = {}, out_free[kDepth] = {}, dens[kDepth] = {};
     ~RasterPipe() {
         for (int i = 0; i < kDepth; i++) {
             if (mask_ready[i]) cudaEventDestroy(mask_ready[i]);
             if (done[i]) cudaEventDestroy(done[i]);
             if (out_free[i]) cudaEventDestroy(out_free[i]);
+            if (dens[i]) cudaEventDestroy(dens[i]);
         }
         if (h2d) cudaStreamDestroy(h2d);
         if (d2h) cudaStreamDestroy(d2h);
+        if (alt) cudaStreamDestroy(alt);
+        if (mrg) cudaStreamDestroy(mrg);
     }
     cudaError_t init() {
         cudaError_t e = cudaStreamCreateWithFlags(&h2d, cudaStreamNonBlocking);
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&d2h, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&alt, cudaStreamNonBlocking);
+        // the merges of split blocks at the highest priority: a band's merge
+        // is scheduled ahead of the next band's pending CTAs
+        int least = 0, greatest = 0;
+        if (e == cudaSuccess) e = cudaDeviceGetStreamPriorityRange(&least, &greatest);
+        if (e == cudaSuccess) e = cudaStreamCreateWithPriority(&mrg, cudaStreamNonBlocking, greatest);
         for (int i = 0; i < kDepth && e == cudaSuccess; i++) {
             e = cudaEventCreateWithFlags(&mask_ready[i], cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&done[i], cudaEventDisableTiming);
             if (e == cudaSuccess) e = cudaEventCreateWithFlags(&out_free[i], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&dens[i], cudaEventDisableTiming);
         }
         return e;
     }
@@ -821,9 +883,12 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         tr = std::max<int64_t>(256, ((nrows + kRasterBands - 1) / kRasterBands + 63) / 64 * 64);
         tr = std::min<int64_t>(tr, nrows);
         tc = dg->ncols;
-        const int64_t tail = nrows > 2 * 256 ? 256 : 0;
-        for (int64_t r0 = row_lo; r0 < row_hi - tail; r0 += tr) band_r0.push_back(r0);
-        if (tail) band_r0.push_back(row_hi - tail);
+        // the last band: the rows from the first 64-row block boundary at
+        // most 256 rows before the end (band boundaries are block boundaries,
+        // and no band is taller than tr)
+        const int64_t tail_r0 = nrows > 2 * 256 ? row_lo + (nrows - 256 + 63) / 64 * 64 : row_hi;
+        for (int64_t r0 = row_lo; r0 < tail_r0; r0 += tr) band_r0.push_back(r0);
+        if (tail_r0 < row_hi) band_r0.push_back(tail_r0);
         band_r0.push_back(row_hi);
     }
     const int64_t ntc = (dg->ncols + tc - 1) / tc;
@@ -955,16 +1020,86 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         const size_t nblk = (size_t)((tr + 63) / 64) * (size_t)((tc + 127) / 128);
         st = mgk_host_stage_slot(c, i, 64 * nblk + 4096, &hs, &ds);
     }
-    if (st == MGK_OK && ntiles > 0 && (st = count_of(0)) == MGK_OK) {
+    std::vector<mgk_dplan*> band_plans;
+    unsigned* d_flag = nullptr;  // [band] its last CTA has started
+    if (st == MGK_OK && !band_r0.empty()) {
+        // ---- full-width bands ----
+        // One count of all rows; each band planned from its slice while the
+        // one before computes.  With stream memory operations the bands
+        // alternate over two streams and band k waits for band k - 1's last
+        // CTA to start, so its CTAs fill the SMs that band k - 1's tail
+        // frees; a stream write after each band ends that wait in any case.
+        const StreamMemOps& ops = stream_memops();
+        const bool two = stream_memops_work(c);
+        if (two && (st = mgk_alloc(c, (void**)&d_flag, sizeof(unsigned) * ntiles)) == MGK_OK &&
+            (ce = cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * ntiles, c->stream)) != cudaSuccess)
+            st = mgk_cuda_fail(c, ce, "kde_raster flags");
+        if (st == MGK_OK) st = mgk_density_counts_launch(c, idx, dg, row_lo, 0, nrows, dg->ncols, 0, c->stream);
+        if (st == MGK_OK && (ce = cudaStreamSynchronize(c->stream)) != cudaSuccess)
+            st = mgk_cuda_fail(c, ce, "kde_raster plan");
+        // the alternate stream follows the preparation on the context stream
+        if (st == MGK_OK && two && ((ce = cudaEventRecord(counted, c->stream)) != cudaSuccess ||
+                                    (ce = cudaStreamWaitEvent(pipe.alt, counted, 0)) != cudaSuccess))
+            st = mgk_cuda_fail(c, ce, "kde_raster");
+        const int64_t* counts = st == MGK_OK ? mgk_density_counts_host(c, 0) : nullptr;
+        const int64_t nbx = (dg->ncols + 127) / 128;
+        band_plans.assign(ntiles, nullptr);
+        for (int64_t k = 1; k < kDepth - 1 && st == MGK_OK; k++)
+            if ((ce = mask_in(k)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
+        for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
+            const int db = (int)(k % kDepth);
+            const cudaStream_t ks = two && (k & 1) ? pipe.alt : c->stream;
+            // band k - 2 staged its work list from the same slot before its density
+            if (k >= 2 && (ce = cudaEventSynchronize(pipe.done[(k - 2) % kDepth])) != cudaSuccess) {
+                st = mgk_cuda_fail(c, ce, "kde_raster plan");
+                break;
+            }
+            const int64_t r0 = band_r0[k], nr = band_r0[k + 1] - r0;
+            if (nr > tr || (r0 - row_lo) % 64) {  // the buffers hold tr rows; plans slice whole block rows
+                st = mgk_fail(c, MGK_ERR_INVALID, "kde_raster: band layout");
+                break;
+            }
+            if ((st = mgk_density_plan_from_counts(c, idx, dg, r0, 0, nr, dg->ncols, counts + (r0 - row_lo) / 64 * nbx,
+                                                   d_mask[db], d_out[db], d_ev, 1 + (int)(k & 1), &band_plans[k])))
+                break;
+            if (two) mgk_density_set_tail_flag(band_plans[k], d_flag + k);
+            ce = mask_in(k + kDepth - 1);
+            if (ce == cudaSuccess && dmask) ce = cudaStreamWaitEvent(ks, pipe.mask_ready[db], 0);
+            if (ce == cudaSuccess && k >= kDepth) ce = cudaStreamWaitEvent(ks, pipe.out_free[db], 0);
+            if (ce != cudaSuccess) {
+                st = mgk_cuda_fail(c, ce, "kde_raster tile");
+                break;
+            }
+            if (two && k >= 1 &&
+                ops.wait((CUstream)ks, (CUdeviceptr)(uintptr_t)(d_flag + k - 1), 1u, CU_STREAM_WAIT_VALUE_GEQ) != CUDA_SUCCESS) {
+                st = mgk_fail(c, MGK_ERR_CUDA, "kde_raster: stream wait failed");
+                break;
+            }
+            bool merged_on_mrg = false;
+            if ((st = mgk_density_launch_split(c, band_plans[k], ks, pipe.mrg, pipe.dens[db], &merged_on_mrg))) break;
+            if (two && ops.write((CUstream)ks, (CUdeviceptr)(uintptr_t)(d_flag + k), 1u, CU_STREAM_WRITE_VALUE_DEFAULT) !=
+                           CUDA_SUCCESS) {
+                st = mgk_fail(c, MGK_ERR_CUDA, "kde_raster: stream write failed");
+                break;
+            }
+            ce = cudaEventRecord(pipe.done[db], merged_on_mrg ? pipe.mrg : ks);
+            if (ce == cudaSuccess) ce = out_copy(k);
+            if (ce != cudaSuccess) {
+                st = mgk_cuda_fail(c, ce, "kde_raster tile");
+                break;
+            }
+        }
+    }
+    if (st == MGK_OK && band_r0.empty() && ntiles > 0 && (st = count_of(0)) == MGK_OK) {
         if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster plan");
         else st = plan_of(0);
     }
     // the masks of the first kDepth - 1 tiles are on their way; tile k's loop
     // step sends the one of tile k + kDepth - 1 (its buffer's last reader is
     // tile k - 1's density)
-    for (int64_t k = 1; k < kDepth - 1 && st == MGK_OK; k++)
+    for (int64_t k = 1; k < kDepth - 1 && st == MGK_OK && band_r0.empty(); k++)
         if ((ce = mask_in(k)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
-    for (int64_t k = 0; st == MGK_OK && k < ntiles; k++) {
+    for (int64_t k = 0; st == MGK_OK && band_r0.empty() && k < ntiles; k++) {
         const int b = (int)(k & 1), db = (int)(k % kDepth);
         ce = mask_in(k + kDepth - 1);
         if (ce != cudaSuccess) {
@@ -1004,7 +1139,11 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     if ((ce = cudaStreamSynchronize(pipe.h2d)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
     if ((ce = cudaStreamSynchronize(pipe.d2h)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
     if ((ce = cudaStreamSynchronize(c->stream)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
+    if ((ce = cudaStreamSynchronize(pipe.alt)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
+    if ((ce = cudaStreamSynchronize(pipe.mrg)) != cudaSuccess && st == MGK_OK) st = mgk_cuda_fail(c, ce, "kde_raster");
     for (int i = 0; i < 2; i++) mgk_density_discard(c, plans[i]);  // every kernel has ended
+    for (mgk_dplan* D : band_plans) mgk_density_discard(c, D);
+    if (d_flag) mgk_free(c, d_flag, sizeof(unsigned) * ntiles);
     if (counted) cudaEventDestroy(counted);
     if (st == MGK_OK) {  // counters 4 (density evals) and 7 (staging-wait flag)
         ce = cudaMemcpy(c->h_counter + 4, c->d_counter + 4, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);

@@ -89,6 +89,7 @@ struct DParams {
     float gcut;  // 2^-(cutoff in log2 units): the in-cutoff threshold on E_j F'_i
     unsigned long long* evals;
     unsigned long long* err;
+    unsigned* tail_flag;  // set to 1 when the launch's last CTA starts (null: none)
 };
 
 // Bin range covering [lo, hi] (coordinates), clamped; returns false if empty.
@@ -860,6 +861,9 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 
 template <bool VARH, bool COUNT>
 __global__ void __launch_bounds__(kThreads, MGK_DENSITY_MIN_CTAS) k_density(DParams P) {
+    // the last CTA to start tells a stream waiting on the flag (the next
+    // band's launch) that this launch's tail has begun
+    if (P.tail_flag && blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) atomicExch(P.tail_flag, 1u);
     density_item<VARH, COUNT>(P, P.items[blockIdx.x]);
 }
 
@@ -1111,6 +1115,7 @@ struct mgk_dplan {
     void* d_tab = nullptr;
     const void* src_tab = nullptr;
     size_t b_tab = 0;
+    bool staged = false;  // d_tab already filled (mgk_density_stage) for the next launch
 };
 
 static void dplan_release(mgk_ctx* ctx, mgk_dplan* D) {
@@ -1166,9 +1171,29 @@ static int counts_launch(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, 
 // The plan of a tile from the counts in staging slot `slot` (its counting
 // kernel has finished); the work list, split tables and error flag go into
 // the same slot.
+static int plan_from_counts(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                            int64_t nr, int64_t nc, const int64_t* counts, const float* d_mask, float* d_out,
+                            unsigned long long* d_evals, bool fp64, int slot, mgk_dplan** out);
+
 static int plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
                         int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
                         bool fp64, int slot, mgk_dplan** out) {
+    *out = nullptr;
+    if (nr <= 0 || nc <= 0) return MGK_OK;
+    const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
+    char *h_st = nullptr, *d_st = nullptr;
+    const int st = mgk_host_stage_slot(ctx, slot, sizeof(int64_t) * nbx_t * nby_t, (void**)&h_st, (void**)&d_st);
+    if (st) return st;
+    // the counts are consumed (plan_tile) before the slot is written again
+    return plan_from_counts(ctx, idx, g, row0, col0, nr, nc, reinterpret_cast<const int64_t*>(h_st), d_mask, d_out,
+                            d_evals, fp64, slot, out);
+}
+
+// The plan of a tile from its per-block candidate counts (host memory); the
+// work list, split tables and error flag go into staging slot `slot`.
+static int plan_from_counts(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                            int64_t nr, int64_t nc, const int64_t* counts, const float* d_mask, float* d_out,
+                            unsigned long long* d_evals, bool fp64, int slot, mgk_dplan** out) {
     *out = nullptr;
     if (nr <= 0 || nc <= 0) return MGK_OK;
     mgk_dplan* D = new (std::nothrow) mgk_dplan();
@@ -1183,14 +1208,7 @@ static int plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, i
     const int nbx_t = (int)((nc + kBC - 1) / kBC), nby_t = (int)((nr + kBR - 1) / kBR);
     int st;
     TilePlan& T = D->T;
-    {
-        char *h_st = nullptr, *d_st = nullptr;
-        if ((st = mgk_host_stage_slot(ctx, slot, sizeof(int64_t) * nbx_t * nby_t, (void**)&h_st, (void**)&d_st))) {
-            delete D;
-            return st;
-        }
-        plan_tile(reinterpret_cast<const int64_t*>(h_st), nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
-    }
+    plan_tile(counts, nbx_t, nby_t, ctx->sm_count, ctx->split_waves, 0, T);
     sort_items(T.items);
     const int32_t nslots = T.nslots;
     D->b_scr = sizeof(double) * (size_t)kCells * (size_t)std::max(nslots, 1);
@@ -1255,12 +1273,33 @@ int mgk_density_plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid*
     return plan_counted(ctx, idx, g, row0, col0, nr, nc, d_mask, d_out, d_evals, false, slot, out);
 }
 
+int mgk_density_plan_from_counts(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                                 int64_t nr, int64_t nc, const int64_t* counts, const float* d_mask, float* d_out,
+                                 unsigned long long* d_evals, int slot, mgk_dplan** out) {
+    return plan_from_counts(ctx, idx, g, row0, col0, nr, nc, counts, d_mask, d_out, d_evals, false, slot, out);
+}
+
+const int64_t* mgk_density_counts_host(mgk_ctx* ctx, int slot) {
+    return static_cast<const int64_t*>(ctx->h_stage[slot]);
+}
+
+void mgk_density_set_tail_flag(mgk_dplan* D, unsigned* flag) {
+    if (D) D->P.tail_flag = flag;
+}
+
+int mgk_density_stage(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
+    if (!D) return MGK_OK;
+    const int st = stage_tables(ctx, D, s);
+    if (st == MGK_OK) D->staged = true;
+    return st;
+}
+
 int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
     if (!D) return MGK_OK;
     const DParams& P = D->P;
     const bool varh = D->idx->varh;
     const unsigned grid = (unsigned)D->T.items.size();
-    const int st = stage_tables(ctx, D, s);
+    const int st = D->staged ? MGK_OK : stage_tables(ctx, D, s);
     if (st) return st;
     if (D->count) {
         if (varh) launch_density<true, true>(grid, s, P);
@@ -1276,6 +1315,37 @@ int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {
     }
     const cudaError_t ce = cudaGetLastError();
     if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density");
+    return MGK_OK;
+}
+
+int mgk_density_launch_split(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s, cudaStream_t s_merge, cudaEvent_t ev,
+                             bool* merged_on_s_merge) {
+    *merged_on_s_merge = false;
+    if (!D) return MGK_OK;
+    if (!D->T.nslots || !s_merge) return mgk_density_launch_plan(ctx, D, s);
+    const DParams& P = D->P;
+    const bool varh = D->idx->varh;
+    const unsigned grid = (unsigned)D->T.items.size();
+    int st = D->staged ? MGK_OK : stage_tables(ctx, D, s);
+    if (st) return st;
+    if (D->count) {
+        if (varh) launch_density<true, true>(grid, s, P);
+        else launch_density<false, true>(grid, s, P);
+    } else {
+        if (varh) launch_density<true, false>(grid, s, P);
+        else launch_density<false, false>(grid, s, P);
+    }
+    MGK_COUNT_LAUNCH(ctx, 1);
+    cudaError_t ce = cudaGetLastError();
+    if (ce == cudaSuccess) ce = cudaEventRecord(ev, s);
+    if (ce == cudaSuccess) ce = cudaStreamWaitEvent(s_merge, ev, 0);
+    if (ce == cudaSuccess) {
+        k_merge<<<dim3((unsigned)D->T.split_blocks.size(), kMergeParts), 256, 0, s_merge>>>(P, D->d_sb, D->d_sbeg);
+        ce = cudaGetLastError();
+    }
+    if (ce != cudaSuccess) return mgk_cuda_fail(ctx, ce, "density");
+    MGK_COUNT_LAUNCH(ctx, 1);
+    *merged_on_s_merge = true;
     return MGK_OK;
 }
 

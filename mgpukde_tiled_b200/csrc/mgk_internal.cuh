@@ -261,6 +261,25 @@ int mgk_density_plan_counted(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid*
                              int64_t nr, int64_t nc, const float* d_mask, float* d_out, unsigned long long* d_evals,
                              int slot, mgk_dplan** out);
 int mgk_density_launch_plan(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s);
+// The plan of rows/columns of a tile from per-block candidate counts in host
+// memory (block-row major, ceil(nc / 128) per block row; e.g. a slice of one
+// count of a larger tile whose block rows it shares); tables into `slot`.
+int mgk_density_plan_from_counts(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0, int64_t col0,
+                                 int64_t nr, int64_t nc, const int64_t* counts, const float* d_mask, float* d_out,
+                                 unsigned long long* d_evals, int slot, mgk_dplan** out);
+// Host view of the counts mgk_density_counts_launch wrote into `slot`.
+const int64_t* mgk_density_counts_host(mgk_ctx* ctx, int slot);
+// Copies a plan's work list from its staging slot to device memory on `s`
+// now (mgk_density_launch_plan then skips that copy); the slot may be
+// rewritten once this copy has run.
+int mgk_density_stage(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s);
+// mgk_density_launch_plan with the merge of split blocks (if any) on
+// s_merge, after the density on s (event ev); *merged_on_s_merge tells where
+// the plan's last kernel went.
+int mgk_density_launch_split(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s, cudaStream_t s_merge, cudaEvent_t ev,
+                             bool* merged_on_s_merge);
+// The plan's density kernel sets *flag = 1 when its last CTA starts.
+void mgk_density_set_tail_flag(mgk_dplan* plan, unsigned* flag);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
 int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, mgk_raster* r, double cap);
