@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <new>
@@ -1029,8 +1030,11 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         // alternate over two streams and band k waits for band k - 1's last
         // CTA to start, so its CTAs fill the SMs that band k - 1's tail
         // frees; a stream write after each band ends that wait in any case.
+        // MGK_RASTER_ONE_STREAM=1 forces the one-stream schedule, the one
+        // taken without stream memory operations (same plans, same raster)
         const StreamMemOps& ops = stream_memops();
-        const bool two = stream_memops_work(c);
+        const char* one = std::getenv("MGK_RASTER_ONE_STREAM");
+        const bool two = !(one && one[0] == '1') && stream_memops_work(c);
         if (two && (st = mgk_alloc(c, (void**)&d_flag, sizeof(unsigned) * ntiles)) == MGK_OK &&
             (ce = cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * ntiles, c->stream)) != cudaSuccess)
             st = mgk_cuda_fail(c, ce, "kde_raster flags");

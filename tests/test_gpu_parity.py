@@ -148,6 +148,26 @@ def test_single_large_crop(ctx):
         assert gev == rev + eev
 
 
+def test_raster_band_schedules_agree(ctx, monkeypatch):
+    """The whole-raster path's full-width bands (a 1500^2 raster: six bands)
+    give bitwise the same raster whether the bands alternate over two
+    streams, each waiting for the previous band's last CTA to start, or run
+    on one stream (the schedule taken without stream memory operations),
+    with and without the pair count."""
+    c = synth.single_large(scale=0.15, seed=3)
+    dg = mk.Grid.of(c["density_grid"])
+    dmask = synth.rasterize_polygon(c["polygon"], c["density_grid"])
+    args = (ctx, c["x"], c["y"], c["w"], c["h"], dg, dmask, mk.Grid.of(c["edge_grid"]), c["edge_mask"])
+    for count in (False, True):
+        monkeypatch.delenv("MGK_RASTER_ONE_STREAM", raising=False)
+        two, _, ev2 = mk.kde_raster(*args, count=count)
+        monkeypatch.setenv("MGK_RASTER_ONE_STREAM", "1")
+        one, _, ev1 = mk.kde_raster(*args, count=count)
+        assert np.array_equal(two.view(np.uint32), one.view(np.uint32))
+        assert ev1 == ev2
+    monkeypatch.delenv("MGK_RASTER_ONE_STREAM", raising=False)
+
+
 def test_boundary_distance_exact_large(ctx):
     """Binned candidate-list search vs the oracle's brute force, bit for bit,
     on a 1000 x 1000 polygon mask with points inside, near the boundary and
