@@ -56,6 +56,13 @@ struct LevelDesc {
 #ifndef MGK_LOO_PREFILTER
 #define MGK_LOO_PREFILTER 1
 #endif
+// candidates per trip of the scan loop: 8 measured fastest on the
+// 64-bandwidth selection (C2: 317, 290, 282, 271, 274 and 290 ms at 1, 2, 4,
+// 8, 16 and 32; the compiler's own choice gave 290)
+#ifndef MGK_LOO_UNROLL
+#define MGK_LOO_UNROLL 8
+#endif
+constexpr int kLooUnroll = MGK_LOO_UNROLL;
 
 struct LooParams {
     const LevelDesc* lev;  // [nlev], device
@@ -269,6 +276,7 @@ __global__ void __launch_bounds__(kLooQ) k_loo_multi(LooParams P) {
             if (qv) {
                 float part = 0.0f;
                 const MgkPt* st = stage[buf];
+#pragma unroll kLooUnroll
                 for (int t = 0; t < m; t++) {
                     const float4 cp = *reinterpret_cast<const float4*>(&st[t]);
 #if MGK_LOO_PREFILTER
