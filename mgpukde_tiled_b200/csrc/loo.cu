@@ -15,8 +15,9 @@
 // counter.  The points are indexed once per bandwidth octave (row-major bins
 // of side in (0.375 h, 0.75 h] for the h that use the level), so the
 // candidates of a group are one contiguous range per bin row; they arrive in
-// batches of 32 through a double-buffered TMA bulk copy into shared memory
-// and every thread (one query) scans them.  The cutoff is decided in FP32
+// batches of up to 128 (one bin row's range at a time) through a
+// double-buffered TMA bulk copy into shared memory, and every thread (one
+// query) scans them.  The cutoff is decided in FP32
 // with a band around 9h^2 re-decided by the oracle's exact FP64 test, so the
 // summed pair set is exactly the oracle's; terms are FP32 (an exp2 by range
 // reduction and a polynomial, free of the systematic bias an approximate
@@ -37,7 +38,11 @@
 namespace {
 
 constexpr int kLooQ = 128;    // queries (threads) per work item
-constexpr int kLooB = 32;     // candidates per staged batch
+// candidates per staged batch (at most one per thread, which reads its
+// candidate's weight): with the scan unrolled by 8, 32, 64 and 128 gave
+// 271, 257 and 251 ms for the 64-bandwidth selection (C2)
+constexpr int kLooB = 128;
+static_assert(kLooB <= kLooQ, "one thread per staged candidate");
 constexpr int kMaxLev = 16;   // bandwidth octaves
 constexpr long long kLooSpin = 1ll << 24;
 
