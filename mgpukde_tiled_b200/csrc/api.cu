@@ -664,8 +664,8 @@ int mgk_loo_loglik_batch(mgk_ctx* c, mgk_points* p, const mgk_raster* r, const f
     if (r && !cap_covers(p, hi))
         return mgk_fail(c, MGK_ERR_INVALID, "loo: the boundary distances are exact only within " +
                                                 std::to_string(p->dist2_cap) + ", less than 3 h_max");
-    mgk_loo_batch* B = nullptr;
-    if ((st = mgk_loo_batch_create(c, p, r, lo, hi, nh, &B))) return st;
+    mgk_loo_batch* B = nullptr;  // runs once: no graph
+    if ((st = mgk_loo_batch_create_share(c, p, r, lo, hi, nh, 0, 1, nullptr, 0, &B, false))) return st;
     st = mgk_loo_batch_run(B, h_grid, logl, argmax, nullptr, nullptr);
     mgk_loo_batch_destroy(B);
     return st;
@@ -713,7 +713,7 @@ int mgk_loo_share_loglik(mgk_ctx* c, mgk_points* p, const float* h_grid, int nh,
     if (st) return st;
     mgk_loo_batch* B = nullptr;
     if ((st = mgk_loo_batch_create_share(c, p, nullptr, lo, hi, nh, part, nparts, d_ew_all,
-                                         share_chunk(p->n, nparts), &B)))
+                                         share_chunk(p->n, nparts), &B, false)))  // runs once: no graph
         return st;
     st = mgk_loo_batch_run(B, h_grid, partial_logL, nullptr, nullptr, evals);
     mgk_loo_batch_destroy(B);

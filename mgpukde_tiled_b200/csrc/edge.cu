@@ -17,8 +17,8 @@
 // (an estimate from sqrt(9h^2 - dy^2), verified, with a binary search when the
 // estimate misses), so the summed cell set and the eval count are exactly the
 // reference's.  Work per (point, h) is O(window width + window height) rather
-// than O(width x height); factors and sums are FP64, so the weight is the
-// FP64 value to a few ulps before its rounding to float.
+// than O(width x height); the sums are FP64, the factors FP64 (per-point h)
+// or FP32 to about 1e-7 (fixed h, edge_factor).
 //
 // One warp per point: the lanes build the prefix table of a chunk of up to
 // 1024 window columns in shared memory (a contiguous segment per lane and a
@@ -88,6 +88,22 @@ __device__ __forceinline__ int64_t clamp_index(double v, int64_t lo, int64_t hi)
 
 __device__ __forceinline__ double cell_xd(const mgk_grid& g, int64_t c) { return (double)mgk_cell_x(g.xll, g.cs, c); }
 
+// exp(-d2 / 2h^2) for d2 within the cutoff (exponent <= 4.5).  Fixed h:
+// 2^-(d2 k2) with the exponent in FP64, split into a float pair, 2^-hi by
+// the unbiased FP32 polynomial and a first-order correction for the low part
+// (relative error about 1e-7; the weights then meet the 1e-6 density and
+// likelihood tolerances).  Per-point h (the adaptive search, whose
+// Hooke-Jeeves steps compare nearby likelihoods): the FP64 exp.
+template <bool VARH>
+__device__ __forceinline__ double edge_factor(double d2, double h2, double k2) {
+    if (VARH) return exp(d2 / (-2.0 * h2));
+    const double a = d2 * k2;
+    const float ah = (float)a;
+    const float al = (float)(a - (double)ah);
+    const float e = mgk_exp2_neg_poly(ah);
+    return (double)__fmaf_rn(__fmul_rn(-al, MGK_LN2F), e, e);
+}
+
 // The oracle's FP64 cutoff decision for column c of a row at dy^2.
 __device__ __forceinline__ bool in_cut(const mgk_grid& g, int64_t c, double px, double dy2, double cut) {
     const double dx = __dsub_rn(cell_xd(g, c), px);
@@ -153,7 +169,7 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
             ru = ru > g.nrows - 1 ? g.nrows - 1 : ru;
             cl = cl < 0 ? 0 : cl;
             cu = cu > g.ncols - 1 ? g.ncols - 1 : cu;
-            const double m2h2 = -2.0 * h2;
+            const double k2 = MGK_LOG2E / (2.0 * h2);
             double acc = 0.0;
             unsigned long long cnt = 0;
             for (int64_t c0 = cl; c0 <= cu && rl <= ru; c0 += kEdgeChunk) {
@@ -165,7 +181,7 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
                 double run = 0.0;
                 for (int j = j0; j < j1; j++) {
                     const double dx = __dsub_rn(cell_xd(g, c0 + j), px);
-                    run += exp(__dmul_rn(dx, dx) / m2h2);
+                    run += edge_factor<VARH>(__dmul_rn(dx, dx), h2, k2);
                     Q[j + 1] = run;
                 }
                 double off = run;
@@ -224,7 +240,7 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
                         S += Q[rb - c0 + 1] - Q[ra - c0];
                         cnt += (unsigned long long)(rb - ra + 1);
                     }
-                    if (S != 0.0) acc += exp(dy2 / m2h2) * S;
+                    if (S != 0.0) acc += edge_factor<VARH>(dy2, h2, k2) * S;
                 }
                 __syncwarp();
             }

@@ -440,7 +440,7 @@ void mgk_loo_batch_destroy(mgk_loo_batch* B) {
 // bandwidth octave, buffers, and the captured graph.
 int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi, int nh,
                          mgk_loo_batch** out) {
-    return mgk_loo_batch_create_share(c, p, r, h_lo, h_hi, nh, 0, 1, nullptr, 0, out);
+    return mgk_loo_batch_create_share(c, p, r, h_lo, h_hi, nh, 0, 1, nullptr, 0, out, true);
 }
 
 // Share `part` of `nparts` of a batch: the query groups
@@ -449,7 +449,7 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
 // and h in chunks of ew_chunk points, each nh rows of ew_chunk floats.
 int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi,
                                int nh, int part, int nparts, const float* ew_ext, int64_t ew_chunk,
-                               mgk_loo_batch** out) {
+                               mgk_loo_batch** out, bool replay) {
     mgk_loo_batch* B = new (std::nothrow) mgk_loo_batch();
     if (!B) return mgk_fail(c, MGK_ERR_INVALID, "loo batch: out of host memory");
     B->ctx = c;
@@ -544,9 +544,10 @@ int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster
     P.evals = B->d_evals + 1;
     P.err = B->d_err;
     // capture the sequence into a graph on a private stream (the graph is
-    // then launched into the context's stream); if capture fails the batch
-    // launches its kernels directly
-    if (cudaStreamSynchronize(c->stream) == cudaSuccess &&
+    // then launched into the context's stream); if capture fails, or the
+    // batch runs once (replay false: capture and instantiation would cost
+    // more than they save), the batch launches its kernels directly
+    if (replay && cudaStreamSynchronize(c->stream) == cudaSuccess &&
         cudaStreamCreateWithFlags(&B->cap, cudaStreamNonBlocking) == cudaSuccess &&
         cudaStreamBeginCapture(B->cap, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
         cudaStream_t keep = c->stream;

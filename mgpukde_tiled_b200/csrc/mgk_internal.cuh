@@ -304,7 +304,7 @@ int mgk_loo_batch_create(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, f
                          mgk_loo_batch** out);
 int mgk_loo_batch_create_share(mgk_ctx* c, const mgk_points* p, const mgk_raster* r, float h_lo, float h_hi,
                                int nh, int part, int nparts, const float* ew_ext, int64_t ew_chunk,
-                               mgk_loo_batch** out);
+                               mgk_loo_batch** out, bool replay = true);
 int mgk_loo_batch_run(mgk_loo_batch* B, const float* hs, double* logl, int* best, int64_t* edge_evals,
                       int64_t* loo_evals);
 void mgk_loo_batch_destroy(mgk_loo_batch* B);
