@@ -142,6 +142,7 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     const mgk_grid g = E.g;
     const double xll = g.xll, yll = g.yll, cs = g.cs;
+    const double inv_cs = 1.0 / cs;  // for the interval estimates, which the exact test then verifies
     const double cell_area = (double)(g.cs * g.cs);  // float product, kde_cuda_kdtr_tiled.cu:2698
     const int nh = VARH ? 1 : E.nh;
     unsigned long long cnt_total = 0;
@@ -207,13 +208,13 @@ __global__ void __launch_bounds__(kEdgeWarps * 32) k_edge_rows(EdgeParams E) {
                     const double dy2 = __dmul_rn(dy, dy);
                     if (dy2 >= cut || !in_cut(g, cm, px, dy2, cut)) continue;
                     const double t = sqrt(cut - dy2);
-                    int64_t lo = clamp_index(ceil((px - t - xll) / cs - 0.5), c0, cm);
+                    int64_t lo = clamp_index(ceil((px - t - xll) * inv_cs - 0.5), c0, cm);
                     if (in_cut(g, lo, px, dy2, cut)) {
                         if (lo > c0 && in_cut(g, lo - 1, px, dy2, cut)) lo = first_in(g, c0, lo - 1, px, dy2, cut);
                     } else {
                         lo = first_in(g, lo + 1, cm, px, dy2, cut);
                     }
-                    int64_t hi = clamp_index(floor((px + t - xll) / cs - 0.5), cm, c1);
+                    int64_t hi = clamp_index(floor((px + t - xll) * inv_cs - 0.5), cm, c1);
                     if (in_cut(g, hi, px, dy2, cut)) {
                         if (hi < c1 && in_cut(g, hi + 1, px, dy2, cut)) hi = last_in(g, hi + 1, c1, px, dy2, cut);
                     } else {
