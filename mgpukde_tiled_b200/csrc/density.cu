@@ -8,7 +8,7 @@
 //   den(c) = sum_p [d^2 < 9 h_p^2] exp(-d^2 / 2 h_p^2) / (h_p^2 TWO_PI) w_p e_p
 //
 // Layout: a CTA (256 threads) owns a 64 x 128 block of cells; warp w owns a
-// 16 x 64 sub-block, lane l a 4 x 8 micro-tile.  A block whose cells are all
+// 32 x 32 sub-block, lane l a 4 x 8 micro-tile.  A block whose cells are all
 // NoData stages no candidates and writes NoData (the reference skips NoData
 // cells, kde_kernel_kdtr.cu:426-428).  Candidates (points of the bins within
 // 3h of the block, one contiguous range per bin row) arrive in mini-batches
@@ -403,9 +403,22 @@ constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab;
 #define MGK_DENSITY_SPLITLOOP 1
 #endif
 
+// Warp sub-blocks: 32 x 32 cells (lanes of 4 rows and 8 contiguous columns;
+// a disc's edge crosses fewer square sub-blocks, 9.57 against 9.71 ms on
+// the full raster), or with MGK_DENSITY_SQUARE=0 16 x 64 (lanes of 4 rows and
+// two groups of 4 columns 32 apart).
+#ifndef MGK_DENSITY_SQUARE
+#define MGK_DENSITY_SQUARE 1
+#endif
+constexpr int kWR = MGK_DENSITY_SQUARE ? 32 : 16;  // rows of a warp's sub-block
+constexpr int kWC = MGK_DENSITY_SQUARE ? 32 : 64;  // columns of a warp's sub-block
+constexpr int kNWC = kBC / kWC;                    // warps across the block
+constexpr int kLC = MGK_DENSITY_SQUARE ? 4 : 8;    // lanes across a sub-block
+constexpr int kE2 = MGK_DENSITY_SQUARE ? 4 : 32;   // offset of a lane's second group of 4 columns
+
 // Block column of cell j (0..7) of lane column tc in warp column wc.
 __device__ __forceinline__ int lane_col(int wc, int tc, int j) {
-    return wc * 64 + (j < 4 ? tc * 4 + j : 32 + tc * 4 + (j - 4));
+    return MGK_DENSITY_SQUARE ? wc * 32 + tc * 8 + j : wc * 64 + (j < 4 ? tc * 4 + j : 32 + tc * 4 + (j - 4));
 }
 
 // The thread's FP32 partial sums into its Kahan-compensated accumulators in
@@ -450,10 +463,11 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 
     const BlockGeom G = block_geom(P, it.bx, it.by);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int wr = warp >> 1, wc = warp & 1;  // warp sub-block: rows wr*16.., cols wc*64..
-    // lane micro-tile: rows tr*4.. (4); columns tc*4.. and 32+tc*4.. (2 x 4) of
-    // the warp's 64, so the 8 lanes of a row read 128 contiguous bytes of E
-    const int tr = lane >> 3, tc = lane & 7;
+    const int wr = warp / kNWC, wc = warp % kNWC;  // warp sub-block: rows wr*kWR.., cols wc*kWC..
+    // lane micro-tile: rows tr*4.. (4) and the 8 columns lane_col(wc, tc, 0..7)
+    // (contiguous in 32 x 32 sub-blocks: the 4 lanes of a row read 128
+    // contiguous bytes of E; in 16 x 64 ones two groups of 4, 32 apart)
+    const int tr = lane / kLC, tc = lane % kLC;
 
     // cell centres of the block: global floats and their quantum split
     bool regular = true;
@@ -499,7 +513,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 8; j++) {
-            const int r = wr * 16 + tr * 4 + i, c = lane_col(wc, tc, j);
+            const int r = wr * kWR + tr * 4 + i, c = lane_col(wc, tc, j);
             bool v = r < G.nrow && c < G.ncol;
             if (v && P.mask) v = P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata;
             valid |= (unsigned)v << (i * 8 + j);
@@ -518,10 +532,10 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     // phase A roles: point q = tid / 8, part k = tid % 8: columns k, k+8, ...,
     // k+120, rows k, k+8, ..., k+56, and the skip test of warp k
     const int qa = tid >> 3, ka = tid & 7;
-    const int sk_wr = ka >> 1, sk_wc = ka & 1;
-    const bool sk_on = (sk_wr * 16 < G.nrow) && (sk_wc * 64 < G.ncol);
-    const int sk_c0 = sk_wc * 64, sk_c1 = min(sk_wc * 64 + 63, G.ncol - 1);
-    const int sk_r0 = sk_wr * 16, sk_r1 = min(sk_wr * 16 + 15, G.nrow - 1);
+    const int sk_wr = ka / kNWC, sk_wc = ka % kNWC;
+    const bool sk_on = (sk_wr * kWR < G.nrow) && (sk_wc * kWC < G.ncol);
+    const int sk_c0 = sk_wc * kWC, sk_c1 = min(sk_wc * kWC + kWC - 1, G.ncol - 1);
+    const int sk_r0 = sk_wr * kWR, sk_r1 = min(sk_wr * kWR + kWR - 1, G.nrow - 1);
 
     if (tid == 0) {
         for (int c = 0; c < kNCur; c++) cur_init(P, G, it, c, s_cur[c]);
@@ -581,7 +595,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             }
             const unsigned bal = __ballot_sync(0xffffffffu, proc);
             const unsigned balf = __ballot_sync(0xffffffffu, full);
-            // the sub-blocks that sum point pq: bit k is sub-block (k >> 1, k & 1).
+            // the sub-blocks that sum point pq: bit k is sub-block (k / kNWC, k % kNWC).
             // Only their column halves and rows of the tables are built; the
             // other entries are never read (the warps that would read them skip
             // the point)
@@ -592,18 +606,13 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 float* cE = colE + pq * kFStrideC;
                 float* rF = rowF + pq * kFStride;
                 float* rG = rowG + pq * kFStride;
-                if (pb & 0x55u) {  // columns 0-63, read by the warps of column half 0
+                // columns in groups of kWC: group u is read by the warps of warp column u
 #pragma unroll
-                    for (int c = 0; c < 8; c++) {
-                        const int j = ka + 8 * c;
-                        float ah, al, d2;
-                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                        cE[j] = exp2_pair(ah, al);
-                    }
-                }
-                if (pb & 0xaau) {  // columns 64-127
+                for (int u = 0; u < kNWC; u++) {
+                    const unsigned colmask = (kNWC == 2 ? 0x55u : 0x11u) << u;
+                    if (!(pb & colmask)) continue;
 #pragma unroll
-                    for (int c = 8; c < 16; c++) {
+                    for (int c = u * (kWC / 8); c < (u + 1) * (kWC / 8); c++) {
                         const int j = ka + 8 * c;
                         float ah, al, d2;
                         exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
@@ -613,13 +622,15 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
 #pragma unroll
                 for (int c = 0; c < 8; c++) {
-                    if (!((pb >> (2 * (c >> 1))) & 3u)) continue;  // row ka + 8c lies in warp row c / 2
+                    // row ka + 8c lies in warp row c / (kWR / 8)
+                    if (!((pb >> (kNWC * (c / (kWR / 8)))) & ((1u << kNWC) - 1u))) continue;
                     const int i = ka + 8 * c;
                     float bh, bl, d2;
                     exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
                     const float fb = exp2_pair(bh, bl);
                     rF[i] = __fmul_rn(r.wk, fb);
-                    if (!((pbp >> (2 * (c >> 1))) & 3u)) continue;  // no partial sub-block reads the row's G
+                    // no partial sub-block reads the row's G
+                    if (!((pbp >> (kNWC * (c / (kWR / 8)))) & ((1u << kNWC) - 1u))) continue;
                     // a_j < cutl - b_i  <=>  E_j > G_i = 2^-cutl / 2^-b_i (2^-x is decreasing);
                     // G = inf for rows off the disc (2^-b_i flushed to zero)
                     rG[i] = __fmul_rn(P.gcut, rcp_approx(fb));
@@ -689,7 +700,14 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                 const bool lv = pl < m;
                 const bool pm = lv && ((procmask[pl] >> warp) & 1u);
                 const bool fm = lv && ((fullmask[pl] >> warp) & 1u);
+#if MGK_DENSITY_SQUARE
+                // the 32 rows of the warp in its column half (wc / 2), point pl
+                const unsigned myflag =
+                    lv ? reinterpret_cast<const unsigned*>(&rowflag[0][0])[pl * 4 + (wc >> 1) * 2 + wr] : 0u;
+                (void)rf16;
+#else
                 const unsigned myflag = lv ? (unsigned)rf16[pl * 8 + wc * 4 + wr] : 0u;  // 16 rows, point pl
+#endif
                 unsigned todo = __ballot_sync(0xffffffffu, pm);
                 const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
                 const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
@@ -710,10 +728,10 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     while (todo) {
                         const int q = __ffs(todo) - 1, qq = q + 32 * hq;
                         todo &= todo - 1u;
-                        const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
-                        const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
+                        const float* pE = colE + qq * kFStrideC + lane_col(wc, tc, 0);
+                        const float* pF = rowF + qq * kFStride + wr * kWR + tr * 4;
                         const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                        const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE + kE2);
                         const float4 f4 = *reinterpret_cast<const float4*>(pF);
                         const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                         const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
@@ -730,10 +748,10 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     while (todo) {
                         const int q = __ffs(todo) - 1, qq = q + 32 * hq;
                         todo &= todo - 1u;
-                        const float* pE = colE + qq * kFStrideC + wc * 64 + tc * 4;
-                        const float* pF = rowF + qq * kFStride + wr * 16 + tr * 4;
+                        const float* pE = colE + qq * kFStrideC + lane_col(wc, tc, 0);
+                        const float* pF = rowF + qq * kFStride + wr * kWR + tr * 4;
                         const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                        const float4 e4b = *reinterpret_cast<const float4*>(pE + 32);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE + kE2);
                         const float4 f4 = *reinterpret_cast<const float4*>(pF);
                         const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                         const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
@@ -744,7 +762,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
                                 for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
                         } else {
-                            const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * 16 + tr * 4);
+                            const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * kWR + tr * 4);
                             const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
                             unsigned inm = 0;
                             if (COUNT) {
@@ -775,7 +793,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
                                         for (int j = 0; j < 8; j++) {
                                             const bool ex = mgk_d2_exact(px, py, s_cxg[lane_col(wc, tc, j)],
-                                                                         s_cyg[wr * 16 + tr * 4 + i]) < cut;
+                                                                         s_cyg[wr * kWR + tr * 4 + i]) < cut;
                                             const bool fi = rg[i] < ce[j];
                                             if (ex != fi) {
                                                 const float t = __fmul_rn(ce[j], rv[i]);
@@ -836,7 +854,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
         for (int u = 0; u < 8; u++) {
             const int k = q8 * 8 + u, i = k >> 3, j = k & 7;
-            const int r = wr * 16 + tr * 4 + i, c = lane_col(wc, tc, j);
+            const int r = wr * kWR + tr * 4 + i, c = lane_col(wc, tc, j);
             if (r >= G.nrow || c >= G.ncol) continue;
             const double v = ((double)ss[u] - (double)cc[u]) * norm;
             if (it.slot >= 0) {
