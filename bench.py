@@ -429,7 +429,7 @@ def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_b
         out["traffic_note"] = ("dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch, from the ncu "
                                "capture summarised in profiles/k_density_traffic.txt (not measured in this run)")
     # the pipe utilisation behind frac (frac counts 8 flop-equivalents per in-cutoff pair, not issued ops)
-    out["pipes_ncu"] = {"fma_pct": 31.9, "alu_pct": 34.4, "xu_pct": 17.2, "lsu_pct": 17.0, "issue_active_pct": 61.2,
+    out["pipes_ncu"] = {"fma_pct": 30.9, "alu_pct": 31.9, "xu_pct": 17.4, "lsu_pct": 16.6, "issue_active_pct": 59.0,
                         "source": "ncu --set full of one half-scale launch, profiles/k_density_single_large_half.md "
                                   "(not measured in this run)"}
     if hbm_gbs:
