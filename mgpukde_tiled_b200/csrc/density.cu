@@ -172,6 +172,16 @@ __device__ __forceinline__ void kahan_add(float& s, float& c, float v) {
     s = t;
 }
 
+// kahan_add on two cells at once, in packed FP32 (add/sub.rn.f32x2): each
+// half is bitwise the scalar form.
+__device__ __forceinline__ void kahan_add2(float& s0, float& s1, float& c0, float& c1, float v0, float v1) {
+    asm("{\n .reg .b64 s, c, v, y, t;\n mov.b64 s, {%0, %1};\n mov.b64 c, {%2, %3};\n mov.b64 v, {%4, %5};\n"
+        " sub.rn.f32x2 y, v, c;\n add.rn.f32x2 t, s, y;\n sub.rn.f32x2 c, t, s;\n sub.rn.f32x2 c, c, y;\n"
+        " mov.b64 {%0, %1}, t;\n mov.b64 {%2, %3}, c;\n}\n"
+        : "+f"(s0), "+f"(s1), "+f"(c0), "+f"(c1)
+        : "f"(v0), "f"(v1));
+}
+
 // ---- TMA bulk copy + mbarrier (sm_90+ PTX) ---------------------------------
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
@@ -281,6 +291,15 @@ __device__ __forceinline__ float rsqrt_approx(float x) {
     return y;
 }
 
+// (a0, a1) += (e0, e1) * f as one packed FP32 FMA (fma.rn.f32x2): each half
+// is the correctly rounded a + e * f, bitwise the scalar __fmaf_rn.
+__device__ __forceinline__ void fma2_bcast(float& a0, float& a1, float e0, float e1, float f) {
+    asm("{\n .reg .b64 a, e, f;\n mov.b64 a, {%0, %1};\n mov.b64 e, {%2, %3};\n mov.b64 f, {%4, %4};\n"
+        " fma.rn.f32x2 a, e, f, a;\n mov.b64 {%0, %1}, a;\n}\n"
+        : "+f"(a0), "+f"(a1)
+        : "f"(e0), "f"(e1), "f"(f));
+}
+
 // acc += e * f when a < t: one compare and one predicated FFMA.
 __device__ __forceinline__ void fma_if_less(float& acc, float a, float t, float e, float f) {
     asm("{\n .reg .pred p;\n setp.lt.f32 p, %1, %2;\n @p fma.rn.f32 %0, %3, %4, %0;\n}\n"
@@ -378,19 +397,27 @@ __device__ __forceinline__ int fill_batch(const DParams& P, const BlockGeom& G, 
 }
 
 // Dynamic shared memory of k_density (bytes): the staged points and the
-// factor tables (row strides of 136 and 72 floats, both 8 mod 32, so that the
-// phase-A stores of 4 points hit distinct banks).  The per-cell Kahan
+// factor tables, 128 column and 64 row entries per point.  A warp stores 32
+// consecutive entries of one point at a time, so the tables need no padding
+// against bank conflicts, and three CTAs fit on an SM.  The per-cell Kahan
 // accumulators are in tensor memory.
-constexpr int kFStrideC = 136;  // column table, floats per point
-constexpr int kFStride = 72;    // row tables, floats per point
+constexpr int kFStrideC = 128;  // column table, floats per point
+constexpr int kFStride = 64;    // row tables, floats per point
 constexpr size_t kSmemStage = 2 * kMB * sizeof(MgkPt);
 constexpr size_t kSmemColTab = (size_t)kMB * kFStrideC * sizeof(float);
 constexpr size_t kSmemRowTab = (size_t)kMB * kFStride * sizeof(float);
 constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab;
 
+// Resident CTAs per SM: three (24 warps) need at most 80 registers per
+// thread and about 72 KB of shared memory per CTA; with two (128 registers)
+// the C1 kernel took 9.58 ms against 8.72 ms.
 #ifndef MGK_DENSITY_MIN_CTAS
-#define MGK_DENSITY_MIN_CTAS 2  // resident CTAs per SM (shared memory allows two)
+#define MGK_DENSITY_MIN_CTAS 3
 #endif
+
+// Table entry of column j (row i) of batch point q.
+__device__ __forceinline__ int col_slot(int q, int j) { return q * kFStrideC + j; }
+__device__ __forceinline__ int row_slot(int q, int i) { return q * kFStride + i; }
 // Phase A builds the cutoff thresholds and ambiguity flags of a row only when
 // a sub-block that sums the point is partial in that row's warp row (fully
 // inside sub-blocks read neither).
@@ -403,23 +430,19 @@ constexpr size_t kDensitySmem = kSmemStage + kSmemColTab + 2 * kSmemRowTab;
 #define MGK_DENSITY_SPLITLOOP 1
 #endif
 
-// Warp sub-blocks: 32 x 32 cells (lanes of 4 rows and 8 contiguous columns;
-// a disc's edge crosses fewer square sub-blocks, 9.57 against 9.71 ms on
-// the full raster), or with MGK_DENSITY_SQUARE=0 16 x 64 (lanes of 4 rows and
-// two groups of 4 columns 32 apart).
-#ifndef MGK_DENSITY_SQUARE
-#define MGK_DENSITY_SQUARE 1
-#endif
-constexpr int kWR = MGK_DENSITY_SQUARE ? 32 : 16;  // rows of a warp's sub-block
-constexpr int kWC = MGK_DENSITY_SQUARE ? 32 : 64;  // columns of a warp's sub-block
-constexpr int kNWC = kBC / kWC;                    // warps across the block
-constexpr int kLC = MGK_DENSITY_SQUARE ? 4 : 8;    // lanes across a sub-block
-constexpr int kE2 = MGK_DENSITY_SQUARE ? 4 : 32;   // offset of a lane's second group of 4 columns
+// Warp sub-blocks: 32 x 32 cells, 2 warp rows x 4 warp columns; lanes own
+// 4 rows and 8 contiguous columns (the 4 lanes of a row read 128 contiguous
+// bytes of a column table).  A disc's edge crosses fewer square sub-blocks
+// than 16 x 64 ones (9.57 against 9.71 ms on the C1 raster).
+constexpr int kWR = 32;           // rows of a warp's sub-block
+constexpr int kWC = 32;           // columns of a warp's sub-block
+constexpr int kNWC = kBC / kWC;   // warps across the block (4)
+constexpr int kLC = 4;            // lanes across a sub-block
+constexpr int kE2 = 4;            // offset of a lane's second group of 4 columns
+static_assert(kBR == 2 * kWR && kNWC == 4 && kThreads == 256, "phase A assumes 2 x 4 warps of 32 x 32 cells");
 
 // Block column of cell j (0..7) of lane column tc in warp column wc.
-__device__ __forceinline__ int lane_col(int wc, int tc, int j) {
-    return MGK_DENSITY_SQUARE ? wc * 32 + tc * 8 + j : wc * 64 + (j < 4 ? tc * 4 + j : 32 + tc * 4 + (j - 4));
-}
+__device__ __forceinline__ int lane_col(int wc, int tc, int j) { return wc * 32 + tc * 8 + j; }
 
 // The thread's FP32 partial sums into its Kahan-compensated accumulators in
 // tensor memory (sum at tS, compensation at tC), then zeroed.
@@ -433,9 +456,10 @@ __device__ __forceinline__ void flush_partials(unsigned tS, unsigned tC, float (
         tmem_ld8(tC + 8u * c, cv);
         tmem_wait_ld(sv, cv);
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            kahan_add(sv[u], cv[u], part[c * 8 + u]);
+        for (int u = 0; u < 8; u += 2) {
+            kahan_add2(sv[u], sv[u + 1], cv[u], cv[u + 1], part[c * 8 + u], part[c * 8 + u + 1]);
             part[c * 8 + u] = 0.0f;
+            part[c * 8 + u + 1] = 0.0f;
         }
         tmem_st8(tS + 8u * c, sv);
         tmem_st8(tC + 8u * c, cv);
@@ -529,8 +553,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     unsigned long long cnt = 0;
     unsigned pc = 0;  // points processed by this warp (warp-uniform)
 
-    // phase A roles: point q = tid / 8, part k = tid % 8: columns k, k+8, ...,
-    // k+120, rows k, k+8, ..., k+56, and the skip test of warp k
+    // phase-A skip tests: thread tid tests point qa = tid / 8 (and qa + 32)
+    // against sub-block ka = tid % 8
     const int qa = tid >> 3, ka = tid & 7;
     const int sk_wr = ka / kNWC, sk_wc = ka % kNWC;
     const bool sk_on = (sk_wr * kWR < G.nrow) && (sk_wc * kWC < G.ncol);
@@ -560,27 +584,20 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         const MgkPt* st = stage + buf * kMB;
 
         // ---------------- phase A ----------------
-        // thread (qa, ka) builds part ka of the tables of points qa, qa + 32
+        // Warp w takes points 4w..4w+3 and 32+4w..32+4w+3.  For each group of
+        // four, lane (k, ka) = (lane / 8, lane % 8) tests point k against
+        // sub-block ka; then the warp builds the tables of the four points one
+        // at a time, every lane one column of each summed 32-column group and
+        // one row of each summed warp row (the warp takes one point's
+        // branches, and its stores fill 32 consecutive entries).
 #pragma unroll 1
         for (int hq = 0; hq < kMB / 32; hq++) {
             const int pq = qa + 32 * hq;
             const bool act = ok && pq < m;
             bool proc = false, full = false;
-            unsigned lo32 = 0, hi32 = 0, lo32h = 0, hi32h = 0;
-            const MgkPt r = st[act ? pq : 0];
-            float k2h, k2l, cutf, epsd2;
-            if (VARH) {
-                k2h = r.k2h;
-                k2l = r.k2l;
-                cutf = 9.0f * r.hh;
-                epsd2 = r.hh * (4.0f * kAmbEps / (float)MGK_LOG2E);
-            } else {
-                k2h = P.k2h;
-                k2l = P.k2l;
-                cutf = P.cutf;
-                epsd2 = P.epsd2;
-            }
             if (act && sk_on) {
+                const MgkPt r = st[pq];
+                const float cutf = VARH ? 9.0f * r.hh : P.cutf;
                 // distance from the point to the sub-block rectangle of cell centres
                 const float dxl = __fadd_rn(__fsub_rn(s_cxh[sk_c0], r.xh), __fsub_rn(s_cxl[sk_c0], r.xl));
                 const float dxr = __fadd_rn(__fsub_rn(r.xh, s_cxh[sk_c1]), __fsub_rn(r.xl, s_cxl[sk_c1]));
@@ -595,75 +612,72 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
             }
             const unsigned bal = __ballot_sync(0xffffffffu, proc);
             const unsigned balf = __ballot_sync(0xffffffffu, full);
-            // the sub-blocks that sum point pq: bit k is sub-block (k / kNWC, k % kNWC).
-            // Only their column halves and rows of the tables are built; the
-            // other entries are never read (the warps that would read them skip
-            // the point)
-            const unsigned pb = (bal >> (8 * (qa & 3))) & 0xffu;
-            // sub-blocks that sum point pq with the cutoff test (all of them in the counting variant)
-            const unsigned pbp = (MGK_DENSITY_ROWSKIP && !COUNT) ? pb & ~((balf >> (8 * (qa & 3))) & 0xffu) : pb;
-            if (pb) {
-                float* cE = colE + pq * kFStrideC;
-                float* rF = rowF + pq * kFStride;
-                float* rG = rowG + pq * kFStride;
-                // columns in groups of kWC: group u is read by the warps of warp column u
-#pragma unroll
-                for (int u = 0; u < kNWC; u++) {
-                    const unsigned colmask = (kNWC == 2 ? 0x55u : 0x11u) << u;
-                    if (!(pb & colmask)) continue;
-#pragma unroll
-                    for (int c = u * (kWC / 8); c < (u + 1) * (kWC / 8); c++) {
-                        const int j = ka + 8 * c;
-                        float ah, al, d2;
-                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                        cE[j] = exp2_pair(ah, al);
-                    }
-                }
-                const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
-#pragma unroll
-                for (int c = 0; c < 8; c++) {
-                    // row ka + 8c lies in warp row c / (kWR / 8)
-                    if (!((pb >> (kNWC * (c / (kWR / 8)))) & ((1u << kNWC) - 1u))) continue;
-                    const int i = ka + 8 * c;
-                    float bh, bl, d2;
-                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
-                    const float fb = exp2_pair(bh, bl);
-                    rF[i] = __fmul_rn(r.wk, fb);
-                    // no partial sub-block reads the row's G
-                    if (!((pbp >> (kNWC * (c / (kWR / 8)))) & ((1u << kNWC) - 1u))) continue;
-                    // a_j < cutl - b_i  <=>  E_j > G_i = 2^-cutl / 2^-b_i (2^-x is decreasing);
-                    // G = inf for rows off the disc (2^-b_i flushed to zero)
-                    rG[i] = __fmul_rn(P.gcut, rcp_approx(fb));
-                    const float s2 = cutf - d2;
-                    const unsigned a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2 ? 3u : 0u);
-                    const unsigned sh = (ka + 8 * c) & 31;
-                    if (c < 4) {
-                        lo32 |= (a & 1u) << sh;
-                        lo32h |= (a >> 1) << sh;
-                    } else {
-                        hi32 |= (a & 1u) << sh;
-                        hi32h |= (a >> 1) << sh;
-                    }
-                }
-            }
-            // the row flags of point pq come from its 8 threads (same warp)
-#pragma unroll
-            for (int o = 1; o < 8; o <<= 1) {
-                lo32 |= __shfl_xor_sync(0xffffffffu, lo32, o);
-                hi32 |= __shfl_xor_sync(0xffffffffu, hi32, o);
-                lo32h |= __shfl_xor_sync(0xffffffffu, lo32h, o);
-                hi32h |= __shfl_xor_sync(0xffffffffu, hi32h, o);
-            }
             if (lane < 8) {
                 // this warp's points (4) that sub-block warp `lane` sums
                 const int nl = __popc(bal & (0x01010101u << lane));
                 if (nl) atomicAdd(&s_load[buf][lane], nl);
             }
             if (ka == 0) {
-                rowflag[pq][0] = ((unsigned long long)hi32 << 32) | lo32;
-                rowflag[pq][1] = ((unsigned long long)hi32h << 32) | lo32h;
                 procmask[pq] = (unsigned char)((bal >> (8 * (qa & 3))) & 0xffu);
                 fullmask[pq] = (unsigned char)((balf >> (8 * (qa & 3))) & 0xffu);
+            }
+#pragma unroll 1
+            for (int k = 0; k < 4; k++) {
+                // the sub-blocks that sum point pk: bit b is sub-block (b / 4, b % 4).
+                // Only their column groups and warp rows of the tables are
+                // built; the other entries are never read (the warps that
+                // would read them skip the point)
+                const unsigned pb = (bal >> (8 * k)) & 0xffu;
+                if (!pb) continue;
+                // sub-blocks that sum the point with the cutoff test (all of them in the counting variant)
+                const unsigned pbp = (MGK_DENSITY_ROWSKIP && !COUNT) ? pb & ~((balf >> (8 * k)) & 0xffu) : pb;
+                const int pk = 4 * warp + k + 32 * hq;
+                const MgkPt r = st[pk];
+                float k2h, k2l, cutf, epsd2;
+                if (VARH) {
+                    k2h = r.k2h;
+                    k2l = r.k2l;
+                    cutf = 9.0f * r.hh;
+                    epsd2 = r.hh * (4.0f * kAmbEps / (float)MGK_LOG2E);
+                } else {
+                    k2h = P.k2h;
+                    k2l = P.k2l;
+                    cutf = P.cutf;
+                    epsd2 = P.epsd2;
+                }
+#pragma unroll
+                for (int u = 0; u < kNWC; u++) {
+                    if (!((pb >> u) & 0x11u)) continue;
+                    const int j = lane + 32 * u;
+                    float ah, al, d2;
+                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
+                    colE[col_slot(pk, j)] = exp2_pair(ah, al);
+                }
+                const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
+                unsigned flw[2][2] = {{0u, 0u}, {0u, 0u}};  // [column half][warp row]: row bits
+#pragma unroll
+                for (int v = 0; v < 2; v++) {
+                    const bool row_on = (pb >> (4 * v)) & 0xfu;  // warp-uniform
+                    if (!row_on) continue;
+                    const int i = lane + 32 * v;
+                    float bh, bl, d2;
+                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
+                    const float fb = exp2_pair(bh, bl);
+                    rowF[row_slot(pk, i)] = __fmul_rn(r.wk, fb);
+                    // no partial sub-block reads the row's G
+                    if (!((pbp >> (4 * v)) & 0xfu)) continue;
+                    // a_j < cutl - b_i  <=>  E_j > G_i = 2^-cutl / 2^-b_i (2^-x is decreasing);
+                    // G = inf for rows off the disc (2^-b_i flushed to zero)
+                    rowG[row_slot(pk, i)] = __fmul_rn(P.gcut, rcp_approx(fb));
+                    const float s2 = cutf - d2;
+                    const unsigned a = regular ? amb_row(s2, epsd2, pc0, inv_cs) : (s2 >= -epsd2 ? 3u : 0u);
+                    flw[0][v] = __ballot_sync(0xffffffffu, a & 1u);
+                    flw[1][v] = __ballot_sync(0xffffffffu, a >> 1);
+                }
+                if (lane == 0) {
+                    rowflag[pk][0] = ((unsigned long long)flw[0][1] << 32) | flw[0][0];
+                    rowflag[pk][1] = ((unsigned long long)flw[1][1] << 32) | flw[1][0];
+                }
             }
         }
         if (__syncthreads_or(!ok)) {
@@ -695,19 +709,13 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll 1
             for (int hq = 0; hq < kMB / 32; hq++) {
                 // this warp's processed, fully-inside and flagged points of the batch as bit masks
-                const unsigned short* rf16 = reinterpret_cast<const unsigned short*>(&rowflag[0][0]);
                 const int pl = lane + 32 * hq;  // this lane's point of the half
                 const bool lv = pl < m;
                 const bool pm = lv && ((procmask[pl] >> warp) & 1u);
                 const bool fm = lv && ((fullmask[pl] >> warp) & 1u);
-#if MGK_DENSITY_SQUARE
                 // the 32 rows of the warp in its column half (wc / 2), point pl
                 const unsigned myflag =
                     lv ? reinterpret_cast<const unsigned*>(&rowflag[0][0])[pl * 4 + (wc >> 1) * 2 + wr] : 0u;
-                (void)rf16;
-#else
-                const unsigned myflag = lv ? (unsigned)rf16[pl * 8 + wc * 4 + wr] : 0u;  // 16 rows, point pl
-#endif
                 unsigned todo = __ballot_sync(0xffffffffu, pm);
                 const unsigned fullb = __ballot_sync(0xffffffffu, pm && fm);
                 const unsigned ambb = __ballot_sync(0xffffffffu, pm && myflag != 0u);
@@ -728,17 +736,19 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     while (todo) {
                         const int q = __ffs(todo) - 1, qq = q + 32 * hq;
                         todo &= todo - 1u;
-                        const float* pE = colE + qq * kFStrideC + lane_col(wc, tc, 0);
-                        const float* pF = rowF + qq * kFStride + wr * kWR + tr * 4;
+                        const float* pE = colE + col_slot(qq, lane_col(wc, tc, 0));
+                        const float* pE2 = pE + kE2;
+                        const float* pF = rowF + row_slot(qq, wr * kWR + tr * 4);
                         const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                        const float4 e4b = *reinterpret_cast<const float4*>(pE + kE2);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE2);
                         const float4 f4 = *reinterpret_cast<const float4*>(pF);
                         const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                         const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
 #pragma unroll
                         for (int i = 0; i < 4; i++)
 #pragma unroll
-                            for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
+                            for (int j = 0; j < 8; j += 2)
+                                fma2_bcast(part[i * 8 + j], part[i * 8 + j + 1], ce[j], ce[j + 1], rv[i]);
                     }
                     todo = rest;
                     rest = 0u;
@@ -748,10 +758,11 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     while (todo) {
                         const int q = __ffs(todo) - 1, qq = q + 32 * hq;
                         todo &= todo - 1u;
-                        const float* pE = colE + qq * kFStrideC + lane_col(wc, tc, 0);
-                        const float* pF = rowF + qq * kFStride + wr * kWR + tr * 4;
+                        const float* pE = colE + col_slot(qq, lane_col(wc, tc, 0));
+                        const float* pE2 = pE + kE2;
+                        const float* pF = rowF + row_slot(qq, wr * kWR + tr * 4);
                         const float4 e4a = *reinterpret_cast<const float4*>(pE);
-                        const float4 e4b = *reinterpret_cast<const float4*>(pE + kE2);
+                        const float4 e4b = *reinterpret_cast<const float4*>(pE2);
                         const float4 f4 = *reinterpret_cast<const float4*>(pF);
                         const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                         const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
@@ -762,7 +773,7 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
 #pragma unroll
                                 for (int j = 0; j < 8; j++) part[i * 8 + j] = __fmaf_rn(ce[j], rv[i], part[i * 8 + j]);
                         } else {
-                            const float4 g4 = *reinterpret_cast<const float4*>(rowG + qq * kFStride + wr * kWR + tr * 4);
+                            const float4 g4 = *reinterpret_cast<const float4*>(rowG + row_slot(qq, wr * kWR + tr * 4));
                             const float rg[4] = {g4.x, g4.y, g4.z, g4.w};
                             unsigned inm = 0;
                             if (COUNT) {
@@ -1021,6 +1032,9 @@ __global__ void k_merge_jobs(const DParams* __restrict__ jobs, const int4* __res
 template <bool VARH, bool COUNT>
 void launch_density(unsigned grid, cudaStream_t s, const DParams& P) {
     cudaFuncSetAttribute(k_density<VARH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kDensitySmem);
+    // the largest shared-memory carveout: three CTAs of about 75 KB per SM
+    cudaFuncSetAttribute(k_density<VARH, COUNT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     k_density<VARH, COUNT><<<grid, kThreads, kDensitySmem, s>>>(P);
 }
 
@@ -1028,6 +1042,8 @@ template <bool VARH, bool COUNT>
 void launch_density_jobs(unsigned grid, cudaStream_t s, const DParams* jobs, const Item* items) {
     cudaFuncSetAttribute(k_density_jobs<VARH, COUNT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)kDensitySmem);
+    cudaFuncSetAttribute(k_density_jobs<VARH, COUNT>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                         cudaSharedmemCarveoutMaxShared);
     k_density_jobs<VARH, COUNT><<<grid, kThreads, kDensitySmem, s>>>(jobs, items);
 }
 
