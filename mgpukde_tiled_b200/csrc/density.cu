@@ -274,6 +274,32 @@ __device__ __forceinline__ void exponent_pair(float t, float lo, float k2h, floa
     al = __fmaf_rn(pe, k2h, __fmaf_rn(p, k2l, ae));
 }
 
+// exponent_pair and exp2_pair of two entries at once, in packed FP32
+// (f32x2).  The negations are arranged so that every half is bitwise the
+// scalar form: fma(-a, b, c) = -fma(a, b, -c) under round-to-nearest, so pen
+// = -pe and ahn = -ah exactly.  Returns the two factors 2^-(a_0), 2^-(a_1)
+// and the approximate squares d2.
+__device__ __forceinline__ void exp2_pair2(float t0, float t1, float lo0, float lo1, float k2h, float k2l,
+                                           float& e0, float& e1, float& d20, float& d21) {
+    float ahn0, ahn1, al0, al1;
+    asm("{\n .reg .b64 t, lo, dh, tmp, de, p, dhn, err, dh2n, pen, kh, khn, kl, ahn, ae, x, al, d2;\n"
+        " mov.b64 t, {%6, %7};\n mov.b64 lo, {%8, %9};\n"
+        " mov.b64 kh, {%10, %10};\n mov.b64 kl, {%11, %11};\n mov.b64 khn, {%12, %12};\n"
+        " add.rn.f32x2 dh, t, lo;\n sub.rn.f32x2 tmp, dh, t;\n sub.rn.f32x2 de, lo, tmp;\n"
+        " mul.rn.f32x2 p, dh, dh;\n mov.b64 dhn, 0xBF800000BF800000;\n mul.rn.f32x2 dhn, dh, dhn;\n"
+        " fma.rn.f32x2 err, dhn, dh, p;\n add.rn.f32x2 dh2n, dhn, dhn;\n fma.rn.f32x2 pen, dh2n, de, err;\n"
+        " sub.rn.f32x2 d2, p, pen;\n mul.rn.f32x2 ahn, p, khn;\n fma.rn.f32x2 ae, p, kh, ahn;\n"
+        " fma.rn.f32x2 x, p, kl, ae;\n fma.rn.f32x2 al, pen, khn, x;\n"
+        " mov.b64 {%0, %1}, ahn;\n mov.b64 {%2, %3}, al;\n mov.b64 {%4, %5}, d2;\n}\n"
+        : "=f"(ahn0), "=f"(ahn1), "=f"(al0), "=f"(al1), "=f"(d20), "=f"(d21)
+        : "f"(t0), "f"(t1), "f"(lo0), "f"(lo1), "f"(k2h), "f"(k2l), "f"(-k2h));
+    const float x0 = mgk_ex2(ahn0), x1 = mgk_ex2(ahn1);
+    asm("{\n .reg .b64 al, c, x, e;\n mov.b64 al, {%2, %3};\n mov.b64 c, {%6, %6};\n mov.b64 x, {%4, %5};\n"
+        " mul.rn.f32x2 al, al, c;\n fma.rn.f32x2 e, al, x, x;\n mov.b64 {%0, %1}, e;\n}\n"
+        : "=f"(e0), "=f"(e1)
+        : "f"(al0), "f"(al1), "f"(x0), "f"(x1), "f"(-MGK_LN2F));
+}
+
 __device__ __forceinline__ float exp2_pair(float ah, float al) {
     const float e = mgk_ex2(-ah);
     return __fmaf_rn(__fmul_rn(-al, MGK_LN2F), e, e);
@@ -330,12 +356,14 @@ __device__ __forceinline__ unsigned amb_row(float s2, float eps_d2, float pc0, f
 
 // A mini-batch takes its points from kNCur cursors over equal consecutive
 // parts of the item's candidate range (round robin, up to kMB / kNCur from
-// each, then whatever is left), so that the points of one batch come from
-// bin rows spread over the candidate window.  Points from one bin row all
-// touch the same warp rows of the block; mixing rows keeps the eight warps'
-// phase-B work per batch even and shortens the waits at the batch barriers.
+// each, then whatever is left).  With several cursors the points of one batch
+// come from bin rows spread over the candidate window, which evens the eight
+// warps' phase-B work per batch; with one, neighbouring points share their
+// branches in phase A.  Since three CTAs share an SM (the others issue while
+// one waits at a batch barrier) one cursor is the faster: 8.01 ms on the C1
+// raster against 8.34 ms with two and 8.42 ms with eight.
 #ifndef MGK_DENSITY_NCUR
-#define MGK_DENSITY_NCUR 2
+#define MGK_DENSITY_NCUR 1
 #endif
 constexpr int kNCur = MGK_DENSITY_NCUR;
 struct BatchCur {
@@ -645,24 +673,47 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     cutf = P.cutf;
                     epsd2 = P.epsd2;
                 }
+                // column groups in pairs (0, 1) and (2, 3): two entries in packed FP32
+                const unsigned ub = (pb | (pb >> 4)) & 0xfu;
 #pragma unroll
-                for (int u = 0; u < kNWC; u++) {
-                    if (!((pb >> u) & 0x11u)) continue;
-                    const int j = lane + 32 * u;
-                    float ah, al, d2;
-                    exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                    colE[col_slot(pk, j)] = exp2_pair(ah, al);
+                for (int h2 = 0; h2 < 2; h2++) {
+                    const unsigned two = (ub >> (2 * h2)) & 3u;
+                    if (!two) continue;
+                    const int j0 = lane + 64 * h2, j1 = j0 + 32;
+                    if (two == 3u) {
+                        float e0, e1, d20, d21;
+                        exp2_pair2(__fsub_rn(r.xh, s_cxh[j0]), __fsub_rn(r.xh, s_cxh[j1]), __fsub_rn(r.xl, s_cxl[j0]),
+                                   __fsub_rn(r.xl, s_cxl[j1]), k2h, k2l, e0, e1, d20, d21);
+                        colE[col_slot(pk, j0)] = e0;
+                        colE[col_slot(pk, j1)] = e1;
+                    } else {
+                        const int j = two == 1u ? j0 : j1;
+                        float ah, al, d2;
+                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
+                        colE[col_slot(pk, j)] = exp2_pair(ah, al);
+                    }
                 }
                 const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
                 unsigned flw[2][2] = {{0u, 0u}, {0u, 0u}};  // [column half][warp row]: row bits
+                // row factors of both warp rows (packed when both are summed)
+                float fbv[2], d2v[2];
+                if ((pb & 0xfu) && (pb >> 4)) {
+                    exp2_pair2(__fsub_rn(r.yh, s_cyh[lane]), __fsub_rn(r.yh, s_cyh[lane + 32]),
+                               __fsub_rn(r.yl, s_cyl[lane]), __fsub_rn(r.yl, s_cyl[lane + 32]), k2h, k2l, fbv[0],
+                               fbv[1], d2v[0], d2v[1]);
+                } else {
+                    const int i = (pb & 0xfu) ? lane : lane + 32;
+                    float bh, bl, d2;
+                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
+                    fbv[0] = fbv[1] = exp2_pair(bh, bl);
+                    d2v[0] = d2v[1] = d2;
+                }
 #pragma unroll
                 for (int v = 0; v < 2; v++) {
                     const bool row_on = (pb >> (4 * v)) & 0xfu;  // warp-uniform
                     if (!row_on) continue;
                     const int i = lane + 32 * v;
-                    float bh, bl, d2;
-                    exponent_pair(__fsub_rn(r.yh, s_cyh[i]), __fsub_rn(r.yl, s_cyl[i]), k2h, k2l, bh, bl, d2);
-                    const float fb = exp2_pair(bh, bl);
+                    const float fb = fbv[v], d2 = d2v[v];
                     rowF[row_slot(pk, i)] = __fmul_rn(r.wk, fb);
                     // no partial sub-block reads the row's G
                     if (!((pbp >> (4 * v)) & 0xfu)) continue;
