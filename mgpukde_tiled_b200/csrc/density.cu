@@ -559,17 +559,34 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
     }
     const float inv_cs = 1.0f / (float)P.cs;
 
-    // validity of the lane's 32 cells (inside the tile and not NoData); bit i*8+j
+    // validity of the lane's 32 cells (inside the tile and not NoData); bit
+    // i*8+j.  Mask rows (and output rows, in the epilogue) go 8 cells, two
+    // 16-byte vectors, at a time where the raster rows keep 16-byte alignment.
     unsigned valid = 0;
+    {
+    const bool vec = (P.nc & 3) == 0 && (reinterpret_cast<uintptr_t>(P.mask) & 15u) == 0;
+    const int lc0 = lane_col(wc, tc, 0);
 #pragma unroll
-    for (int i = 0; i < 4; i++)
+    for (int i = 0; i < 4; i++) {
+        const int r = wr * kWR + tr * 4 + i;
+        if (r >= G.nrow) continue;
+        const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + lc0 - P.col0);
+        if (P.mask && vec && lc0 + 8 <= G.ncol) {
+            const float4 a = __ldg(reinterpret_cast<const float4*>(P.mask + o));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(P.mask + o + 4));
+            const float m8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
 #pragma unroll
-        for (int j = 0; j < 8; j++) {
-            const int r = wr * kWR + tr * 4 + i, c = lane_col(wc, tc, j);
-            bool v = r < G.nrow && c < G.ncol;
-            if (v && P.mask) v = P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata;
-            valid |= (unsigned)v << (i * 8 + j);
+            for (int j = 0; j < 8; j++) valid |= (unsigned)(m8[j] != P.nodata) << (i * 8 + j);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 8; j++) {
+                bool v = lc0 + j < G.ncol;
+                if (v && P.mask) v = P.mask[o + j] != P.nodata;
+                valid |= (unsigned)v << (i * 8 + j);
+            }
         }
+    }
+    }
     // A block whose cells are all NoData gathers no candidates: its output
     // is NoData throughout (the reference skips NoData cells before any sum,
     // kde_kernel_kdtr.cu:426-428).
@@ -913,17 +930,28 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         tmem_wait_ld(ss, cc);
 #pragma unroll
         for (int u = 0; u < 8; u++) kahan_add(ss[u], cc[u], part[q8 * 8 + u]);
+        // row q8 of the lane's micro-tile: cells k = q8 * 8 + u, columns ec0 + u
+        const int r = wr * kWR + tr * 4 + q8, ec0 = lane_col(wc, tc, 0);
+        if (r >= G.nrow) continue;
+        if (it.slot >= 0) {
+            double* d = P.scratch + (size_t)it.slot * kCells + r * kBC + ec0;
 #pragma unroll
-        for (int u = 0; u < 8; u++) {
-            const int k = q8 * 8 + u, i = k >> 3, j = k & 7;
-            const int r = wr * kWR + tr * 4 + i, c = lane_col(wc, tc, j);
-            if (r >= G.nrow || c >= G.ncol) continue;
-            const double v = ((double)ss[u] - (double)cc[u]) * norm;
-            if (it.slot >= 0) {
-                P.scratch[(size_t)it.slot * kCells + r * kBC + c] = v;
+            for (int u = 0; u < 8; u++)
+                if (ec0 + u < G.ncol) d[u] = ((double)ss[u] - (double)cc[u]) * norm;
+        } else {
+            float* d = P.out + (G.r0 + r - P.row0) * P.nc + (G.c0 + ec0 - P.col0);
+            float f[8];
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+                f[u] = ((valid >> (q8 * 8 + u)) & 1u) ? (float)(((double)ss[u] - (double)cc[u]) * norm) : P.nodata;
+            const bool vec = (P.nc & 3) == 0 && (reinterpret_cast<uintptr_t>(P.out) & 15u) == 0;
+            if (vec && ec0 + 8 <= G.ncol) {
+                *reinterpret_cast<float4*>(d) = make_float4(f[0], f[1], f[2], f[3]);
+                *reinterpret_cast<float4*>(d + 4) = make_float4(f[4], f[5], f[6], f[7]);
             } else {
-                const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0);
-                P.out[o] = ((valid >> k) & 1u) ? (float)v : P.nodata;
+#pragma unroll
+                for (int u = 0; u < 8; u++)
+                    if (ec0 + u < G.ncol) d[u] = f[u];
             }
         }
     }

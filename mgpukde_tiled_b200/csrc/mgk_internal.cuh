@@ -1,5 +1,6 @@
 // Internal declarations shared by the CUDA translation units of libmgk.
 #pragma once
+#include <cstring>
 
 #include <cuda_runtime.h>
 
@@ -215,9 +216,17 @@ __device__ __forceinline__ double mgk_d2_exact(float x0, float y0, float x1, flo
 
 // Splits a float coordinate on the quantum 2^-qexp: hi = nearest multiple,
 // lo = remainder, both exact floats (|v| < 2^(22 - qexp) assumed).
+// 2^k for a double exponent in the normal range (|k| < 1000), from its bits.
+__device__ __host__ __forceinline__ double mgk_pow2(int k) {
+    const unsigned long long b = (unsigned long long)(1023 + k) << 52;
+    double d;
+    memcpy(&d, &b, sizeof d);
+    return d;
+}
 __device__ __host__ __forceinline__ void mgk_qsplit(float v, int qexp, float& hi, float& lo) {
-    const double s = ldexp(1.0, qexp);
-    hi = (float)(rint((double)v * s) / s);
+    // scaling by powers of two is exact, so multiplying by 2^-qexp is the
+    // division by 2^qexp
+    hi = (float)(rint((double)v * mgk_pow2(qexp)) * mgk_pow2(-qexp));
     lo = (float)((double)v - (double)hi);
 }
 
