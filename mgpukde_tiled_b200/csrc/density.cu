@@ -834,7 +834,8 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                         const float4 f4 = *reinterpret_cast<const float4*>(pF);
                         const float ce[8] = {e4a.x, e4a.y, e4a.z, e4a.w, e4b.x, e4b.y, e4b.z, e4b.w};
                         const float rv[4] = {f4.x, f4.y, f4.z, f4.w};
-                        if (!COUNT && ((fullb >> q) & 1u)) {
+                        // (with the split loops no fully-inside point is left here)
+                        if (!COUNT && !MGK_DENSITY_SPLITLOOP && ((fullb >> q) & 1u)) {
                             // the whole sub-block is inside the cutoff: one FFMA per cell
 #pragma unroll
                             for (int i = 0; i < 4; i++)
