@@ -3,14 +3,19 @@
 // main(), kde_cuda_kdtr_tiled.cu:877-1521, for one GPU).
 #include <cudaTypedefs.h>
 
+#include <immintrin.h>
+
 #include <algorithm>
+#include <atomic>
 #include <cfloat>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
+#include <memory>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "mgk_internal.cuh"
@@ -863,6 +868,100 @@ struct RasterPipe {
 // hold those rows only).  A strict row range keeps, on the device, only the
 // points within 3 h_max of its rows (the densities of its cells need no
 // others), and out_ew must then be NULL.
+// ---- bit-packed density masks --------------------------------------------
+// The whole-raster path sends its NoData mask to the device as 1 bit per cell
+// (1 = valid) instead of 32: with the density coming back over the same link,
+// the float mask's upload set the pace of the bands (about 36 GB/s each way).
+// Worker threads pack the bands in order, ahead of their uploads.
+
+// One mask row: bit c % 8 of byte c / 8 is (src[c] != nodata), as the float
+// kernels compare (so a NaN NoData value marks every cell valid); the row's
+// padding bytes up to `bytes` are zero.
+__attribute__((target("avx2"))) static void pack_mask_row_avx2(const float* src, int64_t n, float nodata,
+                                                              unsigned char* dst, int64_t bytes) {
+    const __m256 nd = _mm256_set1_ps(nodata);
+    int64_t c = 0;
+    for (; c + 8 <= n; c += 8)
+        dst[c >> 3] = (unsigned char)_mm256_movemask_ps(_mm256_cmp_ps(_mm256_loadu_ps(src + c), nd, _CMP_NEQ_UQ));
+    int64_t b = c >> 3;
+    if (c < n) {
+        unsigned v = 0;
+        for (int64_t k = c; k < n; k++) v |= (unsigned)(src[k] != nodata) << (k - c);
+        dst[b++] = (unsigned char)v;
+    }
+    for (; b < bytes; b++) dst[b] = 0;
+}
+
+static void pack_mask_row(const float* src, int64_t n, float nodata, unsigned char* dst, int64_t bytes) {
+    int64_t b = 0;
+    for (int64_t c = 0; c < n; c += 8, b++) {
+        unsigned v = 0;
+        for (int64_t k = c; k < std::min<int64_t>(n, c + 8); k++) v |= (unsigned)(src[k] != nodata) << (k - c);
+        dst[b] = (unsigned char)v;
+    }
+    for (; b < bytes; b++) dst[b] = 0;
+}
+
+class MaskPacker {
+  public:
+    // rows [band_r0[k] - row_lo, band_r0[k + 1] - row_lo) of src form band k
+    MaskPacker(const float* src, int64_t ncols, float nodata, unsigned char* dst, int64_t stride,
+               const std::vector<int64_t>& band_r0, int64_t row_lo)
+        : src_(src), ncols_(ncols), nodata_(nodata), dst_(dst), stride_(stride),
+          avx2_(__builtin_cpu_supports("avx2")) {
+        const int64_t nb = (int64_t)band_r0.size() - 1;
+        band_rows_.resize(nb);
+        done_ = std::vector<std::atomic<int64_t>>(nb);
+        for (int64_t k = 0; k < nb; k++) {
+            band_rows_[k] = band_r0[k + 1] - band_r0[k];
+            done_[k].store(0);
+            for (int64_t r = band_r0[k]; r < band_r0[k + 1]; r += kChunk)
+                chunks_.push_back({k, r - row_lo, std::min<int64_t>(band_r0[k + 1], r + kChunk) - r});
+        }
+        const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+        const int nt = (int)std::min<unsigned>(8, std::max(1u, hw / 2));
+        for (int t = 0; t < nt; t++) threads_.emplace_back([this] { work(); });
+    }
+    ~MaskPacker() {
+        stop_.store(true);
+        for (std::thread& t : threads_) t.join();
+    }
+    // returns once band k is packed
+    void wait_band(int64_t k) {
+        while (done_[k].load(std::memory_order_acquire) < band_rows_[k]) std::this_thread::yield();
+    }
+
+  private:
+    struct Chunk {
+        int64_t band, row, rows;
+    };
+    static constexpr int64_t kChunk = 64;
+    void work() {
+        for (;;) {
+            const int64_t i = next_.fetch_add(1);
+            if (i >= (int64_t)chunks_.size() || stop_.load()) return;
+            const Chunk& ch = chunks_[i];
+            for (int64_t r = ch.row; r < ch.row + ch.rows; r++) {
+                if (avx2_) pack_mask_row_avx2(src_ + r * ncols_, ncols_, nodata_, dst_ + r * stride_, stride_);
+                else pack_mask_row(src_ + r * ncols_, ncols_, nodata_, dst_ + r * stride_, stride_);
+            }
+            done_[ch.band].fetch_add(ch.rows, std::memory_order_release);
+        }
+    }
+    const float* src_;
+    int64_t ncols_;
+    float nodata_;
+    unsigned char* dst_;
+    int64_t stride_;
+    bool avx2_;
+    std::vector<Chunk> chunks_;
+    std::vector<int64_t> band_rows_;
+    std::vector<std::atomic<int64_t>> done_;
+    std::atomic<int64_t> next_{0};
+    std::atomic<bool> stop_{false};
+    std::vector<std::thread> threads_;
+};
+
 static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y, const float* w, const float* h_pp,
                            float h, int edge_correction, const mgk_grid* eg, const float* emask, const mgk_grid* dg,
                            int64_t row_lo, int64_t row_hi, const float* dmask, int64_t tile_side,
@@ -895,6 +994,11 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     const int64_t ntc = (dg->ncols + tc - 1) / tc;
     const int64_t ntiles = band_r0.empty() ? (nrows + tr - 1) / tr * ntc : (int64_t)band_r0.size() - 1;
     const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
+    // full-width bands take the mask as bits (rows of mstride bytes, a
+    // multiple of 16); explicit tiles take it as floats
+    const bool packed = dmask && !band_r0.empty();
+    const int64_t mstride = (dg->ncols + 127) / 128 * 16;
+    const size_t tbm = packed ? (size_t)tr * (size_t)mstride : tb;
     RasterPipe pipe;
     cudaError_t ce = pipe.init();
     if (ce != cudaSuccess) return mgk_cuda_fail(c, ce, "kde_raster streams");
@@ -908,7 +1012,17 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     int st = MGK_OK;
     for (int i = 0; i < (int)std::min<int64_t>(ntiles, kDepth) && st == MGK_OK; i++) {
         st = mgk_alloc(c, (void**)&d_out[i], tb);
-        if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask[i], tb);
+        if (st == MGK_OK && dmask) st = mgk_alloc(c, (void**)&d_mask[i], tbm);
+    }
+    // the packed mask of all rows, in page-locked memory (staging slot 3),
+    // filled band by band by the packer's threads while the GPU works
+    unsigned char* h_bits = nullptr;
+    std::unique_ptr<MaskPacker> packer;
+    if (st == MGK_OK && packed) {
+        void* dev_alias = nullptr;
+        st = mgk_host_stage_slot(c, 3, (size_t)nrows * (size_t)mstride, (void**)&h_bits, &dev_alias);
+        if (st == MGK_OK)
+            packer.reset(new MaskPacker(dmask, dg->ncols, dg->nodata, h_bits, mstride, band_r0, row_lo));
     }
     auto tile_of = [&](int64_t k, int64_t& r0, int64_t& c0, int64_t& nr, int64_t& nc) {
         if (!band_r0.empty()) {
@@ -930,9 +1044,14 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         tile_of(k, r0, c0, nr, nc);
         const int b = (int)(k % kDepth);
         cudaError_t e = k >= kDepth ? cudaStreamWaitEvent(pipe.h2d, pipe.done[b], 0) : cudaSuccess;
-        if (e == cudaSuccess)
+        if (e == cudaSuccess && packed) {
+            packer->wait_band(k);
+            e = cudaMemcpyAsync(d_mask[b], h_bits + (r0 - row_lo) * mstride, (size_t)nr * (size_t)mstride,
+                                cudaMemcpyHostToDevice, pipe.h2d);
+        } else if (e == cudaSuccess) {
             e = cudaMemcpy2DAsync(d_mask[b], sizeof(float) * nc, dmask + (r0 - row_lo) * dg->ncols + c0,
                                   sizeof(float) * dg->ncols, sizeof(float) * nc, nr, cudaMemcpyHostToDevice, pipe.h2d);
+        }
         if (e == cudaSuccess) e = cudaEventRecord(pipe.mask_ready[b], pipe.h2d);
         return e;
     };
@@ -1064,8 +1183,11 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
                 break;
             }
             if ((st = mgk_density_plan_from_counts(c, idx, dg, r0, 0, nr, dg->ncols, counts + (r0 - row_lo) / 64 * nbx,
-                                                   d_mask[db], d_out[db], d_ev, 1 + (int)(k & 1), &band_plans[k])))
+                                                   packed ? nullptr : d_mask[db], d_out[db], d_ev, 1 + (int)(k & 1),
+                                                   &band_plans[k])))
                 break;
+            if (packed)
+                mgk_density_set_mask_bits(band_plans[k], reinterpret_cast<const unsigned char*>(d_mask[db]), mstride);
             if (two) mgk_density_set_tail_flag(band_plans[k], d_flag + k);
             ce = mask_in(k + kDepth - 1);
             if (ce == cudaSuccess && dmask) ce = cudaStreamWaitEvent(ks, pipe.mask_ready[db], 0);
@@ -1157,7 +1279,7 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     }
     for (int i = 0; i < kDepth; i++) {
         if (d_out[i]) mgk_free(c, d_out[i], tb);
-        if (d_mask[i]) mgk_free(c, d_mask[i], tb);
+        if (d_mask[i]) mgk_free(c, d_mask[i], tbm);
     }
     mgk_index_destroy(idx);
     mgk_raster_destroy(em);

@@ -74,6 +74,11 @@ struct DParams {
     int64_t row0, col0, nr, nc;
     float nodata;
     const float* mask;
+    // the same NoData mask as bits (1 = valid; row r of the tile at byte
+    // r * mbstride, column c at bit c % 8 of byte c / 8), used instead of
+    // `mask` when set
+    const unsigned char* mbits;
+    int64_t mbstride;
     float* out;
     double* scratch;  // [slot][kCells]
     const Item* items;
@@ -91,6 +96,12 @@ struct DParams {
     unsigned long long* err;
     unsigned* tail_flag;  // set to 1 when the launch's last CTA starts (null: none)
 };
+
+// Is cell (rr, cc) of the tile (tile-relative) valid: inside the mask and not NoData?
+__device__ __forceinline__ bool cell_valid(const DParams& P, int64_t rr, int64_t cc) {
+    if (P.mbits) return (P.mbits[rr * P.mbstride + (cc >> 3)] >> (cc & 7)) & 1u;
+    return !P.mask || P.mask[rr * P.nc + cc] != P.nodata;
+}
 
 // Bin range covering [lo, hi] (coordinates), clamped; returns false if empty.
 __device__ __forceinline__ bool bin_range(double lo, double hi, double o, double inv_side, int64_t nb,
@@ -571,7 +582,13 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
         const int r = wr * kWR + tr * 4 + i;
         if (r >= G.nrow) continue;
         const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + lc0 - P.col0);
-        if (P.mask && vec && lc0 + 8 <= G.ncol) {
+        if (P.mbits) {
+            // one byte holds the lane's 8 columns (lc0 and the tile's block
+            // origins are multiples of 8); bits past the tile's edge are dropped
+            const unsigned b = P.mbits[(G.r0 + r - P.row0) * P.mbstride + ((G.c0 - P.col0 + lc0) >> 3)];
+            const int nv = min(8, max(0, G.ncol - lc0));
+            valid |= (b & ((1u << nv) - 1u)) << (i * 8);
+        } else if (P.mask && vec && lc0 + 8 <= G.ncol) {
             const float4 a = __ldg(reinterpret_cast<const float4*>(P.mask + o));
             const float4 b = __ldg(reinterpret_cast<const float4*>(P.mask + o + 4));
             const float m8[8] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w};
@@ -1019,8 +1036,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
     bool mine = false;
     for (int k = 0; k < 32 && !mine; k++) {
         const int r = wr * 16 + tr * 4 + (k >> 3), c = wc * 64 + tc * 8 + (k & 7);
-        mine = r < G.nrow && c < G.ncol &&
-               (!P.mask || P.mask[(G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0)] != P.nodata);
+        mine = r < G.nrow && c < G.ncol && cell_valid(P, G.r0 + r - P.row0, G.c0 + c - P.col0);
     }
     if (__syncthreads_or(mine) && G.any) {
         int64_t seq = 0;
@@ -1064,8 +1080,7 @@ __global__ void __launch_bounds__(kThreads, 2) k_density_fp64(DParams P) {
                 P.scratch[(size_t)it.slot * kCells + r * kBC + c] = v;
             } else {
                 const int64_t o = (G.r0 + r - P.row0) * P.nc + (G.c0 + c - P.col0);
-                const bool valid = !P.mask || P.mask[o] != P.nodata;
-                P.out[o] = valid ? (float)v : P.nodata;
+                P.out[o] = cell_valid(P, G.r0 + r - P.row0, G.c0 + c - P.col0) ? (float)v : P.nodata;
             }
         }
 }
@@ -1087,8 +1102,7 @@ __device__ __forceinline__ void merge_block(const DParams& P, int32_t blk, int s
         double v = 0.0;
         for (int s = s0; s < s1; s++) v += P.scratch[(size_t)s * kCells + e];
         const int64_t o = (r0 + r - P.row0) * P.nc + (c0 + c - P.col0);
-        const bool valid = !P.mask || P.mask[o] != P.nodata;
-        P.out[o] = valid ? (float)v : P.nodata;
+        P.out[o] = cell_valid(P, r0 + r - P.row0, c0 + c - P.col0) ? (float)v : P.nodata;
     }
 }
 
@@ -1399,6 +1413,13 @@ const int64_t* mgk_density_counts_host(mgk_ctx* ctx, int slot) {
 
 void mgk_density_set_tail_flag(mgk_dplan* D, unsigned* flag) {
     if (D) D->P.tail_flag = flag;
+}
+
+void mgk_density_set_mask_bits(mgk_dplan* D, const unsigned char* bits, int64_t stride) {
+    if (!D) return;
+    D->P.mask = nullptr;
+    D->P.mbits = bits;
+    D->P.mbstride = stride;
 }
 
 int mgk_density_stage(mgk_ctx* ctx, mgk_dplan* D, cudaStream_t s) {

@@ -37,8 +37,9 @@ struct mgk_ctx {
     double* d_sum = nullptr;                  // 256 doubles
     double* h_sum = nullptr;                  // pinned mirror
     // mapped page-locked staging of plans and counts (mgk_host_stage), in
-    // kStageSlots independent slots; h_stage[i] and d_stage[i] address the same bytes
-    static constexpr int kStageSlots = 3;
+    // kStageSlots independent slots; h_stage[i] and d_stage[i] address the same
+    // bytes.  Slot 3 holds the bit-packed density mask of mgk_kde_raster.
+    static constexpr int kStageSlots = 4;
     void* h_stage[kStageSlots] = {};
     void* d_stage[kStageSlots] = {};
     size_t h_stage_bytes[kStageSlots] = {};
@@ -289,6 +290,9 @@ int mgk_density_launch_split(mgk_ctx* ctx, mgk_dplan* plan, cudaStream_t s, cuda
                              bool* merged_on_s_merge);
 // The plan's density kernel sets *flag = 1 when its last CTA starts.
 void mgk_density_set_tail_flag(mgk_dplan* plan, unsigned* flag);
+// The plan's kernels read the tile's NoData mask as bits (device, 1 = valid,
+// row r at byte r * stride, column c at bit c % 8 of byte c / 8) instead of floats.
+void mgk_density_set_mask_bits(mgk_dplan* plan, const unsigned char* bits, int64_t stride);
 int mgk_launch_mark_boundary(mgk_ctx* ctx, mgk_raster* r);
 int mgk_raster_runs(mgk_ctx* ctx, mgk_raster* r);
 int mgk_launch_dist2(mgk_ctx* ctx, mgk_points* p, mgk_raster* r, double cap);
