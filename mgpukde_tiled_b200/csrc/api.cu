@@ -1074,9 +1074,24 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
         mgk_points_destroy(p);
         p = q;
     }
-    if (st == MGK_OK && edge_correction) st = mgk_raster_upload(c, eg, emask, &em);
-    // the first tile's mask travels while the points are prepared
-    if (st == MGK_OK && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
+    // The edge mask travels on the copy stream while the index is built from
+    // the points (its records take the edge weights once they are known).
+    float* d_em = nullptr;
+    const size_t b_em = edge_correction ? sizeof(float) * (size_t)eg->ncols * (size_t)eg->nrows : 0;
+    cudaEvent_t em_ready = nullptr;
+    if (st == MGK_OK && edge_correction) {
+        if ((st = mgk_alloc(c, (void**)&d_em, b_em)) == MGK_OK) {
+            ce = cudaEventCreateWithFlags(&em_ready, cudaEventDisableTiming);
+            if (ce == cudaSuccess) ce = cudaMemcpyAsync(d_em, emask, b_em, cudaMemcpyHostToDevice, pipe.h2d);
+            if (ce == cudaSuccess) ce = cudaEventRecord(em_ready, pipe.h2d);
+            if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster edge mask");
+        }
+        if (st == MGK_OK) st = mgk_raster_wrap(c, eg, d_em, &em);
+    }
+    // the first tile's float mask travels while the points are prepared (a
+    // packed band's bits follow the counts: the packer may still be at work)
+    if (st == MGK_OK && !packed && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
+    if (st == MGK_OK) st = mgk_index_build(c, p, hfix, 0.0f, &idx);
     if (st == MGK_OK) {
         if (edge_correction) {
             // distances exact up to 3 h_max: all the edge-weight short-circuit reads
@@ -1084,13 +1099,15 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
             if (h_pp)
                 for (int64_t i = 0; i < n; i++) hmax = std::max(hmax, h_pp[i]);
             const double reach = 3.0 * (double)hmax * (1.0 + 1e-6);
-            if ((st = mgk_boundary_dist_within(c, p, em, reach)) == MGK_OK)
-                st = mgk_edge_weights(c, p, em, hfix, evals ? &ev_edge : nullptr);
+            if ((ce = cudaStreamWaitEvent(c->stream, em_ready, 0)) != cudaSuccess)
+                st = mgk_cuda_fail(c, ce, "kde_raster edge mask");
+            if (st == MGK_OK && (st = mgk_boundary_dist_within(c, p, em, reach)) == MGK_OK &&
+                (st = mgk_edge_weights(c, p, em, hfix, evals ? &ev_edge : nullptr)) == MGK_OK)
+                st = mgk_index_refresh_weights(c, idx, p);
         } else {
-            st = mgk_edge_weights_unit(c, p);
+            st = mgk_edge_weights_unit(c, p);  // w * 1: the records built above hold the same weights
         }
     }
-    if (st == MGK_OK) st = mgk_index_build(c, p, hfix, 0.0f, &idx);
     if (st == MGK_OK && out_ew) {
         ce = cudaMemcpyAsync(out_ew, p->ew, sizeof(float) * n, cudaMemcpyDeviceToHost, c->stream);
         if (ce != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster ew");
@@ -1158,6 +1175,7 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
             (ce = cudaMemsetAsync(d_flag, 0, sizeof(unsigned) * ntiles, c->stream)) != cudaSuccess)
             st = mgk_cuda_fail(c, ce, "kde_raster flags");
         if (st == MGK_OK) st = mgk_density_counts_launch(c, idx, dg, row_lo, 0, nrows, dg->ncols, 0, c->stream);
+        if (st == MGK_OK && packed && (ce = mask_in(0)) != cudaSuccess) st = mgk_cuda_fail(c, ce, "kde_raster mask");
         if (st == MGK_OK && (ce = cudaStreamSynchronize(c->stream)) != cudaSuccess)
             st = mgk_cuda_fail(c, ce, "kde_raster plan");
         // the alternate stream follows the preparation on the context stream
@@ -1283,6 +1301,8 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
     }
     mgk_index_destroy(idx);
     mgk_raster_destroy(em);
+    if (d_em) mgk_free(c, d_em, b_em);
+    if (em_ready) cudaEventDestroy(em_ready);
     mgk_points_destroy(p);
     if (st == MGK_OK && evals) *evals = ev_den + ev_edge;
     return st;

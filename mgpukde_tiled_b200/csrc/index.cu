@@ -175,6 +175,25 @@ __global__ void k_bin_starts(int64_t n, const unsigned* __restrict__ keys, int64
     for (int64_t b = prev + 1; b <= cur; b++) start[b] = (int32_t)i;
 }
 
+// A record's weight: w * e, divided by h^2 TWO_PI for per-point bandwidths
+// (the per-point normalisation of the kernel).
+__device__ __forceinline__ float record_wk(const float* __restrict__ w, const float* __restrict__ ew,
+                                          const float* __restrict__ hpp, int32_t j) {
+    float wk = (w ? w[j] : 1.0f) * (ew ? ew[j] : 1.0f);
+    if (hpp) {
+        const float hh = hpp[j] * hpp[j];
+        wk = (float)((double)wk / ((double)hh * (double)MGK_TWO_PI_F));
+    }
+    return wk;
+}
+
+// The records' weights again, from the points' current edge weights.
+__global__ void k_refresh_wk(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ w,
+                             const float* __restrict__ ew, const float* __restrict__ hpp, MgkPt* __restrict__ out) {
+    const int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    if (i < n) out[i].wk = record_wk(w, ew, hpp, perm[i]);
+}
+
 __global__ void k_gather(int64_t n, const int32_t* __restrict__ perm, const float* __restrict__ x,
                          const float* __restrict__ y, const float* __restrict__ w,
                          const float* __restrict__ ew, const float* __restrict__ hpp, int qexp,
@@ -185,13 +204,11 @@ __global__ void k_gather(int64_t n, const int32_t* __restrict__ perm, const floa
     MgkPt r;
     mgk_qsplit(x[j], qexp, r.xh, r.xl);
     mgk_qsplit(y[j], qexp, r.yh, r.yl);
-    r.wk = (w ? w[j] : 1.0f) * (ew ? ew[j] : 1.0f);
+    r.wk = record_wk(w, ew, hpp, j);
     r.k2h = r.k2l = r.hh = 0.0f;
     if (hpp) {
         const float hh = hpp[j] * hpp[j];
         const double h2 = (double)hh;
-        // w * e / (h^2 TWO_PI): the per-point normalisation of the kernel
-        r.wk = (float)((double)r.wk / (h2 * (double)MGK_TWO_PI_F));
         const double k2 = MGK_LOG2E / (2.0 * h2);
         r.k2h = (float)k2;
         r.k2l = (float)(k2 - (double)r.k2h);
@@ -384,6 +401,16 @@ int mgk_index_zorder(mgk_ctx* ctx, const mgk_index* idx, int32_t* d_order) {
     mgk_free(ctx, v0, b_vals);
     mgk_free(ctx, cnt, b_cnt);
     if (e != cudaSuccess) return mgk_cuda_fail(ctx, e, "index_zorder");
+    return MGK_OK;
+}
+
+int mgk_index_refresh_weights(mgk_ctx* ctx, mgk_index* idx, const mgk_points* pts) {
+    if (!idx || !pts || idx->n != pts->n) return mgk_fail(ctx, MGK_ERR_INVALID, "index_refresh_weights: bad arguments");
+    if (idx->n == 0) return MGK_OK;
+    k_refresh_wk<<<(unsigned)((idx->n + 255) / 256), 256, 0, ctx->stream>>>(
+        idx->n, idx->perm, pts->w, pts->has_ew ? pts->ew : nullptr, idx->varh ? pts->h : nullptr, idx->pts);
+    MGK_CHECK_LAUNCH(ctx, "k_refresh_wk");
+    MGK_COUNT_LAUNCH(ctx, 1);
     return MGK_OK;
 }
 

@@ -239,6 +239,9 @@ __device__ __host__ __forceinline__ double mgk_h2(float h) {
 
 // ---- kernels launched across translation units ------------------------------
 int mgk_launch_index_build(mgk_ctx* ctx, const mgk_points* pts, float h, float bin_size, mgk_index* idx);
+// The index records' weights from the points' current edge weights (an index
+// built before the edge weights were known), stream-ordered on ctx->stream.
+int mgk_index_refresh_weights(mgk_ctx* ctx, mgk_index* idx, const mgk_points* pts);
 // d_order[k] = position of the k-th record of idx in Z-order of the bins (n entries, device).
 int mgk_index_zorder(mgk_ctx* ctx, const mgk_index* idx, int32_t* d_order);
 int mgk_launch_density(mgk_ctx* ctx, const mgk_index* idx, const mgk_grid* g, int64_t row0,
