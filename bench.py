@@ -429,7 +429,10 @@ def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_b
         out["traffic_note"] = ("dram__bytes_read.sum + dram__bytes_write.sum of one full-size launch, from the ncu "
                                "capture summarised in profiles/k_density_traffic.txt (not measured in this run)")
     # the pipe utilisation behind frac (frac counts 8 flop-equivalents per in-cutoff pair, not issued ops)
-    out["pipes_ncu"] = {"fma_pct": 30.9, "alu_pct": 31.9, "xu_pct": 17.4, "lsu_pct": 16.6, "issue_active_pct": 59.0,
+    # (fma_pct: FMA-pipe instruction issue; fma_cycles_pct: cycles the FMA pipe is busy, in which a packed
+    # f32x2 instruction counts twice)
+    out["pipes_ncu"] = {"fma_pct": 30.4, "fma_cycles_pct": 40.7, "alu_pct": 33.5, "xu_pct": 13.8, "lsu_pct": 21.0,
+                        "issue_active_pct": 71.0, "thread_inst_per_eval": 5.0,
                         "source": "ncu --set full of one half-scale launch, profiles/k_density_single_large_half.md "
                                   "(not measured in this run)"}
     if hbm_gbs:
