@@ -902,6 +902,10 @@ static void pack_mask_row(const float* src, int64_t n, float nodata, unsigned ch
     for (; b < bytes; b++) dst[b] = 0;
 }
 
+#ifndef MGK_MASK_PACK_THREADS
+#define MGK_MASK_PACK_THREADS 8  // at most this many, and at most half the host's hardware threads
+#endif
+
 class MaskPacker {
   public:
     // rows [band_r0[k] - row_lo, band_r0[k + 1] - row_lo) of src form band k
@@ -919,7 +923,7 @@ class MaskPacker {
                 chunks_.push_back({k, r - row_lo, std::min<int64_t>(band_r0[k + 1], r + kChunk) - r});
         }
         const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-        const int nt = (int)std::min<unsigned>(8, std::max(1u, hw / 2));
+        const int nt = (int)std::min<unsigned>(MGK_MASK_PACK_THREADS, std::max(1u, hw / 2));
         for (int t = 0; t < nt; t++) threads_.emplace_back([this] { work(); });
     }
     ~MaskPacker() {
@@ -1207,8 +1211,7 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
             if (packed)
                 mgk_density_set_mask_bits(band_plans[k], reinterpret_cast<const unsigned char*>(d_mask[db]), mstride);
             if (two) mgk_density_set_tail_flag(band_plans[k], d_flag + k);
-            ce = mask_in(k + kDepth - 1);
-            if (ce == cudaSuccess && dmask) ce = cudaStreamWaitEvent(ks, pipe.mask_ready[db], 0);
+            ce = dmask ? cudaStreamWaitEvent(ks, pipe.mask_ready[db], 0) : cudaSuccess;
             if (ce == cudaSuccess && k >= kDepth) ce = cudaStreamWaitEvent(ks, pipe.out_free[db], 0);
             if (ce != cudaSuccess) {
                 st = mgk_cuda_fail(c, ce, "kde_raster tile");
@@ -1228,6 +1231,9 @@ static int kde_raster_rows(mgk_ctx* c, int64_t n, const float* x, const float* y
             }
             ce = cudaEventRecord(pipe.done[db], merged_on_mrg ? pipe.mrg : ks);
             if (ce == cudaSuccess) ce = out_copy(k);
+            // the mask of band k + kDepth - 1 (into the buffer band k - 1 read),
+            // after band k is queued: a packed band may still be at the packer
+            if (ce == cudaSuccess) ce = mask_in(k + kDepth - 1);
             if (ce != cudaSuccess) {
                 st = mgk_cuda_fail(c, ce, "kde_raster tile");
                 break;

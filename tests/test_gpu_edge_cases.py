@@ -164,3 +164,31 @@ def test_single_point(ctx):
     dg = o.grid(21, 21, 0.0, 0.0, 1.0, NODATA)
     den, ref = check_raster(ctx, [10.3], [10.6], [2.0], 2.0, dg, None)
     assert den.max() > 0 and np.count_nonzero(den) == np.count_nonzero(ref)
+
+
+@pytest.mark.parametrize("ncols,nrows", [(1005, 700), (13, 600), (257, 1100)])
+def test_band_path_mask_as_bits(ctx, ncols, nrows):
+    """Full-width bands (no tile side) send the NoData mask as bits, packed on
+    host threads: ragged widths (row padding to 128 columns), a short last
+    band, NoData runs and scattered NoData cells."""
+    dg = o.grid(ncols, nrows, 0.0, 0.0, 1.0, NODATA)
+    r = np.random.default_rng(ncols + nrows)
+    x = r.uniform(0, ncols, 1500).astype(np.float32)
+    y = r.uniform(0, nrows, 1500).astype(np.float32)
+    m = np.ones((nrows, ncols), np.float32)
+    m[r.random((nrows, ncols)) < 0.1] = NODATA
+    m[nrows // 3: nrows // 3 + 70, : ncols // 2] = NODATA
+    check_raster(ctx, x, y, r.lognormal(0, 0.5, len(x)), 6.0, dg, m, tile=0)
+
+
+def test_band_path_nan_nodata(ctx):
+    """A NaN NoData value marks no cell as NoData (x != NaN holds for every
+    x), in the packed bits as in the float kernels."""
+    dg = o.grid(300, 600, 0.0, 0.0, 1.0, float("nan"))
+    r = np.random.default_rng(11)
+    x = r.uniform(0, 300, 800).astype(np.float32)
+    y = r.uniform(0, 600, 800).astype(np.float32)
+    m = np.ones((600, 300), np.float32)
+    m[::7, ::3] = np.nan
+    den, ref = check_raster(ctx, x, y, np.ones_like(x), 5.0, dg, m, tile=0)
+    assert np.isfinite(den).all()
