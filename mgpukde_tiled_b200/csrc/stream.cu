@@ -24,6 +24,14 @@
 
 #include "mgk_internal.cuh"
 
+// device result buffers in flight: tile k computes into buffer k % kOutBufs
+// while the copies of the tiles before it leave
+#ifndef MGK_STREAM_OUT_BUFS
+#define MGK_STREAM_OUT_BUFS 3
+#endif
+constexpr int kOutBufs = MGK_STREAM_OUT_BUFS;
+static_assert(kOutBufs >= 2 && kOutBufs <= 3, "the copy slots are three");
+
 namespace {
 
 struct Slot {
@@ -80,13 +88,13 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
     const int64_t ntx = (g->ncols + tc - 1) / tc, nty = (g->nrows + tr - 1) / tr;
     const size_t tb = sizeof(float) * (size_t)tr * (size_t)tc;
     cudaStream_t cs = nullptr;
-    float *d_out[2] = {nullptr, nullptr}, *d_mask = nullptr, *h_mask = nullptr;
-    cudaEvent_t ev_den[2] = {nullptr, nullptr}, ev_mask = nullptr;
+    float *d_out[kOutBufs] = {}, *d_mask = nullptr, *h_mask = nullptr;
+    cudaEvent_t ev_den[kOutBufs] = {}, ev_mask = nullptr;
     Slot slots[3];
     unsigned long long* d_ev = nullptr;
     int st = MGK_OK;
     if (cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) != cudaSuccess) return mgk_fail(c, MGK_ERR_CUDA, "stream");
-    for (int b = 0; b < 2 && st == MGK_OK; b++) {
+    for (int b = 0; b < kOutBufs && st == MGK_OK; b++) {
         st = mgk_alloc(c, (void**)&d_out[b], tb);
         if (st == MGK_OK && cudaEventCreateWithFlags(&ev_den[b], cudaEventDisableTiming) != cudaSuccess)
             st = mgk_fail(c, MGK_ERR_CUDA, "event");
@@ -163,7 +171,7 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
         const int b = (int)(k & 1);
         mgk_density_discard(c, plans[b]);  // tile k - 2's, whose kernels have ended
         plans[b] = nullptr;
-        return mgk_density_plan_counted(c, idx, g, r0, c0, nr, nc, mask_src ? d_mask : nullptr, d_out[b], d_ev,
+        return mgk_density_plan_counted(c, idx, g, r0, c0, nr, nc, mask_src ? d_mask : nullptr, d_out[k % kOutBufs], d_ev,
                                         1 + b, &plans[b]);
     };
     if (st == MGK_OK && !todo.empty() && (st = count_of(0)) == MGK_OK) {
@@ -181,7 +189,7 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
         }
         int64_t r0, c0, nr, nc;
         geom(t, r0, c0, nr, nc);
-        const int b = (int)(k_out & 1);
+        const int b = (int)(k_out % kOutBufs);
         // the mask tile: read on this thread, copied on the copy stream
         if (mask_src) {
             if (ev_mask && cudaEventSynchronize(ev_mask) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
@@ -190,7 +198,7 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
                 break;
             }
             // the previous density must be done with d_mask before it is overwritten
-            if (cudaStreamWaitEvent(cs, ev_den[b ^ 1], 0) != cudaSuccess ||
+            if (cudaStreamWaitEvent(cs, ev_den[(b + kOutBufs - 1) % kOutBufs], 0) != cudaSuccess ||
                 cudaMemcpyAsync(d_mask, h_mask, sizeof(float) * nr * nc, cudaMemcpyHostToDevice, cs) != cudaSuccess ||
                 cudaEventRecord(ev_mask, cs) != cudaSuccess) {
                 st = mgk_fail(c, MGK_ERR_CUDA, "density_stream: mask copy");
@@ -203,12 +211,12 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
             if (cudaEventRecord(counted, c->stream) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
         }
         if (mask_src && cudaStreamWaitEvent(c->stream, ev_mask, 0) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
-        // d_out[b] was last copied out two tiles ago: the copy stream's order covers it
-        if (k_out >= 2 && cudaStreamWaitEvent(c->stream, slots[(k_out - 2) % 3].copied, 0) != cudaSuccess) {
+        // d_out[b] was last copied out kOutBufs tiles ago
+        if (k_out >= (size_t)kOutBufs && cudaStreamWaitEvent(c->stream, slots[(k_out - kOutBufs) % 3].copied, 0) != cudaSuccess) {
             st = MGK_ERR_CUDA;
             break;
         }
-        if ((st = mgk_density_launch_plan(c, plans[b], c->stream))) break;
+        if ((st = mgk_density_launch_plan(c, plans[k_out & 1], c->stream))) break;
         if (cudaEventRecord(ev_den[b], c->stream) != cudaSuccess) { st = MGK_ERR_CUDA; break; }
         if (direct) {
             if (cudaStreamWaitEvent(cs, ev_den[b], 0) != cudaSuccess ||
@@ -273,7 +281,7 @@ extern "C" int mgk_density_stream(mgk_ctx* c, const mgk_index* idx, const mgk_gr
         if (cudaMemcpy(&v, d_ev, sizeof(v), cudaMemcpyDeviceToHost) != cudaSuccess) st = MGK_ERR_CUDA;
         *evals = (int64_t)v;
     }
-    for (int b = 0; b < 2; b++) {
+    for (int b = 0; b < kOutBufs; b++) {
         mgk_free(c, d_out[b], tb);
         if (ev_den[b]) cudaEventDestroy(ev_den[b]);
     }
