@@ -1219,10 +1219,28 @@ void plan_tile(const int64_t* counts, int nbx_t, int nby_t, int sm_count, int wa
     T.split_begin.push_back(T.nslots);
 }
 
-// heaviest items first (they are the tail otherwise)
+// Heaviest items first (they are the tail otherwise); equal weights keep
+// their order.  A stable LSD radix sort on (largest weight - weight), 8 bits a
+// pass and only as many passes as the largest weight needs: the order
+// std::stable_sort gives, in linear time (the plan of a 10^4^2 raster sorts
+// about 13,000 items while the GPU waits).
 void sort_items(std::vector<Item>& items) {
-    std::stable_sort(items.begin(), items.end(),
-                     [](const Item& a, const Item& b) { return (a.k1 - a.k0) > (b.k1 - b.k0); });
+    const size_t n = items.size();
+    if (n < 2) return;
+    uint32_t wmax = 0;
+    for (const Item& it : items) wmax = std::max<uint32_t>(wmax, (uint32_t)(it.k1 - it.k0));
+    std::vector<Item> tmp(n);
+    Item *src = items.data(), *dst = tmp.data();
+    bool in_tmp = false;
+    for (int shift = 0; shift < 32 && (wmax >> shift) != 0; shift += 8) {
+        size_t cnt[257] = {};
+        for (size_t i = 0; i < n; i++) cnt[((wmax - (uint32_t)(src[i].k1 - src[i].k0)) >> shift & 0xffu) + 1]++;
+        for (int d = 0; d < 256; d++) cnt[d + 1] += cnt[d];
+        for (size_t i = 0; i < n; i++) dst[cnt[(wmax - (uint32_t)(src[i].k1 - src[i].k0)) >> shift & 0xffu]++] = src[i];
+        std::swap(src, dst);
+        in_tmp = !in_tmp;
+    }
+    if (in_tmp) items.swap(tmp);
 }
 
 }  // namespace
