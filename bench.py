@@ -443,6 +443,42 @@ def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_b
     return out
 
 
+def algo_roofline(evals, seconds, scope, device):
+    """Roofline object of a workload whose time is several kernels: its
+    algorithmic rate (8 flop-equivalents per in-cutoff pair, as for the
+    density kernel) over `seconds` against the nominal FP32 peak.  `scope`
+    says which kernels the time covers."""
+    import torch
+
+    peaks, peak_kind = load_peaks()
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    nsm = torch.cuda.get_device_properties(device).multi_processor_count
+    fp32_peak = nsm * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = evals * FLOP_PER_EVAL / seconds / 1e12
+    return {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak,
+            "traffic": None, "flop_per_eval": FLOP_PER_EVAL, "scope": scope,
+            "peak_note": f"nominal FP32 FMA peak {nsm} SMs x 128 lanes x 2 x {sm_max:.0f} MHz "
+                         f"(MEASURED_PEAKS.json has no FP32 figure; its clocks are {peak_kind})"}
+
+
+def d2h_link_gbs(nbytes=256 << 20, reps=5):
+    """Measured device -> page-locked host copy rate (GB/s): the bound of a
+    workload that streams its output to host memory."""
+    import torch
+
+    dev = torch.empty(nbytes, dtype=torch.uint8, device="cuda")
+    host = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+    s = torch.cuda.current_stream()
+    host.copy_(dev, non_blocking=True)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    for _ in range(reps):
+        host.copy_(dev, non_blocking=True)
+    e1.record(s)
+    torch.cuda.synchronize()
+    return nbytes * reps / (e0.elapsed_time(e1) / 1e3) / 1e9
+
+
 def run_reference_arm(args):
     rank, world, _ = env_rank()
     if rank != 0:
@@ -822,7 +858,10 @@ def run_bandwidth_select(args):
                                       f"all-gather, leave-one-out sums by query share + all-reduce")},
            "evals_per_step": evals, "edge_evals": ev_edge, "loo_evals": ev_loo,
            "batch_ms": float(np.mean(loo_ms)), "argmax": best, "h_best": float(hgrid[best]),
-           "gpu_launches": launches, "clocks": clocks}
+           "gpu_launches": launches, "clocks": clocks,
+           "roofline": algo_roofline(evals, float(np.mean(loo_ms)) / 1e3,
+                                     "one LOO batch: per-h edge weights, k_loo_multi (about 90 % of it), prep, "
+                                     "finish and argmax (the batch's CUDA-event time)", local)}
     if rank == 0:
         if world == 1:
             unbind_numa()
@@ -961,7 +1000,9 @@ def run_adaptive(args):
            "search": {"h": h, "alpha": alpha, "lmax": lmax, "iterations": iters},
            "e2e": {"value": evals / (e2e_ms / 1e3), "unit": UNIT, "ms_per_step": e2e_ms,
                    "h2d_bytes_per_step": int(3 * 4 * n + c["edge_mask"].nbytes), "d2h_bytes_per_step": int(4 * n)},
-           "gpu_launches": launches, "clocks": clocks}
+           "gpu_launches": launches, "clocks": clocks,
+           "roofline": algo_roofline(evals, ms / 1e3, "one Hooke-Jeeves search: point densities, bandwidths, "
+                                                      "edge weights and leave-one-out sums of every step", local)}
     if not args.no_cpu_baseline:
         unbind_numa()
         mk.calc_dist2_boundary(ctx, pts, em)
@@ -1050,6 +1091,14 @@ def run_out_of_core(args):
            "evals_per_step": evals, "density_evals": ev_d, "edge_evals": ev_e,
            "output_bytes": int(host.nbytes), "output_gb_s": host.nbytes / (ms / 1e3) / 1e9,
            "gpu_launches": launches, "clocks": clocks}
+    # the job streams 6.4 GB to page-locked host memory: bound by the copy link
+    link = d2h_link_gbs()
+    achieved = host.nbytes / (ms / 1e3) / 1e9
+    out["roofline"] = {"bound": "d2h link", "achieved": achieved, "peak": link, "unit": "GB/s", "frac": achieved / link,
+                       "traffic": None, "algorithmic_bytes": int(host.nbytes),
+                       "peak_note": "device -> page-locked host copy rate measured in this run (256 MB, 5 copies)",
+                       "fp32_view": algo_roofline(total_evals, ms / 1e3, "the whole job (every kernel and copy)",
+                                                  local)}
     if rank == 0 and world == 1:
         unbind_numa()
         if not args.no_cpu_baseline:
