@@ -707,24 +707,29 @@ __device__ __forceinline__ void density_item(const DParams& P, const Item it) {
                     cutf = P.cutf;
                     epsd2 = P.epsd2;
                 }
-                // column groups in pairs (0, 1) and (2, 3): two entries in packed FP32
-                const unsigned ub = (pb | (pb >> 4)) & 0xfu;
+                // the summed column groups two at a time (the first two left,
+                // whichever they are), two entries in packed FP32; a last odd
+                // group alone
+                unsigned ub = (pb | (pb >> 4)) & 0xfu;
 #pragma unroll
                 for (int h2 = 0; h2 < 2; h2++) {
-                    const unsigned two = (ub >> (2 * h2)) & 3u;
-                    if (!two) continue;
-                    const int j0 = lane + 64 * h2, j1 = j0 + 32;
-                    if (two == 3u) {
+                    if (!ub) break;
+                    const int u0 = __ffs(ub) - 1;
+                    ub &= ub - 1u;
+                    const int j0 = lane + 32 * u0;
+                    if (ub) {
+                        const int u1 = __ffs(ub) - 1;
+                        ub &= ub - 1u;
+                        const int j1 = lane + 32 * u1;
                         float e0, e1, d20, d21;
                         exp2_pair2(__fsub_rn(r.xh, s_cxh[j0]), __fsub_rn(r.xh, s_cxh[j1]), __fsub_rn(r.xl, s_cxl[j0]),
                                    __fsub_rn(r.xl, s_cxl[j1]), k2h, k2l, e0, e1, d20, d21);
                         colE[col_slot(pk, j0)] = e0;
                         colE[col_slot(pk, j1)] = e1;
                     } else {
-                        const int j = two == 1u ? j0 : j1;
                         float ah, al, d2;
-                        exponent_pair(__fsub_rn(r.xh, s_cxh[j]), __fsub_rn(r.xl, s_cxl[j]), k2h, k2l, ah, al, d2);
-                        colE[col_slot(pk, j)] = exp2_pair(ah, al);
+                        exponent_pair(__fsub_rn(r.xh, s_cxh[j0]), __fsub_rn(r.xl, s_cxl[j0]), k2h, k2l, ah, al, d2);
+                        colE[col_slot(pk, j0)] = exp2_pair(ah, al);
                     }
                 }
                 const float pc0 = __fadd_rn(__fsub_rn(r.xh, s_cxh[0]), __fsub_rn(r.xl, s_cxl[0])) * inv_cs;
