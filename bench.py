@@ -431,8 +431,8 @@ def density_roofline(evals, kernel_s, nsm, sm_max_mhz, peak_kind, traffic, alg_b
     # the pipe utilisation behind frac (frac counts 8 flop-equivalents per in-cutoff pair, not issued ops)
     # (fma_pct: FMA-pipe instruction issue; fma_cycles_pct: cycles the FMA pipe is busy, in which a packed
     # f32x2 instruction counts twice)
-    out["pipes_ncu"] = {"fma_pct": 30.4, "fma_cycles_pct": 40.7, "alu_pct": 33.5, "xu_pct": 13.8, "lsu_pct": 21.0,
-                        "issue_active_pct": 71.0, "thread_inst_per_eval": 5.0,
+    out["pipes_ncu"] = {"fma_pct": 30.3, "fma_cycles_pct": 40.7, "alu_pct": 33.8, "xu_pct": 14.0, "lsu_pct": 21.7,
+                        "issue_active_pct": 71.2, "thread_inst_per_eval": 4.97,
                         "source": "ncu --set full of one half-scale launch, profiles/k_density_single_large_half.md "
                                   "(not measured in this run)"}
     if hbm_gbs:
