@@ -333,7 +333,7 @@ float mgk_rule_of_thumb(int64_t n, const float* x, const float* y, const float* 
 /* Launch-shape settings of a context.  bin_factor: index bin side / h when
  * mgk_index_build gets bin_size 0 (default 0.5); split_waves: the density
  * plan splits blocks into work items of at most total / (resident CTAs x
- * split_waves) candidates (default 8); tile_side: density tile side used by
+ * split_waves) candidates (default 4); tile_side: density tile side used by
  * mgk_kde_raster when its tile argument is 0 (0: the whole raster). */
 typedef struct mgk_tuning {
     float bin_factor;

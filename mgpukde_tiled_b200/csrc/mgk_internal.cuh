@@ -51,7 +51,7 @@ struct mgk_ctx {
     float last_loo_ms = 0.0f;
     // tuning (mgk_autotune / mgk_ctx_set_tuning)
     float bin_factor = 0.5f;   // default index bin side / h (fastest of 0.5-1.25 on the 1e6-point raster)
-    int split_waves = 8;       // density work items per resident CTA slot
+    int split_waves = 4;       // density work items per resident CTA slot (4 of 2-32 fastest on the C1 raster)
     int64_t tile_side = 0;     // streamed tile side (0: whole raster when it fits)
 };
 

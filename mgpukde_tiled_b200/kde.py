@@ -347,7 +347,7 @@ def get_tuning(ctx: Context) -> dict:
     return _tuning_dict(t)
 
 
-def set_tuning(ctx: Context, bin_factor=0.5, split_waves=8, tile_side=0):
+def set_tuning(ctx: Context, bin_factor=0.5, split_waves=4, tile_side=0):
     t = MgkTuning(float(bin_factor), int(split_waves), int(tile_side), 0.0, 0)
     ctx.check(lib().mgk_ctx_set_tuning(ctx.handle, C.byref(t)))
 
